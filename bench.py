@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""Benchmark: thick-restart Lanczos on the 3D Anderson model, 256^3.
+
+Workload (the configuration the headline metric is quoted on): real
+symmetric FP64 operator, periodic 7-point stencil with hopping -1 and a
+seeded diagonal potential uniform[-2, 2] (W = 4), n = 16,777,216, CSR
+(117.4M entries); smallest ned = 32 eigenpairs, maxlan = 128, tol = 1e-8,
+start vector seeded uniform[-1, 1].
+
+A step is one trlan() call bounded to one thick-restart cycle
+(maxmv = maxlan = 128): 128 Lanczos steps, each one fused SpMV + alpha, one
+full classical Gram-Schmidt pass against the growing basis (1..128 vectors),
+normalisation, then the Ritz recombination V*Y of the 32 wanted vectors.
+The metric is Lanczos steps (matvec + full reorthogonalisation) per second.
+
+* value: device-resident inputs (CSR and evec on the GPU before timing).
+* e2e:   the same call through the C ABI with host buffers: the CSR arrays
+         and the start vector are copied host->device and the eigenvectors
+         device->host inside the timed region, every step.
+* roofline: the dominant kernel's algorithmic bytes / its CUDA-event time
+         measured inside the engine on its own stream (trlx_options.profile).
+* cpu_baseline / --impl reference: the reference nuTRLan library
+         (oracle/_ref, built from the reference sources with OpenBLAS) on the
+         same operator with a compiled OpenMP CSR callback, on a bounded
+         sample: the first 32 Lanczos steps (maxlan = maxmv = 32) of the same
+         solve.  The sample's basis is 4x smaller on average than a full
+         cycle's, so per-step CPU throughput is overstated, not understated.
+
+Inputs (basis >= 4 GB, CSR 1.4 GB) exceed the 126 MB L2 between steps.
+Multi-GPU (N > 1): every rank solves its own replica (different potential
+seed), no collective in the data path ("replicas only", weak scaling).
+"""
+import os
+
+os.environ.setdefault("OMP_WAIT_POLICY", "PASSIVE")
+
+import argparse
+import ctypes as C
+import json
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "anderson256": dict(kind="anderson", L=256, W=4.0, ned=32, maxlan=128, tol=1e-8),
+    "anderson128": dict(kind="anderson", L=128, W=4.0, ned=32, maxlan=128, tol=1e-8),
+    "laplace128": dict(kind="laplace", L=128, ned=10, maxlan=64, tol=1.4901e-8),
+}
+
+
+def build_operator(w, seed):
+    from nutrlan_b200 import operators as ops
+    if w["kind"] == "anderson":
+        return ops.anderson_3d(w["L"], W=w["W"], seed=seed)
+    return ops.laplacian_2d(w["L"])
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference_sample(A, w, x0, sample_steps):
+    """Reference trlan (CPU) on the first `sample_steps` Lanczos steps."""
+    from oracle import ref
+    ref.build()
+    r = ref.trlan_csr(A, ned=w["ned"], maxlan=sample_steps, lohi=-1, tol=w["tol"], restart=1,
+                      maxmv=sample_steps, start=x0, mev=w["ned"] + 1)
+    return r["info"].matvec, r["seconds"]
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        backend = "nccl" if args.impl == "b200" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reduce_max(pg, value, device):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="anderson256")
+    ap.add_argument("--basis-bits", type=int, choices=[64, 32], default=64)
+    ap.add_argument("--format", choices=["csr", "sell"], default="csr")
+    ap.add_argument("--cpu-sample", type=int, default=32,
+                    help="Lanczos steps in the bounded CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    world, rank, local, pg = dist_setup(args)
+    seed = 2024 + rank
+    metric = f"Lanczos steps/s (SpMV + full CGS reorth), {args.workload}, smallest {w['ned']}"
+    config = {"workload": f"{args.workload}: n={w['L'] ** (3 if w['kind'] == 'anderson' else 2)}, "
+                          f"ned={w['ned']}, maxlan={w['maxlan']}, tol={w['tol']}, "
+                          f"{args.format.upper()}, basis fp{args.basis_bits}, one thick-restart cycle/step",
+              "global_batch": world, "parallelism": f"replicas x{world}",
+              "l2": "inputs larger than L2 (basis >= 4 GB, CSR >= 1 GB)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        A = build_operator(w, seed)
+        from nutrlan_b200 import operators as ops
+        x0 = ops.start_vector(A.n)
+        times, mvs = [], []
+        for s in range(args.warmup + args.steps):
+            mv, dt = run_reference_sample(A, w, x0, args.cpu_sample)
+            if s >= args.warmup:
+                times.append(dt)
+                mvs.append(mv)
+        val = sum(mvs) / sum(times)
+        cores = os.cpu_count()
+        line = {"impl": "reference", "metric": metric, "value": val, "unit": "steps/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config,
+                "cpu_baseline": {"value": val, "unit": "steps/s", "cores": cores, "kind": "reference",
+                                 "sample": f"reference trlan, first {args.cpu_sample} Lanczos steps "
+                                           f"(maxlan=maxmv={args.cpu_sample}) of the same solve, "
+                                           "OpenBLAS + OpenMP CSR callback"},
+                "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from nutrlan_b200 import load, TrlInfo, TrlxOptions, TrlxStats, DeviceOperator
+    from nutrlan_b200 import operators as ops
+    lib = load()
+
+    A = build_operator(w, seed)
+    n = A.n
+    x0 = ops.start_vector(n)
+    ned, maxlan, tol = w["ned"], w["maxlan"], w["tol"]
+    mev = ned + 1
+    steps_per_call = maxlan
+
+    opts = TrlxOptions()
+    lib.trlx_default_options(C.byref(opts))
+    opts.basis_bits = args.basis_bits
+    opts.profile = 1
+    stats = TrlxStats()
+
+    # ---- device-resident arm -------------------------------------------------
+    op = DeviceOperator(A, fmt=args.format)
+    evec = torch.zeros((mev, n), dtype=torch.float64, device=dev)
+    x0_dev = torch.as_tensor(x0, device=dev)
+    eval_ = np.zeros(mev)
+    wrk = np.zeros(mev)
+
+    def one_call(info):
+        lib.trl_init_info(C.byref(info), n, maxlan, -1, ned, tol, 1, steps_per_call, None)
+        info.mvparam = op.handle.value
+        lib.trl_set_iguess(C.byref(info), 0, 1, 0, None)
+        evec[0].copy_(x0_dev)
+        lib.trlx_trlan(op.applier, None, C.byref(info), n, mev, eval_.ctypes.data, evec.data_ptr(), n,
+                       mev, wrk.ctypes.data, C.byref(opts))
+        if info.stat != 0:
+            raise RuntimeError(f"trlan stat {info.stat}")
+
+    info = TrlInfo()
+    for _ in range(args.warmup):
+        one_call(info)
+    torch.cuda.synchronize()
+    barrier(pg)
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ktot = np.zeros(8)
+    kbyt = np.zeros(8)
+    kcnt = np.zeros(8)
+    launches = 0
+    matvecs = 0
+    torch.cuda.synchronize()
+    ev0.record()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one_call(info)
+        lib.trlx_get_last_stats(C.byref(stats))
+        ktot += np.array(stats.kernel_seconds[:])
+        kbyt += np.array(stats.kernel_bytes[:])
+        kcnt += np.array(stats.kernel_count[:])
+        launches += stats.kernel_launches
+        matvecs += info.matvec
+    ev1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    dev_s = ev0.elapsed_time(ev1) * 1e-3
+    elapsed = reduce_max(pg, dev_s, dev)
+    total_steps = reduce_max(pg, matvecs, dev) * world
+    value = total_steps / elapsed
+    ms_per_step = 1e3 * elapsed / args.steps
+
+    # roofline: dominant kernel class by time
+    names = ["spmv", "project", "update", "normalize", "ritz", "dot", "other", "x"]
+    dom = int(np.argmax(ktot))
+    peak, peak_kind = read_peaks()
+    achieved = kbyt[dom] / ktot[dom] / 1e9 if ktot[dom] > 0 else 0.0
+    traffic = None
+    prof_path = os.path.join(ROOT, "profiles", f"traffic_{names[dom]}_{args.workload}_fp{args.basis_bits}.json")
+    if os.path.exists(prof_path):
+        try:
+            with open(prof_path) as f:
+                tr = json.load(f)
+            # dram bytes per algorithmic byte, scaled to this run's average launch
+            traffic = tr["dram_bytes_per_alg_byte"] * kbyt[dom] / max(kcnt[dom], 1)
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "peak_source": peak_kind,
+                "alg_bytes_per_launch": kbyt[dom] / max(kcnt[dom], 1),
+                "launches": int(kcnt[dom]),
+                "per_kernel": {names[i]: {"seconds": ktot[i], "GB/s": (kbyt[i] / ktot[i] / 1e9) if ktot[i] else 0,
+                                          "launches": int(kcnt[i])}
+                               for i in range(7) if kcnt[i]},
+                "spmv_plus_reorth_GBps": float((kbyt[0] + kbyt[1] + kbyt[2]) /
+                                               max(ktot[0] + ktot[1] + ktot[2], 1e-30) / 1e9)}
+    op_obj_bytes = A.row_ptr.nbytes + A.col.nbytes + A.val.nbytes
+
+    # ---- end-to-end arm: host buffers through the C ABI ----------------------
+    e2e = None
+    if not args.no_e2e:
+        rp = np.ascontiguousarray(A.row_ptr)
+        ci = np.ascontiguousarray(A.col)
+        va = np.ascontiguousarray(A.val)
+        hev = np.zeros((mev, n))
+        handle = C.c_void_p()
+        applier = op.applier
+
+        def e2e_call():
+            handle.value = None
+            lib.trlx_csr_create(n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, 0, C.byref(handle))
+            inf = TrlInfo()
+            lib.trl_init_info(C.byref(inf), n, maxlan, -1, ned, tol, 1, steps_per_call, None)
+            inf.mvparam = handle.value
+            lib.trl_set_iguess(C.byref(inf), 0, 1, 0, None)
+            hev[0] = x0
+            lib.trlx_trlan(applier, None, C.byref(inf), n, mev, eval_.ctypes.data, hev.ctypes.data, n, mev,
+                           wrk.ctypes.data, C.byref(opts))
+            lib.trlx_operator_destroy(handle)
+            return inf.matvec
+
+        e2e_call()
+        torch.cuda.synchronize()
+        barrier(pg)
+        t0 = time.perf_counter()
+        mv = 0
+        for _ in range(args.steps):
+            mv += e2e_call()
+        torch.cuda.synchronize()
+        e_wall = reduce_max(pg, time.perf_counter() - t0, dev)
+        e2e = {"value": reduce_max(pg, mv, dev) * world / e_wall, "unit": "steps/s",
+               "h2d_bytes_per_step": int(op_obj_bytes + 8 * n),
+               "d2h_bytes_per_step": int(8 * n * mev + 8 * mev)}
+
+    op.close()
+    del evec
+    torch.cuda.empty_cache()
+
+    # ---- CPU baseline (rank 0, N = 1) ----------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            mv, dt = run_reference_sample(A, w, x0, args.cpu_sample)
+            cpu = {"value": mv / dt, "unit": "steps/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"reference trlan, first {args.cpu_sample} Lanczos steps "
+                             f"(maxlan=maxmv={args.cpu_sample}) of the same solve, OpenBLAS + OpenMP CSR callback",
+                   "seconds": dt}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {"metric": metric, "value": value, "unit": "steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded Anderson potential and start vector)", "config": config,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clocks, "host_wall_s": wall,
+                "matvecs_per_call": int(matvecs // max(args.steps, 1))}
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,150 @@
+/*
+ * trlx.h -- extensions of the B200 Lanczos engine that have no counterpart
+ * in the reference API.  The reference's own entry points (trlan.h,
+ * ztrlan.h) are unchanged; everything new lives in trlx_* functions so that
+ * trl_info keeps its layout.
+ */
+#ifndef TRLAN_B200_TRLX_H
+#define TRLAN_B200_TRLX_H
+
+#include "trlan.h"
+#include "ztrlan.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------------
+ * Built-in device operators.  Passing trlx_matvec (or trlx_zmatvec) as `op`
+ * with info->mvparam pointing at a trlx_operator lets the engine run its
+ * fused kernel (sparse product + alpha dot in one pass) instead of a
+ * callback; called directly they behave like any trl_matvec on device
+ * pointers.  Matrices are square, rows/columns 0-based, CSR row pointers
+ * 64-bit.
+ * ------------------------------------------------------------------------- */
+typedef struct trlx_operator trlx_operator;
+
+#define TRLX_HOST_ARRAYS 0   /* input arrays live in host memory   */
+#define TRLX_DEVICE_ARRAYS 1 /* input arrays are device pointers   */
+
+/* Real CSR (values FP64).  Returns 0 or a negative error code. */
+int trlx_csr_create(int nrow, const long long *row_ptr, const int *col_idx,
+                    const double *val, int where, trlx_operator **out);
+
+/* Real SELL-C-sigma (C = 32) built from CSR input; sigma >= 1 is the
+   row-sorting window (1 keeps the natural order). */
+int trlx_sell_create(int nrow, const long long *row_ptr, const int *col_idx,
+                     const double *val, int sigma, int where,
+                     trlx_operator **out);
+
+/* Complex CSR (values complex128). */
+int trlx_zcsr_create(int nrow, const long long *row_ptr, const int *col_idx,
+                     const trl_dcomplex *val, int where,
+                     trlx_operator **out);
+
+void trlx_operator_destroy(trlx_operator *op);
+
+/* Number of stored entries (including SELL padding) and rows. */
+long long trlx_operator_nnz(const trlx_operator *op);
+int trlx_operator_nrow(const trlx_operator *op);
+
+/* trl_matvec / ztrl_matvec compatible appliers (device x, y). */
+void trlx_matvec(const int nrow, const int ncol, const double *x,
+                 const int ldx, double *y, const int ldy, void *mvparam);
+void trlx_zmatvec(const int nrow, const int ncol, const trl_dcomplex *x,
+                  const int ldx, trl_dcomplex *y, const int ldy,
+                  void *mvparam);
+
+/* ---------------------------------------------------------------------------
+ * Solver options.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    int basis_bits;          /* 64: FP64 (c128) basis; 32: FP32 (c64)     */
+    unsigned long long seed; /* seed of the counter-based random restarts */
+    void *stream;            /* cudaStream_t to run on; NULL: own stream  */
+    int refine;              /* 1: FP64 Rayleigh-Ritz refinement of the
+                                returned pairs (default 1 for 32-bit)      */
+    int profile;             /* 1: time every kernel class with CUDA events
+                                (fills trlx_stats.kernel_*)                */
+} trlx_options;
+
+void trlx_default_options(trlx_options *opts);
+
+/* trlan()/ztrlan() with explicit options (NULL = defaults). */
+void trlx_trlan(trl_matvec op, trl_uo user_ortho, trl_info *info, int nrow,
+                int mev, double *eval, double *evec, int lde, int lwrk,
+                double *wrk, const trlx_options *opts);
+void trlx_ztrlan(ztrl_matvec op, trl_info *info, int nrow, int mev,
+                 double *eval, trl_dcomplex *evec, int lde,
+                 trl_dcomplex *misc, int nmis, double *dwrk, int ldwrk,
+                 const trlx_options *opts);
+
+/* Statistics of the last solve issued from the calling thread. */
+typedef struct {
+    double seconds_total;     /* wall time of the solve                    */
+    double seconds_op;        /* device time in the operator               */
+    double seconds_orth;      /* device time in Gram-Schmidt               */
+    double seconds_restart;   /* restart (host small dense + V*Y)          */
+    double basis_bytes;       /* algorithmic bytes moved by Gram-Schmidt
+                                 and restart kernels                        */
+    double op_bytes;          /* algorithmic bytes of built-in operators   */
+    long long kernel_launches;/* kernels launched by the engine            */
+    int cgs_passes;           /* Gram-Schmidt passes (== info->north)      */
+    int host_syncs;           /* host/device synchronisations              */
+    double max_true_residual; /* refinement: max ||Az - theta z||, or -1   */
+    /* Per kernel class (TRLX_K_*), filled when trlx_options.profile is set:
+       device seconds (CUDA events on the solver's stream), algorithmic
+       bytes moved, and launches. */
+    double kernel_seconds[8];
+    double kernel_bytes[8];
+    long long kernel_count[8];
+} trlx_stats;
+
+#define TRLX_K_SPMV 0      /* built-in operator (+ fused alpha)          */
+#define TRLX_K_PROJECT 1   /* Gram-Schmidt projection h = V^H r          */
+#define TRLX_K_UPDATE 2    /* Gram-Schmidt update r - V h                */
+#define TRLX_K_NORMALIZE 3 /* scaling / storing the new basis vector     */
+#define TRLX_K_RITZ 4      /* restart recombination V Y                  */
+#define TRLX_K_DOT 5       /* standalone dot products                    */
+#define TRLX_K_OTHER 6
+
+void trlx_get_last_stats(trlx_stats *stats);
+
+/* Version string of the library. */
+const char *trlx_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Host-side building blocks, exported for inspection and CPU tests.  They
+ * are the engine's own FP64 routines for the projected problem.
+ * ------------------------------------------------------------------------- */
+/* Ritz values (ascending) and residual estimates of the tridiagonal
+   (alpha, beta) with the first `locked` values treated as locked. */
+int trlx_host_get_eval(int nd, int locked, const double *alpha,
+                       const double *beta, double *lambda, double *res);
+/* Eigenvalues (ascending) and last eigenvector components of a symmetric
+   tridiagonal matrix (diag d[n], off-diagonal e[n-1]). */
+int trlx_host_tridiag_eig_last(int n, const double *d, const double *e,
+                               double *lambda, double *zlast);
+/* Arrow matrix -> tridiagonal with rotation (nd x nd, column-major). */
+int trlx_host_arrow_to_tridiag(int nd, const double *alpha,
+                               const double *beta, double *rot,
+                               double *alfrot, double *betrot);
+/* Symmetric eigen-decomposition in place (A n x n column-major). */
+int trlx_host_sym_eig(int n, double *A, int lda, double *w);
+/* Restart decision: kept pairs (and info->klan for schemes 7/8). */
+void trlx_host_shuffle_eig(int nd, int mnd, double *lambda, double *res,
+                           trl_info *info, int *kept, int locked);
+void trlx_host_convergence_test(int nd, double *lambda, double *res,
+                                trl_info *info, double *wrk);
+void trlx_host_sort_eig(int nd, int lohi, int nec, double ref,
+                        double *lambda, double *res);
+void trlx_host_set_locking(int jnd, int nlam, double *lambda, double *res,
+                           double *yy, double anrm, int *locked);
+/* Paired shell sort, ascending in key. */
+void trlx_host_sort2(int n, double *key, double *other);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TRLAN_B200_TRLX_H */

@@ -1,0 +1,106 @@
+"""Loader for the in-tree libtrlan_b200.so.
+
+The library must have been built (``python -c "import __graft_entry__ as g;
+g.build()"`` or ``make -C nutrlan_b200/csrc``).  There is no fallback: a
+missing or unloadable library raises ImportError.
+"""
+import ctypes as C
+import os
+
+from ._abi import (TrlInfo, MATVEC, USER_ORTHO, declare_common, c_int, c_double,
+                   c_void_p)
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib",
+                        "libtrlan_b200.so")
+
+
+class TrlxStats(C.Structure):
+    _fields_ = [
+        ("seconds_total", c_double), ("seconds_op", c_double),
+        ("seconds_orth", c_double), ("seconds_restart", c_double),
+        ("basis_bytes", c_double), ("op_bytes", c_double),
+        ("kernel_launches", C.c_longlong), ("cgs_passes", c_int),
+        ("host_syncs", c_int), ("max_true_residual", c_double),
+        ("kernel_seconds", c_double * 8), ("kernel_bytes", c_double * 8),
+        ("kernel_count", C.c_longlong * 8),
+    ]
+
+    KERNEL_CLASSES = ("spmv", "project", "update", "normalize", "ritz", "dot", "other")
+
+    def kernels(self):
+        """{class: (seconds, bytes, launches)} for the profiled classes."""
+        return {name: (self.kernel_seconds[i], self.kernel_bytes[i], self.kernel_count[i])
+                for i, name in enumerate(self.KERNEL_CLASSES) if self.kernel_count[i]}
+
+
+class TrlxOptions(C.Structure):
+    _fields_ = [("basis_bits", c_int), ("seed", C.c_ulonglong),
+                ("stream", c_void_p), ("refine", c_int), ("profile", c_int)]
+
+
+def _declare(lib):
+    declare_common(lib)
+    P = C.POINTER
+    lib.trlx_trlan.argtypes = list(lib.trlan.argtypes) + [P(TrlxOptions)]
+    lib.trlx_trlan.restype = None
+    lib.trlx_ztrlan.argtypes = list(lib.ztrlan.argtypes) + [P(TrlxOptions)]
+    lib.trlx_ztrlan.restype = None
+    lib.trlx_default_options.argtypes = [P(TrlxOptions)]
+    lib.trlx_default_options.restype = None
+    lib.trlx_get_last_stats.argtypes = [P(TrlxStats)]
+    lib.trlx_get_last_stats.restype = None
+    lib.trlx_version.restype = C.c_char_p
+    for name in ("trlx_csr_create", "trlx_zcsr_create"):
+        f = getattr(lib, name)
+        f.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_int, P(c_void_p)]
+        f.restype = c_int
+    lib.trlx_sell_create.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_int, c_int,
+                                     P(c_void_p)]
+    lib.trlx_sell_create.restype = c_int
+    lib.trlx_operator_destroy.argtypes = [c_void_p]
+    lib.trlx_operator_destroy.restype = None
+    lib.trlx_operator_nnz.argtypes = [c_void_p]
+    lib.trlx_operator_nnz.restype = C.c_longlong
+    lib.trlx_operator_nrow.argtypes = [c_void_p]
+    lib.trlx_operator_nrow.restype = c_int
+    lib.trlx_host_get_eval.argtypes = [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]
+    lib.trlx_host_get_eval.restype = c_int
+    lib.trlx_host_tridiag_eig_last.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p]
+    lib.trlx_host_tridiag_eig_last.restype = c_int
+    lib.trlx_host_arrow_to_tridiag.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                               c_void_p]
+    lib.trlx_host_arrow_to_tridiag.restype = c_int
+    lib.trlx_host_sym_eig.argtypes = [c_int, c_void_p, c_int, c_void_p]
+    lib.trlx_host_sym_eig.restype = c_int
+    lib.trlx_host_shuffle_eig.argtypes = [c_int, c_int, c_void_p, c_void_p, P(TrlInfo),
+                                          P(c_int), c_int]
+    lib.trlx_host_shuffle_eig.restype = None
+    lib.trlx_host_convergence_test.argtypes = [c_int, c_void_p, c_void_p, P(TrlInfo), c_void_p]
+    lib.trlx_host_convergence_test.restype = None
+    lib.trlx_host_sort_eig.argtypes = [c_int, c_int, c_int, c_double, c_void_p, c_void_p]
+    lib.trlx_host_sort_eig.restype = None
+    lib.trlx_host_set_locking.argtypes = [c_int, c_int, c_void_p, c_void_p, c_void_p, c_double,
+                                          P(c_int)]
+    lib.trlx_host_set_locking.restype = None
+    lib.trlx_host_sort2.argtypes = [c_int, c_void_p, c_void_p]
+    lib.trlx_host_sort2.restype = None
+    return lib
+
+
+_LIB = None
+
+
+def load():
+    """Return the loaded library (raises ImportError if it is not built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"libtrlan_b200.so not found at {LIB_PATH}; build it with "
+                "`make -C nutrlan_b200/csrc` (the CUDA path has no fallback)")
+        _LIB = _declare(C.CDLL(LIB_PATH))
+    return _LIB
+
+
+__all__ = ["load", "LIB_PATH", "TrlInfo", "TrlxStats", "TrlxOptions", "MATVEC",
+           "USER_ORTHO"]

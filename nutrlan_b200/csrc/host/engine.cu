@@ -1,0 +1,1125 @@
+// Thick-restart Lanczos driver with a device-resident basis.
+//
+// Control flow follows the reference's trlanczos (SRC/trlcore.c:723-1532)
+// and ztrlanczos (SRC/ztrlcore.c:436-1286): same restart decisions, same
+// convergence tests, same error codes.  What differs is where the data lives
+// and how the vector work is done:
+//   * the basis is a pool of padded device columns addressed by a device
+//     table of column pointers; restarts write Ritz vectors into free slots
+//     and re-point the table instead of copying columns;
+//   * the matrix-vector product is either the user's callback (device or
+//     host pointers) or a built-in sparse operator fused with the alpha dot;
+//   * trl_orth/trl_cgs run as project/update kernel pairs; the first pass of
+//     every step applies the three-term recurrence on the fly and is issued
+//     before the host has seen alpha (its norm doubles as trl_orth's
+//     pre-orthogonalisation norm), so a Lanczos step costs one host sync;
+//   * the small projected problem stays on the host in FP64.
+#include <algorithm>
+#include <cfloat>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <type_traits>
+#include <vector>
+
+#include "../kernels/lanczos_kernels.h"
+#include "../kernels/spmv.h"
+#include "dense.h"
+#include "engine.h"
+
+namespace trlb {
+
+bool is_device_pointer(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+trlx_stats &last_stats() {
+    static thread_local trlx_stats s;
+    return s;
+}
+
+Options options_from(const trlx_options *o) {
+    Options r;
+    if (!o) return r;
+    r.basis_bits = o->basis_bits == 32 ? 32 : 64;
+    r.seed = o->seed ? o->seed : r.seed;
+    r.stream = static_cast<cudaStream_t>(o->stream);
+    r.refine = o->refine;
+    r.profile = o->profile;
+    return r;
+}
+
+namespace {
+
+enum Scal { kAlpha = 0, kR2Pre = 1, kH2 = 2, kR2Post = 3, kNorm = 4, kNumScal = 8 };
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            std::fprintf(stderr, "TRLAN-B200: CUDA error %s at %s:%d\n",                  \
+                         cudaGetErrorString(e_), __FILE__, __LINE__);                     \
+            return -1001;                                                                 \
+        }                                                                                 \
+    } while (0)
+
+template <class T>
+struct OpTypes;
+template <>
+struct OpTypes<double> {
+    using Fn = trl_matvec;
+    using User = double;
+};
+template <>
+struct OpTypes<float> {
+    using Fn = trl_matvec;
+    using User = double;
+};
+template <>
+struct OpTypes<zd> {
+    using Fn = ztrl_matvec;
+    using User = trl_dcomplex;
+};
+template <>
+struct OpTypes<zf> {
+    using Fn = ztrl_matvec;
+    using User = trl_dcomplex;
+};
+
+template <class T>
+class Engine {
+   public:
+    using C = typename Store<T>::C;
+    static constexpr bool kComplex = std::is_same<C, zd>::value;
+    static constexpr bool kWide = std::is_same<T, C>::value;  // FP64 / c128 storage
+    using OpFn = typename OpTypes<T>::Fn;
+    using User = typename OpTypes<T>::User;
+
+    Engine(OpFn op, trl_uo uo, trl_info *info, int nrow, int mev, double *eval, User *evec, int lde,
+           const Options &opt)
+        : op_(op), uo_(uo), info_(info), nrow_(nrow), mev_(mev), eval_(eval), evec_(evec), lde_(lde),
+          opt_(opt) {}
+
+    ~Engine() { release(); }
+
+    int setup();
+    void run();
+    // Residual norms on exit (reference: wrk[0:j1] = |beta|, rest alpha).
+    void residual_output(double *out, int count) const {
+        for (int i = 0; i < count && i < maxlan_; ++i)
+            out[i] = i < final_j1_ ? std::fabs(beta_[i]) : alpha_[i];
+    }
+
+   private:
+    // ---- device helpers ----
+    T *col(int j) const { return pool_ + (size_t)lslot_[j] * n_pad_; }
+    C *col64(int j) const {
+        if constexpr (kWide)
+            return reinterpret_cast<C *>(col(j));
+        else
+            return nullptr;
+    }
+    int upload_table();
+    int apply_op(const C *x, C *y, bool want_alpha);
+    int sync_scalars();
+    int orth(int m, bool recur, double beta_prev, int kept);
+    int cgs(int m, bool pass_done, double *rnrm, bool *irnd_used);
+    int normalize_into(int m, double scale_fixed, bool use_r2);
+    void rotate_fp64();
+    int initial_guess(int *jnd);
+    int restart_ritz(int locked, int jml, int kept, int jnd);
+    int final_vectors(int jnd, int kept);
+    void log_progress();
+    void release();
+    void count_launch(int k = 1) { launches_ += k; }
+    // Per-kernel-class timing with CUDA events on st_ (options.profile).
+    int pbeg();
+    void pend(int id, int cls, double bytes);
+    void flush_prof();
+    double cs() const { return (double)sizeof(C); }
+    double sv() const { return (double)sizeof(T); }
+
+    OpFn op_;
+    trl_uo uo_;
+    trl_info *info_;
+    int nrow_, mev_;
+    double *eval_;
+    User *evec_;
+    int lde_;
+    Options opt_;
+
+    // modes
+    bool user_dev_ = false;
+    const trlx_operator *builtin_ = nullptr;
+    bool host_op_ = false;
+
+    // device state
+    long n_pad_ = 0;
+    int P_ = 0, maxlan_ = 0;
+    T *pool_ = nullptr;
+    std::vector<int> lslot_;
+    T **d_cols_ = nullptr;
+    std::vector<T *> h_cols_;
+    C *fbuf_[3] = {nullptr, nullptr, nullptr};  // FP64 q_cur, q_prev, r (narrow storage)
+    C *qa64_ = nullptr, *qb64_ = nullptr, *r64_ = nullptr;
+    C *d_coef_ = nullptr;
+    double *d_scal_ = nullptr, *h_scal_ = nullptr;
+    double *d_Y_ = nullptr;
+    Scratch scratch_;
+    cudaStream_t st_ = nullptr;
+    bool own_stream_ = false;
+    User *hx_ = nullptr, *hy_ = nullptr;  // pinned staging for host operators
+    cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+
+    // host state (reference names)
+    std::vector<double> alpha_, beta_, alfrot_, betrot_, rot_, lambda_, res_, yy_, wrk2_;
+    int final_j1_ = 0;
+    long long launches_ = 0;
+    int syncs_ = 0;
+    double t_op_ = 0, t_orth_ = 0, t_res_ = 0;
+    double fl_ = 0, fl_h_ = 0, fl_r_ = 0;  // flop counts (excluding matvec)
+    struct ProfRec {
+        cudaEvent_t a, b;
+        int cls;
+        double bytes;
+    };
+    std::vector<ProfRec> prof_;
+    std::vector<cudaEvent_t> evpool_;
+    size_t evnext_ = 0;
+    double kt_[8] = {0}, kb_[8] = {0};
+    long long kc_[8] = {0};
+};
+
+template <class T>
+int Engine<T>::pbeg() {
+    if (!opt_.profile) return -1;
+    if (evnext_ + 2 > evpool_.size()) {
+        for (int k = 0; k < 64; ++k) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            evpool_.push_back(e);
+        }
+    }
+    cudaEvent_t a = evpool_[evnext_++];
+    cudaEventRecord(a, st_);
+    prof_.push_back(ProfRec{a, nullptr, 0, 0.0});
+    return (int)prof_.size() - 1;
+}
+
+template <class T>
+void Engine<T>::pend(int id, int cls, double bytes) {
+    if (id < 0) return;
+    cudaEvent_t b = evpool_[evnext_++];
+    cudaEventRecord(b, st_);
+    prof_[id].b = b;
+    prof_[id].cls = cls;
+    prof_[id].bytes = bytes;
+}
+
+// All recorded events have completed when this runs (after a stream sync).
+template <class T>
+void Engine<T>::flush_prof() {
+    for (auto &r : prof_) {
+        if (!r.b) continue;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        kt_[r.cls] += ms * 1e-3;
+        kb_[r.cls] += r.bytes;
+        kc_[r.cls] += 1;
+    }
+    prof_.clear();
+    evnext_ = 0;
+}
+
+// ---------------------------------------------------------------------------
+template <class T>
+int Engine<T>::setup() {
+    maxlan_ = info_->maxlan;
+    n_pad_ = ((long)nrow_ + 255) / 256 * 256;
+    P_ = 2 * maxlan_ + 2;
+    user_dev_ = is_device_pointer(evec_);
+    if constexpr (kComplex) {
+        if ((void *)op_ == (void *)&trlx_zmatvec && info_->mvparam) builtin_ = static_cast<trlx_operator *>(info_->mvparam);
+    } else {
+        if ((void *)op_ == (void *)&trlx_matvec && info_->mvparam) builtin_ = static_cast<trlx_operator *>(info_->mvparam);
+    }
+    if (builtin_) {
+        if (builtin_->nrow != nrow_ || (builtin_->kind == 2) != kComplex) {
+            std::fprintf(stderr, "TRLAN-B200: built-in operator does not match the problem.\n");
+            return -6;
+        }
+    }
+    host_op_ = !builtin_ && !user_dev_;
+
+    if (opt_.stream) {
+        st_ = opt_.stream;
+    } else {
+        CK(cudaStreamCreate(&st_));  // blocking: ordered with legacy-stream user work
+        own_stream_ = true;
+    }
+    size_t pool_bytes = (size_t)P_ * n_pad_ * sizeof(T);
+    if (cudaMalloc(&pool_, pool_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        std::fprintf(stderr, "TRLAN-B200: cannot allocate %.2f GB basis pool.\n", pool_bytes / 1e9);
+        return -5;
+    }
+    CK(cudaMemsetAsync(pool_, 0, pool_bytes, st_));
+    lslot_.resize(P_);
+    for (int i = 0; i < P_; ++i) lslot_[i] = i;
+    CK(cudaMalloc(&d_cols_, sizeof(T *) * P_));
+    h_cols_.resize(P_);
+    if (!kWide) {
+        for (auto &b : fbuf_) {
+            CK(cudaMalloc(&b, sizeof(C) * n_pad_));
+            CK(cudaMemsetAsync(b, 0, sizeof(C) * n_pad_, st_));
+        }
+    }
+    if (!kWide) {
+        qa64_ = fbuf_[0];
+        qb64_ = fbuf_[1];
+        r64_ = fbuf_[2];
+    }
+    CK(cudaMalloc(&d_coef_, sizeof(C) * P_));
+    CK(cudaMalloc(&d_scal_, sizeof(double) * kNumScal));
+    CK(cudaMemsetAsync(d_scal_, 0, sizeof(double) * kNumScal, st_));
+    CK(cudaMallocHost(&h_scal_, sizeof(double) * kNumScal));
+    CK(cudaMalloc(&d_Y_, sizeof(double) * (size_t)maxlan_ * maxlan_));
+    scratch_.max_blocks = 148 * 8;
+    scratch_.max_cols = P_;
+    CK(cudaMalloc(&scratch_.partials, (size_t)scratch_.max_blocks * (P_ + 2) * sizeof(zd)));
+    CK(cudaMalloc(&scratch_.tickets, sizeof(unsigned) * kNumTickets));
+    CK(cudaMemsetAsync(scratch_.tickets, 0, sizeof(unsigned) * kNumTickets, st_));
+    if (host_op_) {
+        CK(cudaMallocHost(&hx_, sizeof(User) * (size_t)nrow_));
+        CK(cudaMallocHost(&hy_, sizeof(User) * (size_t)nrow_));
+    }
+    for (auto &e : ev_) CK(cudaEventCreate(&e));
+    size_t mm = (size_t)maxlan_ + 1;
+    alpha_.assign(mm, 0.0);
+    beta_.assign(mm, 0.0);
+    alfrot_.assign(mm, 0.0);
+    betrot_.assign(mm, 0.0);
+    rot_.assign(mm * mm, 0.0);
+    lambda_.assign(mm, 0.0);
+    res_.assign(mm, 0.0);
+    yy_.assign(mm * mm, 0.0);
+    wrk2_.assign(4 * mm, 0.0);
+    return upload_table();
+}
+
+template <class T>
+void Engine<T>::release() {
+    cudaStreamSynchronize(st_);
+    cudaFree(pool_);
+    cudaFree(d_cols_);
+    for (auto b : fbuf_) cudaFree(b);
+    cudaFree(d_coef_);
+    cudaFree(d_scal_);
+    cudaFreeHost(h_scal_);
+    cudaFree(d_Y_);
+    cudaFree(scratch_.partials);
+    cudaFree(scratch_.tickets);
+    cudaFreeHost(hx_);
+    cudaFreeHost(hy_);
+    for (auto e : ev_)
+        if (e) cudaEventDestroy(e);
+    for (auto e : evpool_) cudaEventDestroy(e);
+    if (own_stream_) cudaStreamDestroy(st_);
+    pool_ = nullptr;
+}
+
+template <class T>
+int Engine<T>::upload_table() {
+    for (int j = 0; j < P_; ++j) h_cols_[j] = col(j);
+    CK(cudaMemcpyAsync(d_cols_, h_cols_.data(), sizeof(T *) * P_, cudaMemcpyHostToDevice, st_));
+    // The host vector must stay unchanged until the copy ran.
+    CK(cudaStreamSynchronize(st_));
+    return 0;
+}
+
+template <class T>
+int Engine<T>::sync_scalars() {
+    CK(cudaMemcpyAsync(h_scal_, d_scal_, sizeof(double) * kNumScal, cudaMemcpyDeviceToHost, st_));
+    CK(cudaStreamSynchronize(st_));
+    ++syncs_;
+    if (!prof_.empty()) flush_prof();
+    return 0;
+}
+
+// y = A x (+ alpha into d_scal_[kAlpha]).
+template <class T>
+int Engine<T>::apply_op(const C *x, C *y, bool want_alpha) {
+    double *aout = want_alpha ? d_scal_ + kAlpha : nullptr;
+    if (builtin_) {
+        int pid = pbeg();
+        if constexpr (kComplex)
+            spmv_fused_cplx(builtin_, x, y, n_pad_, aout, &scratch_, st_);
+        else
+            spmv_fused_real(builtin_, x, y, n_pad_, aout, &scratch_, st_);
+        pend(pid, TRLX_K_SPMV, spmv_bytes(builtin_));
+        count_launch();
+    } else if (!host_op_) {
+        // The user's operator sees device pointers; our stream is a blocking
+        // stream, so work it issues on the legacy default stream is ordered.
+        CK(cudaStreamSynchronize(st_));
+        op_(nrow_, 1, reinterpret_cast<const User *>(x), (int)n_pad_, reinterpret_cast<User *>(y), (int)n_pad_,
+            info_->mvparam);
+        // The operator may have used any stream: wait for all of its work.
+        CK(cudaDeviceSynchronize());
+        if (want_alpha) {
+            int pid = pbeg();
+            launch_dot<C>(x, y, n_pad_, aout, scratch_, st_);
+            pend(pid, TRLX_K_DOT, 2.0 * nrow_ * cs());
+            count_launch();
+        }
+    } else {
+        CK(cudaMemcpyAsync(hx_, x, sizeof(User) * nrow_, cudaMemcpyDeviceToHost, st_));
+        CK(cudaStreamSynchronize(st_));
+        op_(nrow_, 1, hx_, nrow_, hy_, nrow_, info_->mvparam);
+        CK(cudaMemcpyAsync(y, hy_, sizeof(User) * nrow_, cudaMemcpyHostToDevice, st_));
+        if (want_alpha) {
+            int pid = pbeg();
+            launch_dot<C>(x, y, n_pad_, aout, scratch_, st_);
+            pend(pid, TRLX_K_DOT, 2.0 * nrow_ * cs());
+            count_launch();
+        }
+    }
+    info_->matvec++;
+    return 0;
+}
+
+// Normalise r into basis column m (and the FP64 copy).
+template <class T>
+int Engine<T>::normalize_into(int m, double scale_fixed, bool use_r2) {
+    const double *r2 = use_r2 ? d_scal_ + kNorm : nullptr;
+    int pid = pbeg();
+    if constexpr (kWide) {
+        launch_normalize<T>(r64_, n_pad_, r2, scale_fixed, r64_, nullptr, st_);
+    } else {
+        launch_normalize<T>(r64_, n_pad_, r2, scale_fixed, r64_, col(m), st_);
+    }
+    pend(pid, TRLX_K_NORMALIZE, 2.0 * nrow_ * cs() + (kWide ? 0.0 : nrow_ * sv()));
+    count_launch();
+    return 0;
+}
+
+// After column m got its vector: FP64 copies move one step.
+template <class T>
+void Engine<T>::rotate_fp64() {
+    if constexpr (!kWide) {
+        C *new_cur = r64_;
+        C *old_prev = qb64_;
+        qb64_ = qa64_;
+        qa64_ = new_cur;
+        r64_ = old_prev;
+    }
+}
+
+// Gram-Schmidt against columns 0..m-1 (reference trl_cgs,
+// SRC/trlcore.c:2913-3117).  When pass_done, the first project/update pass
+// has already been issued and its scalars are in h_scal_.
+template <class T>
+int Engine<T>::cgs(int m, bool pass_done, double *rnrm, bool *irnd_used) {
+    const int maxorth = 3;
+    int irnd = 0;
+    double normrr2 = 0.0, normdiff2 = 0.0;
+    if (m > 0) {
+        int cnt = 0;
+        bool first = true;
+        while (cnt <= maxorth) {
+            if (!(first && pass_done)) {
+                Recur<C> none;
+                int p1 = pbeg();
+                launch_project<T>(d_cols_, m, n_pad_, r64_, none, d_coef_, d_scal_ + kR2Pre, scratch_, st_);
+                pend(p1, TRLX_K_PROJECT, (double)m * nrow_ * sv() + nrow_ * cs());
+                int p2 = pbeg();
+                launch_update<T>(d_cols_, m, n_pad_, r64_, none, d_coef_, r64_, d_scal_ + kR2Post, scratch_, st_);
+                pend(p2, TRLX_K_UPDATE, (double)m * nrow_ * sv() + 2.0 * nrow_ * cs());
+                count_launch(2);
+                if (int e = sync_scalars()) return e;
+            }
+            first = false;
+            double ud = 0.0;
+            if (uo_) {
+                if constexpr (!kComplex) {
+                    if (host_op_) {
+                        CK(cudaMemcpy(hx_, r64_, sizeof(double) * nrow_, cudaMemcpyDeviceToHost));
+                        uo_(nrow_, hx_, &ud);
+                        CK(cudaMemcpy(r64_, hx_, sizeof(double) * nrow_, cudaMemcpyHostToDevice));
+                    } else {
+                        uo_(nrow_, reinterpret_cast<double *>(r64_), &ud);
+                    }
+                    launch_dot<C>(r64_, r64_, n_pad_, d_scal_ + kR2Post, scratch_, st_);
+                    count_launch();
+                    if (int e = sync_scalars()) return e;
+                }
+            }
+            info_->north++;
+            cnt++;
+            normdiff2 = h_scal_[kH2];
+            normrr2 = h_scal_[kR2Post];
+            if (uo_) normdiff2 += ud * ud;
+            *rnrm = std::sqrt(normrr2);
+            if (DBL_EPSILON * normrr2 > normdiff2) break;
+            if ((cnt > 1 && (m * DBL_EPSILON * DBL_EPSILON * (normrr2 + normdiff2) < normdiff2)) ||
+                !(normrr2 > DBL_MIN)) {
+                // Linearly dependent on the basis: try one fresh random vector.
+                if (irnd > 0) break;
+                cnt = 0;
+                irnd++;
+                info_->nrand++;
+                launch_random<C>(r64_, nrow_, n_pad_, opt_.seed + 7919ull * (uint64_t)info_->nrand, st_);
+                count_launch();
+            }
+        }
+        if (normrr2 < normdiff2 && !uo_) return -203;
+    }
+    if (*rnrm > DBL_MIN) {
+        normalize_into(m, 1.0 / *rnrm, false);
+    } else {
+        return -204;
+    }
+    if (irnd > 0) *rnrm = 0.0;
+    if (irnd_used) *irnd_used = irnd > 0;
+    return 0;
+}
+
+// trl_orth (SRC/trlcore.c:1766-1975): r (in r64_) against columns 0..m-1,
+// result normalised into column m; sets alpha_[m-1] (from the device) and
+// beta_[m-1].
+template <class T>
+int Engine<T>::orth(int m, bool recur, double beta_prev, int kept) {
+    const int jnd = m, jm1 = jnd - 1;
+    // Optimistic first Gram-Schmidt pass (the full pass is taken in almost
+    // every step); the recurrence r = y - alpha qa - beta qb is applied on
+    // the fly with alpha read from device memory.
+    Recur<C> rec;
+    if (recur) {
+        rec.x = qa64_;
+        rec.xp = qb64_;
+        rec.alpha = d_scal_ + kAlpha;
+        rec.beta = beta_prev;
+        rec.on = 1;
+    }
+    const double recb = recur ? 2.0 * nrow_ * cs() : 0.0;
+    int p1 = pbeg();
+    launch_project<T>(d_cols_, m, n_pad_, r64_, rec, d_coef_, d_scal_ + kR2Pre, scratch_, st_);
+    pend(p1, TRLX_K_PROJECT, (double)m * nrow_ * sv() + nrow_ * cs() + recb);
+    int p2 = pbeg();
+    launch_update<T>(d_cols_, m, n_pad_, r64_, rec, d_coef_, r64_, d_scal_ + kR2Post, scratch_, st_);
+    pend(p2, TRLX_K_UPDATE, (double)m * nrow_ * sv() + 2.0 * nrow_ * cs() + recb);
+    count_launch(2);
+    if (int e = sync_scalars()) return e;
+    alpha_[jnd - 1] = h_scal_[kAlpha];
+    const double normrr2 = h_scal_[kR2Pre];
+    if (!(normrr2 >= 0.0) || !(normrr2 <= DBL_MAX)) return -102;
+    beta_[jnd - 1] = std::sqrt(normrr2);
+    double tmp = alpha_[jnd - 1] * alpha_[jnd - 1];
+    if (jm1 > kept) {
+        tmp += beta_[jm1 - 1] * beta_[jm1 - 1];
+        fl_ += 2 * nrow_ + 4;
+    } else if (kept > 0) {
+        for (int i = 0; i < jm1; ++i) tmp += beta_[i] * beta_[i];
+        fl_ += 2 * (nrow_ + kept + 2);
+    }
+    bool usecgs;
+    if (jm1 == kept) {
+        usecgs = true;
+    } else if (jnd >= info_->ntot) {
+        usecgs = false;
+    } else if (DBL_EPSILON * normrr2 >= tmp) {
+        double anorm = 0.0;
+        for (int i = 0; i < jnd; ++i) anorm = std::max(anorm, std::fabs(alpha_[i]) + std::fabs(beta_[i]));
+        usecgs = beta_[jm1] < DBL_EPSILON * anorm * info_->ntot;
+    } else {
+        usecgs = true;
+    }
+    if (usecgs) {
+        const int nr = info_->nrand, no = info_->north;
+        double rnrm = beta_[jnd - 1];
+        int st = cgs(m, true, &rnrm, nullptr);
+        fl_ += 4 * nrow_ * ((info_->north - no) * jnd + info_->nrand - nr) + nrow_;
+        if (st) return st;
+        beta_[jnd - 1] = rnrm;
+    } else {
+        // Local re-orthogonalisation against the last one or two vectors:
+        // restore the components the optimistic pass removed from the older
+        // columns, then apply the reference's local update and scaling.
+        std::vector<C> h(m);
+        CK(cudaMemcpy(h.data(), d_coef_, sizeof(C) * m, cudaMemcpyDeviceToHost));
+        std::vector<C> g(m);
+        const int nloc = std::min(2, m);
+        for (int c = 0; c < m; ++c) {
+            if (c < m - nloc) {
+                if constexpr (kComplex)
+                    g[c] = zd{-h[c].x, -h[c].y};
+                else
+                    g[c] = -h[c];
+            } else {
+                if constexpr (kComplex)
+                    g[c] = zd{0.0, 0.0};
+                else
+                    g[c] = 0.0;
+            }
+        }
+        if (m > nloc) {
+            CK(cudaMemcpyAsync(d_coef_, g.data(), sizeof(C) * m, cudaMemcpyHostToDevice, st_));
+            Recur<C> none;
+            launch_update<T>(d_cols_, m, n_pad_, r64_, none, d_coef_, r64_, d_scal_ + kR2Post, scratch_, st_);
+            count_launch();
+        }
+        double dlast;
+        if constexpr (kComplex)
+            dlast = h[m - 1].x;
+        else
+            dlast = h[m - 1];
+        alpha_[jnd - 1] += dlast;
+        normalize_into(m, 1.0 / beta_[jnd - 1], false);
+        fl_ += (jnd > 1 ? 9 : 5) * nrow_;
+    }
+    if (beta_[jnd - 1] <= DBL_EPSILON * std::fabs(alpha_[jnd - 1]))
+        beta_[jnd - 1] = 0.0;
+    else if (jnd >= info_->ntot)
+        beta_[jnd - 1] = 0.0;
+    return 0;
+}
+
+// trl_initial_guess (SRC/trlcore.c:1577-1763), without checkpoint reading
+// beyond what the caller staged: the start vector is column nec of evec
+// (guess == 1), the ones vector (guess == 0), or ones with -guess random
+// perturbations (guess < 0).
+template <class T>
+int Engine<T>::initial_guess(int *jnd_out) {
+    const int nec = info_->nec;
+    const size_t ue = sizeof(User);
+    // Locked vectors 0..nec-1 from the user's evec.
+    for (int j = 0; j < nec; ++j) {
+        C *dst = kWide ? reinterpret_cast<C *>(col(j)) : r64_;
+        CK(cudaMemcpyAsync(dst, evec_ + (size_t)j * lde_, ue * nrow_,
+                           user_dev_ ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st_));
+        if (!kWide) {
+            launch_store<T>(r64_, n_pad_, col(j), st_);
+            count_launch();
+        }
+    }
+    // Start vector into r64_.
+    if constexpr (kWide) r64_ = reinterpret_cast<C *>(col(nec));
+    if (info_->guess == 1) {
+        CK(cudaMemcpyAsync(r64_, evec_ + (size_t)nec * lde_, ue * nrow_,
+                           user_dev_ ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st_));
+    } else {
+        std::vector<User> ones(nrow_);
+        for (auto &v : ones) {
+            if constexpr (kComplex)
+                v = trl_dcomplex{1.0, 0.0};
+            else
+                v = 1.0;
+        }
+        const int nran = 2 * (std::max(0, 1 - info_->guess) / 2);
+        if (nran > 0 && nran < nrow_) {
+            for (int k = 0; k + 1 < nran; k += 2) {
+                long idx = (long)(nrow_ * uniform01(opt_.seed, (uint64_t)k));
+                double pert = uniform01(opt_.seed, (uint64_t)k + 1) - 0.5;
+                if constexpr (kComplex)
+                    ones[idx].r += pert;
+                else
+                    ones[idx] += pert;
+            }
+            fl_ += nran + nran;
+        }
+        CK(cudaMemcpyAsync(r64_, ones.data(), ue * nrow_, cudaMemcpyHostToDevice, st_));
+        CK(cudaStreamSynchronize(st_));
+        if (nran >= nrow_) {
+            launch_random<C>(r64_, nrow_, n_pad_, opt_.seed, st_);
+            count_launch();
+            info_->nrand++;
+        }
+    }
+    launch_dot<C>(r64_, r64_, n_pad_, d_scal_ + kR2Post, scratch_, st_);
+    count_launch();
+    if (int e = sync_scalars()) return e;
+    double normr2 = h_scal_[kR2Post];
+    double rnrm = 0.0;
+    if (normr2 >= DBL_MIN && normr2 <= DBL_MAX) {
+        rnrm = std::sqrt(normr2);
+    } else {
+        launch_random<C>(r64_, nrow_, n_pad_, opt_.seed ^ 0xA5A5A5A5ull, st_);
+        count_launch();
+        info_->nrand++;
+        launch_dot<C>(r64_, r64_, n_pad_, d_scal_ + kR2Post, scratch_, st_);
+        count_launch();
+        if (int e = sync_scalars()) return e;
+        rnrm = std::sqrt(h_scal_[kR2Post]);
+    }
+    const int nr = info_->nrand, no = info_->north;
+    int stt = cgs(nec, false, &rnrm, nullptr);
+    fl_ += 4 * nrow_ * ((info_->north - no) * nec + info_->nrand - nr) + nrow_;
+    if (stt) return stt;
+    if constexpr (!kWide) {
+        // FP64 copy of the start vector becomes q_cur.
+        rotate_fp64();
+    }
+    *jnd_out = nec;
+    return 0;
+}
+
+// Restart: Ritz vectors of columns locked..jnd-1 with coefficients yy_
+// (jml x kept) into free slots, then re-point the table.
+template <class T>
+int Engine<T>::restart_ritz(int locked, int jml, int kept, int jnd) {
+    CK(cudaMemcpyAsync(d_Y_, yy_.data(), sizeof(double) * (size_t)jml * kept, cudaMemcpyHostToDevice, st_));
+    // Output slots: logical jnd+1 .. jnd+kept are free.
+    int pid = pbeg();
+    launch_ritz<T>(d_cols_ + locked, jml, n_pad_, d_Y_, jml, kept, d_cols_ + jnd + 1, st_);
+    pend(pid, TRLX_K_RITZ, (double)nrow_ * (jml + kept) * sv());
+    count_launch();
+    std::vector<int> nl;
+    nl.reserve(P_);
+    for (int j = 0; j < locked; ++j) nl.push_back(lslot_[j]);
+    for (int k = 0; k < kept; ++k) nl.push_back(lslot_[jnd + 1 + k]);
+    nl.push_back(lslot_[jnd]);  // residual vector follows the kept ones
+    for (int j = locked; j < jnd; ++j) nl.push_back(lslot_[j]);
+    for (int j = jnd + 1 + kept; j < P_; ++j) nl.push_back(lslot_[j]);
+    lslot_ = nl;
+    return upload_table();
+}
+
+// Final Ritz vectors (columns 0..jnd-1, yy_ jnd x kept) straight into the
+// user's evec (FP64), plus the last Lanczos vector in column kept.
+template <class T>
+int Engine<T>::final_vectors(int jnd, int kept) {
+    CK(cudaMemcpyAsync(d_Y_, yy_.data(), sizeof(double) * (size_t)jnd * kept, cudaMemcpyHostToDevice, st_));
+    C *out = nullptr;
+    long ldo = lde_;
+    C *tmp = nullptr;
+    if (user_dev_) {
+        out = reinterpret_cast<C *>(evec_);
+    } else {
+        CK(cudaMalloc(&tmp, sizeof(C) * (size_t)n_pad_ * std::max(kept, 1)));
+        out = tmp;
+        ldo = n_pad_;
+    }
+    int pid = pbeg();
+    launch_ritz_out<T>(d_cols_, jnd, n_pad_, d_Y_, jnd, kept, out, ldo, nrow_, st_);
+    pend(pid, TRLX_K_RITZ, (double)nrow_ * jnd * sv() + (double)nrow_ * kept * cs());
+    count_launch();
+    const size_t ue = sizeof(User);
+    if (!user_dev_ && kept > 0) {
+        CK(cudaMemcpy2DAsync(evec_, ue * lde_, tmp, ue * n_pad_, ue * nrow_, kept, cudaMemcpyDeviceToHost, st_));
+    }
+    // Last Lanczos vector (FP64) into column kept.
+    if (kept < mev_) {
+        const C *last = kWide ? reinterpret_cast<const C *>(col(jnd)) : qa64_;
+        CK(cudaMemcpyAsync(evec_ + (size_t)kept * lde_, last, ue * nrow_,
+                           user_dev_ ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st_));
+    }
+    CK(cudaStreamSynchronize(st_));
+    cudaFree(tmp);
+    return 0;
+}
+
+template <class T>
+void Engine<T>::log_progress() {
+    if (info_->verbose <= 0) return;
+    FILE *fp = info_->log_fp ? info_->log_fp : stdout;
+    std::fprintf(fp, "MATVEC: %10d,    Nloop: %10d,     Nec: %10d\n", info_->matvec, info_->nloop, info_->nec);
+    std::fprintf(fp, "Reorth: %10d,    Nrand: %10d,    Ierr: %10d\n", info_->north, info_->nrand, info_->stat);
+    std::fprintf(fp, "Target: %10.3e,   ResNrm: %10.3e,  CFact: %10.3e\n", info_->trgt, info_->tres, info_->crat);
+}
+
+template <class T>
+void Engine<T>::run() {
+    trl_info *info = info_;
+    const double t_start = now_s();
+    int locked = info->nec;
+    if (locked > 0) {
+        for (int i = 0; i < locked; ++i) {
+            alpha_[i] = eval_[i];
+            beta_[i] = 0.0;
+        }
+    }
+    int jnd = 0;
+    int stat = initial_guess(&jnd);
+    int kept = jnd;
+    info->stat = stat;
+    if (stat != 0) {
+        final_j1_ = 0;
+        return;
+    }
+    int i1 = info->ned - jnd;
+    int next_test = i1 + std::min(i1, std::min(6, info->ned / 2));
+    int chkpnt = info->cpflag <= 0 ? info->maxmv + info->maxlan : info->maxmv / info->cpflag;
+    (void)chkpnt;
+    int prek = kept;
+    int j1 = kept;  // columns that map to the caller's evec on exit
+
+    while (info->matvec < info->maxmv && info->nec < info->ned) {
+        // ---- first step after (re)start: arrowhead coupling -------------------
+        jnd++;
+        if (jnd + 1 > maxlan_ + 1 || jnd + 1 >= P_) {
+            stat = -1111;
+            break;
+        }
+        // FP64 views of the current vector and the output slot.
+        if constexpr (kWide) {
+            qa64_ = reinterpret_cast<C *>(col(jnd - 1));
+            qb64_ = jnd >= 2 ? reinterpret_cast<C *>(col(jnd - 2)) : nullptr;
+            r64_ = reinterpret_cast<C *>(col(jnd));
+        }
+        cudaEventRecord(ev_[0], st_);
+        if ((stat = apply_op(qa64_, r64_, true))) break;
+        cudaEventRecord(ev_[1], st_);
+        // Coefficients (beta_0 .. beta_{jnd-2}, alpha_{jnd-1}); the device
+        // writes alpha into the last slot before the coupling update.
+        {
+            std::vector<C> g(jnd);
+            for (int i = 0; i < jnd - 1; ++i) {
+                if constexpr (kComplex)
+                    g[i] = zd{beta_[i], 0.0};
+                else
+                    g[i] = beta_[i];
+            }
+            if constexpr (kComplex)
+                g[jnd - 1] = zd{0.0, 0.0};
+            else
+                g[jnd - 1] = 0.0;
+            if (cudaMemcpyAsync(d_coef_, g.data(), sizeof(C) * jnd, cudaMemcpyHostToDevice, st_) != cudaSuccess) {
+                stat = -1001;
+                break;
+            }
+            cudaMemcpyAsync(reinterpret_cast<double *>(d_coef_ + (jnd - 1)), d_scal_ + kAlpha, sizeof(double),
+                            cudaMemcpyDeviceToDevice, st_);
+            Recur<C> none;
+            int pid = pbeg();
+            launch_update<T>(d_cols_, jnd, n_pad_, r64_, none, d_coef_, r64_, d_scal_ + kR2Post, scratch_, st_);
+            pend(pid, TRLX_K_UPDATE, (double)jnd * nrow_ * sv() + 2.0 * nrow_ * cs());
+            count_launch();
+            cudaStreamSynchronize(st_);  // g must outlive the copy
+        }
+        fl_ += 2 * jnd * nrow_ + nrow_ + nrow_;
+        double f0 = fl_;
+        stat = orth(jnd, false, 0.0, kept);
+        fl_h_ += fl_ - f0;
+        cudaEventRecord(ev_[2], st_);
+        if (stat) break;
+        {
+            cudaEventSynchronize(ev_[2]);
+            float a = 0, b = 0;
+            cudaEventElapsedTime(&a, ev_[0], ev_[1]);
+            cudaEventElapsedTime(&b, ev_[1], ev_[2]);
+            t_op_ += a * 1e-3;
+            t_orth_ += b * 1e-3;
+        }
+        rotate_fp64();
+        // Arrow -> tridiagonal for the non-locked part.
+        for (int i = 0; i < locked; ++i) {
+            alfrot_[i] = alpha_[i];
+            betrot_[i] = 0.0;
+        }
+        i1 = jnd - locked;
+        arrow_to_tridiag(i1, &alpha_[locked], &beta_[locked], rot_.data(), &alfrot_[locked], &betrot_[locked]);
+        fl_ += 8 * i1 * i1 * i1 / 3;
+        betrot_[jnd - 1] = beta_[jnd - 1];
+
+        // ---- regular Lanczos steps ---------------------------------------------
+        while (jnd < info->klan && info->nec < info->ned) {
+            jnd++;
+            if (jnd + 1 >= P_) {
+                stat = -1111;
+                break;
+            }
+            if constexpr (kWide) {
+                qa64_ = reinterpret_cast<C *>(col(jnd - 1));
+                qb64_ = reinterpret_cast<C *>(col(jnd - 2));
+                r64_ = reinterpret_cast<C *>(col(jnd));
+            }
+            cudaEventRecord(ev_[0], st_);
+            if ((stat = apply_op(qa64_, r64_, true))) break;
+            cudaEventRecord(ev_[1], st_);
+            fl_ += 6 * nrow_;
+            double f1 = fl_;
+            stat = orth(jnd, true, beta_[jnd - 2], kept);
+            fl_h_ += fl_ - f1;
+            cudaEventRecord(ev_[2], st_);
+            alfrot_[jnd - 1] = alpha_[jnd - 1];
+            betrot_[jnd - 1] = beta_[jnd - 1];
+            if (stat) break;
+            {
+                cudaEventSynchronize(ev_[2]);
+                float a = 0, b = 0;
+                cudaEventElapsedTime(&a, ev_[0], ev_[1]);
+                cudaEventElapsedTime(&b, ev_[1], ev_[2]);
+                t_op_ += a * 1e-3;
+                t_orth_ += b * 1e-3;
+            }
+            rotate_fp64();
+            if (info->matvec >= next_test) {
+                if ((stat = get_eval(jnd, locked, alfrot_.data(), betrot_.data(), lambda_.data(), res_.data())))
+                    break;
+                const int ne = std::min(mev_, jnd);
+                std::memcpy(eval_, lambda_.data(), sizeof(double) * ne);
+                convergence_test(jnd, lambda_.data(), res_.data(), info, wrk2_.data());
+                if (info->nec < info->ned && info->nec > 0) {
+                    next_test = (int)((double)(info->ned * info->matvec) / (double)info->nec);
+                } else if (info->nec == 0) {
+                    next_test = next_test + next_test;
+                    if (info->maxlan == info->ntot) next_test = (int)std::ceil(0.5 * (info->maxlan + info->matvec));
+                }
+                log_progress();
+            }
+        }
+        if (stat) break;
+
+        // ---- restart or finish -------------------------------------------------
+        const double t_r0 = now_s();
+        const double fr0 = fl_;
+        prek = kept;
+        const int jml = jnd - locked;
+        int i2 = kept - locked + 1;
+        if (info->nec < info->ned) {
+            if ((stat = get_eval(jnd, locked, alfrot_.data(), betrot_.data(), lambda_.data(), res_.data()))) break;
+            convergence_test(jnd, lambda_.data(), res_.data(), info, wrk2_.data());
+            log_progress();
+        }
+        if (info->nec < info->ned && info->matvec < info->maxmv) {
+            shuffle_eig(jml, info->klan - locked, &lambda_[locked], &res_[locked], info, &kept, locked);
+            int tstat = 0;
+            if (kept * 3 < jml) {
+                tstat = get_tvec(jml, &alfrot_[locked], &betrot_[locked], 0, i2, rot_.data(), kept, &lambda_[locked],
+                                 yy_.data());
+                if (tstat == 0 && locked + kept > 0) std::memcpy(alpha_.data(), lambda_.data(), sizeof(double) * (locked + kept));
+            }
+            if (kept * 3 >= jml || tstat != 0) {
+                if (locked + kept > 0) std::memcpy(alfrot_.data(), lambda_.data(), sizeof(double) * (locked + kept));
+                tstat = get_tvec_a(jml, prek - locked, &alpha_[locked], &beta_[locked], kept, &alfrot_[locked],
+                                   yy_.data());
+            }
+            if (tstat) {
+                stat = tstat;
+                break;
+            }
+            for (int i = 0; i < kept; ++i) beta_[locked + i] = yy_[(size_t)(i + 1) * jml - 1] * betrot_[jnd - 1];
+            if (jml > info->ned + (info->ned / 5 + 6))
+                set_locking(jml, kept, &alpha_[locked], &beta_[locked], yy_.data(), info->anrm, &i2);
+            else
+                i2 = 0;
+            if ((stat = restart_ritz(locked, jml, kept, jnd))) break;
+            fl_ += 2 * nrow_ * jml * kept;
+            kept += locked;
+            locked += i2;
+            info->locked = locked;
+            jnd = kept;
+            if (jnd > mev_ && jnd - mev_ >= std::max(1, info->maxlan - mev_ + 1) - 1) {
+                stat = -1111;
+                break;
+            }
+            if (info->nec > 0)
+                next_test = (int)(((double)(info->matvec * info->ned)) / ((double)info->nec));
+            else
+                next_test = next_test + info->maxlan;
+            const int ne = std::min(mev_, jnd);
+            if (ne > 0) std::memcpy(eval_, lambda_.data(), sizeof(double) * ne);
+            j1 = std::min(jnd, mev_);
+        } else {
+            kept = std::min(info->nec, std::max(info->ned, mev_ - 1));
+            info->nec = kept;
+            if (kept == 0) kept = std::min(mev_ - 1, info->ned);
+            sort_eig(jnd, info->lohi, kept, info->ref, lambda_.data(), res_.data());
+            std::memcpy(eval_, lambda_.data(), sizeof(double) * kept);
+            int tstat = 0;
+            if (kept * 3 < jnd)
+                tstat = get_tvec(jnd, alfrot_.data(), betrot_.data(), locked, i2, rot_.data(), kept, eval_, yy_.data());
+            if (kept * 3 >= jnd || tstat != 0) {
+                tstat = get_tvec_a(jnd, prek, alpha_.data(), beta_.data(), kept, eval_, yy_.data());
+                if (tstat) {
+                    stat = tstat;
+                    break;
+                }
+            }
+            if (kept > 0) std::memcpy(alpha_.data(), eval_, sizeof(double) * kept);
+            for (int i = 0; i < kept; ++i) beta_[i] = betrot_[jnd - 1] * yy_[(size_t)(1 + i) * jnd - 1];
+            if ((stat = final_vectors(jnd, kept))) break;
+            fl_ += 2 * nrow_ * jml * kept;
+            jnd = kept;
+            j1 = kept;
+        }
+        t_res_ += now_s() - t_r0;
+        fl_r_ += fl_ - fr0;
+        info->nloop++;
+    }
+    final_j1_ = j1;
+    info->stat = stat;
+    // Flop counts go to the floating-point counters (the int ones would
+    // overflow at these sizes); timers are seconds in the tick_* fields.
+    info->rflp += fl_;
+    info->rflp_h += fl_h_;
+    info->rflp_r += fl_r_;
+    info->tick_o += t_op_;
+    info->tick_h += t_orth_;
+    info->tick_r += t_res_;
+    auto &s = last_stats();
+    s.seconds_total = now_s() - t_start;
+    s.seconds_op = t_op_;
+    s.seconds_orth = t_orth_;
+    s.seconds_restart = t_res_;
+    s.kernel_launches = launches_;
+    s.cgs_passes = info->north;
+    s.host_syncs = syncs_;
+    s.max_true_residual = -1.0;
+    s.op_bytes = builtin_ ? spmv_bytes(builtin_) * info->matvec : 0.0;
+    cudaStreamSynchronize(st_);
+    flush_prof();
+    for (int k = 0; k < 8; ++k) {
+        s.kernel_seconds[k] = kt_[k];
+        s.kernel_bytes[k] = kb_[k];
+        s.kernel_count[k] = kc_[k];
+    }
+    s.basis_bytes = kb_[TRLX_K_PROJECT] + kb_[TRLX_K_UPDATE] + kb_[TRLX_K_RITZ];
+}
+
+template <class T>
+void solve(typename Engine<T>::OpFn op, trl_uo uo, trl_info *info, int nrow, int mev, double *eval,
+           typename Engine<T>::User *evec, int lde, double *res_out, int res_len, const Options &opt) {
+    Engine<T> eng(op, uo, info, nrow, mev, eval, evec, lde, opt);
+    int st = eng.setup();
+    if (st) {
+        info->stat = st;
+        return;
+    }
+    eng.run();
+    if (res_out) eng.residual_output(res_out, res_len);
+}
+
+}  // namespace
+
+void clear_counter(trl_info *info, int nrow, int mev, int lde) {
+    info->stat = 0;
+    if (nrow != info->nloc || nrow > info->ntot) {
+        std::printf("TRLAN: info not setup for this problem.\n");
+        std::printf("       Please reset info before calling TRLAN.\n");
+        info->stat = -1;
+    }
+    if (info->nec < 0) info->nec = 0;
+    if (lde < nrow) {
+        std::printf("TRLAN: leading dimension of EVEC to small.\n");
+        info->stat = -2;
+    }
+    if (info->tol >= 1.0)
+        info->tol = std::sqrt(DBL_EPSILON);
+    else if (info->tol <= DBL_MIN)
+        info->tol = DBL_EPSILON;
+    if (info->ned + info->ned >= info->ntot) {
+        std::printf("TRLAN: info->ned (%d) is large relative to the matrix dimension (%d)\n", info->ned,
+                    info->ntot);
+        std::printf(" **    It is more appropriate to use LAPACK dsyev/ssyev.\n");
+        if (info->ned > info->ntot) {
+            info->ned = std::min(info->ntot - 1, info->maxlan - 3);
+            std::printf("TRLAN: ** reduced ned to %d **\n", info->ned);
+        }
+    }
+    if (mev < info->ned) {
+        std::printf("TRLAN: array EVAL and EVEC can not hold wanted number of eigenpairs.\n");
+        info->stat = -3;
+    }
+    if (info->ntot < 10) {
+        std::printf("TRLAN is not designed to work with such a small matrix(%dx%d).  Please use LAPACK or "
+                    "EISPACK instead.\n",
+                    info->ntot, info->ntot);
+        info->stat = -4;
+    }
+    if (info->maxlan < info->ned + 3) {
+        info->maxlan = info->ned + std::min(info->ned, 20) + (int)std::log((double)info->ntot);
+        info->maxlan = std::min(info->maxlan, info->ntot);
+        std::printf("TRLAN: ** reset maxlan to %d! **\n", info->maxlan);
+    }
+    if (info->maxlan < mev) {
+        int ntmp = std::min(info->ntot, std::max(100 + info->ned, 10 * info->ned));
+        info->maxlan = mev < ntmp ? mev : ntmp;
+    }
+    if (info->maxlan < 5) {
+        std::printf("TRLAN must have at least 5 basis vectors, it is currently %d.\n", info->maxlan);
+        info->stat = -5;
+    }
+    info->tmv = -1;
+    info->klan = std::min(info->maxlan, info->ntot);
+    if (info->restart >= 7) info->klan = std::min(info->maxlan, std::max(100, std::min(info->klan, 2 * info->ned)));
+    info->locked = info->nec;
+    info->matvec = 0;
+    info->nloop = 0;
+    info->north = 0;
+    info->nrand = 0;
+    info->flop = 0;
+    info->rflp = 0;
+    info->flop_h = 0;
+    info->rflp_h = 0;
+    info->flop_r = 0;
+    info->rflp_r = 0;
+    info->tick_t = 0.0;
+    info->clk_op = 0;
+    info->tick_o = 0.0;
+    info->clk_orth = 0;
+    info->tick_h = 0.0;
+    info->clk_res = 0;
+    info->tick_r = 0.0;
+    info->clk_in = 0;
+    info->clk_out = 0;
+    info->wrds_in = 0;
+    info->wrds_out = 0;
+    info->avgm = 0.0;
+}
+
+void run_trlan(trl_matvec op, trl_uo uo, trl_info *info, int nrow, int mev, double *eval, double *evec, int lde,
+               int lwrk, double *wrk, const Options &opt) {
+    const double t0 = now_s();
+    last_stats() = trlx_stats{};
+    if (info->ned > mev) {
+        std::printf("info->ned (%d) is larger than mev (%d) reducing info->ned to %d\n", info->ned, mev, mev);
+        info->ned = mev;
+    }
+    if (info->ned <= info->nec || info->ned <= 0) return;
+    info->stat = 0;
+    clear_counter(info, nrow, mev, lde);
+    if (info->stat != 0) return;
+    if (opt.basis_bits == 32)
+        solve<float>(op, uo, info, nrow, mev, eval, evec, lde, wrk, std::min(mev, lwrk), opt);
+    else
+        solve<double>(op, uo, info, nrow, mev, eval, evec, lde, wrk, std::min(mev, lwrk), opt);
+    info->tick_t += now_s() - t0;
+}
+
+void run_ztrlan(ztrl_matvec op, trl_info *info, int nrow, int mev, double *eval, trl_dcomplex *evec, int lde,
+                trl_dcomplex *misc, int nmis, const Options &opt) {
+    const double t0 = now_s();
+    last_stats() = trlx_stats{};
+    if (info->ned > mev) {
+        std::printf("info->ned (%d) is larger than mev (%d) reducing info->ned to %d\n", info->ned, mev, mev);
+        info->ned = mev;
+    }
+    if (info->ned <= info->nec || info->ned <= 0) return;
+    info->stat = 0;
+    clear_counter(info, nrow, mev, lde);
+    if (info->stat != 0) return;
+    std::vector<double> res(mev, 0.0);
+    if (opt.basis_bits == 32)
+        solve<zf>(op, nullptr, info, nrow, mev, eval, evec, lde, res.data(), mev, opt);
+    else
+        solve<zd>(op, nullptr, info, nrow, mev, eval, evec, lde, res.data(), mev, opt);
+    if (misc && nmis > 0) {
+        for (int i = 0; i < std::min(mev, nmis); ++i) misc[i] = trl_dcomplex{res[i], 0.0};
+    }
+    info->tick_t += now_s() - t0;
+}
+
+}  // namespace trlb

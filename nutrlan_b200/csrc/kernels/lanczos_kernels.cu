@@ -1,0 +1,467 @@
+// Lanczos vector kernels for sm_100a: classical Gram-Schmidt projection and
+// update (tall-skinny V^H r and r - V h), normalisation, and the restart
+// recombination V*Y.  These replace the reference's BLAS-2/3 calls in
+// trl_cgs (SRC/trlcore.c:2993-3011, trl_g_dot_ in SRC/trl_comm_none.c:238)
+// and trl_ritz_vectors (SRC/trlcore.c:2761-2910), and their complex twins
+// (SRC/ztrlcore.c:1977-2203, 1570-1751).
+//
+// All streaming kernels read 16-byte vectors per lane, keep every partial sum
+// in FP64, and reduce across the grid in a fixed order (per-block partials,
+// summed in block order by the last block to finish), so results are
+// bitwise reproducible run to run.
+#include <algorithm>
+#include <cstdio>
+#include <type_traits>
+
+#include "lanczos_kernels.h"
+
+namespace trlb {
+
+namespace {
+
+int g_num_sms = 0;
+
+int num_sms() {
+    if (g_num_sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+        if (g_num_sms <= 0) g_num_sms = 148;
+    }
+    return g_num_sms;
+}
+
+constexpr int kThreads = 256;
+constexpr int kProjColsPerWarp = 16;  // 8 warps x 16 = 128 columns per sweep
+
+enum TicketSlot { kTicketDot = 0, kTicketProject = 1, kTicketUpdate = 2 };
+
+// ---------------------------------------------------------------------------
+template <class C>
+__global__ void __launch_bounds__(kThreads) k_dot(const C *__restrict__ x, const C *__restrict__ y,
+                                                  long n_pad, double *part, unsigned *ticket,
+                                                  double *out) {
+    __shared__ double red[32];
+    double acc = 0.0;
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += stride) {
+        C xv = x[i], yv = y[i];
+        C t = czero(xv);
+        fma_conj(t, xv, yv);
+        acc += real_part(t);
+    }
+    double s = block_sum(acc, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+    if (last_block_arrived(ticket)) {
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (unsigned b = 0; b < gridDim.x; ++b) tot += __ldcg(part + b);
+            *out = tot;
+            *ticket = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Projection h = V^H r.  Block b owns rows [b*chunk, (b+1)*chunk); warp w of a
+// sweep owns columns c0 + w*CPW .. +CPW and keeps one FP64 accumulator per
+// column per lane across all the block's rows, so each basis element is
+// read exactly once and reduced with a single warp shuffle tree at the end.
+template <class T, int CPW>
+__global__ void __launch_bounds__(kThreads)
+    k_project(T *const *__restrict__ cols, int m, long n_pad, long chunk,
+              const typename Store<T>::C *__restrict__ r, Recur<typename Store<T>::C> rec,
+              typename Store<T>::C *part, double *part_r2, unsigned *ticket,
+              typename Store<T>::C *h, double *out2) {
+    using S = Store<T>;
+    using C = typename S::C;
+    constexpr int R = S::R;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long row0 = (long)blockIdx.x * chunk;
+    const long row1 = min(n_pad, row0 + chunk);
+    const double alpha = rec.on ? *rec.alpha : 0.0;
+    double r2acc = 0.0;
+    for (int c0 = 0; c0 < m; c0 += (kThreads / 32) * CPW) {
+        const int cb = c0 + warp * CPW;
+        const T *p[CPW];
+#pragma unroll
+        for (int k = 0; k < CPW; ++k) p[k] = (cb + k < m) ? cols[cb + k] : nullptr;
+        C acc[CPW];
+#pragma unroll
+        for (int k = 0; k < CPW; ++k) acc[k] = czero(C());
+        for (long i = row0 + lane * R; i < row1; i += 32 * R) {
+            C rv[R];
+            load_c<R>(r + i, rv);
+            if (rec.on) {
+                C xv[R], xpv[R];
+                load_c<R>(rec.x + i, xv);
+                load_c<R>(rec.xp + i, xpv);
+#pragma unroll
+                for (int q = 0; q < R; ++q) rv[q] = rv[q] - alpha * xv[q] - rec.beta * xpv[q];
+            }
+            if (c0 == 0 && warp == 0) {
+#pragma unroll
+                for (int q = 0; q < R; ++q) r2acc += abs2(rv[q]);
+            }
+#pragma unroll
+            for (int k = 0; k < CPW; ++k) {
+                if (p[k]) {
+                    C v[R];
+                    S::load(p[k] + i, v);
+#pragma unroll
+                    for (int q = 0; q < R; ++q) fma_conj(acc[k], v[q], rv[q]);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < CPW; ++k) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[k] = acc[k] + shfl_down(acc[k], o);
+            if (lane == 0 && cb + k < m) part[(long)blockIdx.x * m + cb + k] = acc[k];
+        }
+    }
+    if (warp == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r2acc += __shfl_down_sync(0xffffffffu, r2acc, o);
+        if (lane == 0) part_r2[blockIdx.x] = r2acc;
+    }
+    if (last_block_arrived(ticket)) {
+        __shared__ double red[32];
+        const int nb = gridDim.x;
+        double h2loc = 0.0;
+        for (int c = threadIdx.x; c < m; c += blockDim.x) {
+            C s = czero(C());
+            for (int b = 0; b < nb; ++b) s = s + ldcg(part + (long)b * m + c);
+            h[c] = s;
+            h2loc += abs2(s);
+        }
+        double h2 = block_sum(h2loc, red);
+        if (threadIdx.x == 0) {
+            double r2 = 0.0;
+            for (int b = 0; b < nb; ++b) r2 += __ldcg(part_r2 + b);
+            out2[0] = r2;
+            out2[1] = h2;
+            *ticket = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Update r_out = r - V h with h and the column pointers staged in shared
+// memory; each thread owns R consecutive rows and walks the columns with four
+// independent 16-byte loads in flight.
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    k_update(T *const *__restrict__ cols, int m, long n_pad, const typename Store<T>::C *r,
+             Recur<typename Store<T>::C> rec, const typename Store<T>::C *__restrict__ h,
+             typename Store<T>::C *r_out, double *part_r2, unsigned *ticket, double *out_r2) {
+    using S = Store<T>;
+    using C = typename S::C;
+    constexpr int R = S::R;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *hs = reinterpret_cast<C *>(smem_raw);
+    const T **ps = reinterpret_cast<const T **>(smem_raw + sizeof(C) * m);
+    for (int c = threadIdx.x; c < m; c += blockDim.x) {
+        hs[c] = h[c];
+        ps[c] = cols[c];
+    }
+    __syncthreads();
+    const double alpha = rec.on ? *rec.alpha : 0.0;
+    double r2acc = 0.0;
+    const long stride = (long)gridDim.x * blockDim.x * R;
+    for (long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) * R; i < n_pad; i += stride) {
+        C acc[R];
+        load_c<R>(r + i, acc);
+        if (rec.on) {
+            C xv[R], xpv[R];
+            load_c<R>(rec.x + i, xv);
+            load_c<R>(rec.xp + i, xpv);
+#pragma unroll
+            for (int q = 0; q < R; ++q) acc[q] = acc[q] - alpha * xv[q] - rec.beta * xpv[q];
+        }
+        int c = 0;
+        for (; c + 4 <= m; c += 4) {
+            C v0[R], v1[R], v2[R], v3[R];
+            S::load(ps[c] + i, v0);
+            S::load(ps[c + 1] + i, v1);
+            S::load(ps[c + 2] + i, v2);
+            S::load(ps[c + 3] + i, v3);
+            const C h0 = hs[c], h1 = hs[c + 1], h2 = hs[c + 2], h3 = hs[c + 3];
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+                fms(acc[q], v0[q], h0);
+                fms(acc[q], v1[q], h1);
+                fms(acc[q], v2[q], h2);
+                fms(acc[q], v3[q], h3);
+            }
+        }
+        for (; c < m; ++c) {
+            C v[R];
+            S::load(ps[c] + i, v);
+            const C hc = hs[c];
+#pragma unroll
+            for (int q = 0; q < R; ++q) fms(acc[q], v[q], hc);
+        }
+        store_c<R>(r_out + i, acc);
+#pragma unroll
+        for (int q = 0; q < R; ++q) r2acc += abs2(acc[q]);
+    }
+    __shared__ double red[32];
+    double s = block_sum(r2acc, red);
+    if (threadIdx.x == 0) part_r2[blockIdx.x] = s;
+    if (last_block_arrived(ticket)) {
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (unsigned b = 0; b < gridDim.x; ++b) tot += __ldcg(part_r2 + b);
+            *out_r2 = tot;
+            *ticket = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    k_normalize(typename Store<T>::C *r, long n_pad, const double *r2, double fixed,
+                typename Store<T>::C *q, T *vcol) {
+    using S = Store<T>;
+    const double sc = r2 ? 1.0 / sqrt(*r2) : fixed;
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += stride) {
+        auto v = r[i] * sc;
+        q[i] = v;
+        if (vcol) vcol[i] = S::from_c(v);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// out[:,k] = sum_c in[:,c] Y[c,k]: 64x64 output tiles, K in steps of 16,
+// each thread a 4x4 register tile (rows ty+16q, columns tx+16p).
+constexpr int kBM = 64, kBN = 64, kBK = 16;
+
+template <class T, class OutT>
+__global__ void __launch_bounds__(kThreads)
+    k_ritz(T *const *__restrict__ in_cols, int jml, const double *__restrict__ Y, int ldy, int kept,
+           OutT *const *out_cols, OutT *out, long ldo, long n_valid) {
+    using S = Store<T>;
+    using C = typename S::C;
+    __shared__ C As[kBK][kBM + 1];
+    __shared__ double Bs[kBK][kBN + 1];
+    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+    const long i0 = (long)blockIdx.x * kBM;
+    const int k0 = blockIdx.y * kBN;
+    C acc[4][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int p = 0; p < 4; ++p) acc[q][p] = czero(C());
+    for (int c0 = 0; c0 < jml; c0 += kBK) {
+        {  // A tile: column kk = t/16, rows (t%16)*4 .. +4
+            const int kk = t >> 4, rr = (t & 15) * 4;
+            const int c = c0 + kk;
+            if (c < jml) {
+                const T *col = in_cols[c] + i0 + rr;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) As[kk][rr + q] = S::to_c(col[q]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) As[kk][rr + q] = czero(C());
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {  // B tile
+            const int idx = t + e * kThreads;
+            const int kk = idx / kBN, kc = idx % kBN;
+            const int c = c0 + kk, k = k0 + kc;
+            Bs[kk][kc] = (c < jml && k < kept) ? Y[(long)c + (long)k * ldy] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < kBK; ++kk) {
+            C a[4];
+            double b[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) a[q] = As[kk][ty + 16 * q];
+#pragma unroll
+            for (int p = 0; p < 4; ++p) b[p] = Bs[kk][tx + 16 * p];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int p = 0; p < 4; ++p) fma_real(acc[q][p], a[q], b[p]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int k = k0 + tx + 16 * p;
+        if (k >= kept) continue;
+        OutT *dst = out_cols ? out_cols[k] : out + (long)k * ldo;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const long row = i0 + ty + 16 * q;
+            if (row < n_valid) {
+                if constexpr (std::is_same<OutT, C>::value) {
+                    dst[row] = acc[q][p];
+                } else {
+                    dst[row] = S::from_c(acc[q][p]);
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_store(const typename Store<T>::C *src, long n_pad, T *dst) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += stride)
+        dst[i] = Store<T>::from_c(src[i]);
+}
+template <class T>
+__global__ void k_load(const T *src, long n, typename Store<T>::C *dst) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        dst[i] = Store<T>::to_c(src[i]);
+}
+
+// Smoothed random vector: s_i = 2u_i + u_{i+1} + u_{i-1} (cyclic), with the
+// reference's boundary stencil (trl_smooth_rr, SRC/trlcore.c:1534-1575):
+// s_0 uses u_2 and s_{n-1} uses the already smoothed s_1.
+__device__ inline double smooth_at(uint64_t seed, long n, long i) {
+    auto u = [&](long k) { return uniform01(seed, (uint64_t)k); };
+    if (n < 3) return u(i);
+    if (i == 0) return 2.0 * u(0) + u(2) + u(n - 1);
+    if (i == n - 1) {
+        double s1 = 2.0 * u(1) + u(2) + u(0);
+        return 2.0 * u(n - 1) + s1 + u(n - 2);
+    }
+    return 2.0 * u(i) + u(i + 1) + u(i - 1);
+}
+__global__ void k_random_real(double *dst, long n, long n_pad, uint64_t seed) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += stride)
+        dst[i] = i < n ? smooth_at(seed, n, i) : 0.0;
+}
+__global__ void k_random_cplx(zd *dst, long n, long n_pad, uint64_t seed) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    const uint64_t seed_im = seed ^ 0x5DEECE66Dull;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += stride)
+        dst[i] = i < n ? zd{smooth_at(seed, n, i), smooth_at(seed_im, n, i)} : zd{0.0, 0.0};
+}
+
+int elementwise_blocks(long n) {
+    long b = (n + kThreads - 1) / kThreads;
+    return (int)std::max<long>(1, std::min<long>(b, (long)num_sms() * 8));
+}
+
+}  // namespace
+
+int stream_blocks(long n_pad, int rows_per_group) {
+    long need = (n_pad + (long)kThreads * rows_per_group - 1) / ((long)kThreads * rows_per_group);
+    long cap = (long)num_sms() * 4;
+    return (int)std::max<long>(1, std::min(need, cap));
+}
+
+template <class C>
+void launch_dot(const C *x, const C *y, long n_pad, double *out, Scratch &s, cudaStream_t st) {
+    int nb = std::min(stream_blocks(n_pad, 1), s.max_blocks);
+    k_dot<C><<<nb, kThreads, 0, st>>>(x, y, n_pad, reinterpret_cast<double *>(s.partials),
+                                      s.tickets + kTicketDot, out);
+}
+
+template <class T>
+void launch_project(T *const *cols, int m, long n_pad, const typename Store<T>::C *r,
+                    Recur<typename Store<T>::C> rec, typename Store<T>::C *h, double *out2,
+                    Scratch &s, cudaStream_t st) {
+    using C = typename Store<T>::C;
+    constexpr int R = Store<T>::R;
+    int nb = std::min(stream_blocks(n_pad, R), s.max_blocks);
+    long per = (n_pad + nb - 1) / nb;
+    long chunk = (per + 32 * R - 1) / (32 * R) * (32 * R);
+    nb = (int)((n_pad + chunk - 1) / chunk);
+    C *part = reinterpret_cast<C *>(s.partials);
+    double *part_r2 = reinterpret_cast<double *>(part + (long)nb * m);
+    k_project<T, kProjColsPerWarp><<<nb, kThreads, 0, st>>>(
+        cols, m, n_pad, chunk, r, rec, part, part_r2, s.tickets + kTicketProject, h, out2);
+}
+
+template <class T>
+void launch_update(T *const *cols, int m, long n_pad, const typename Store<T>::C *r,
+                   Recur<typename Store<T>::C> rec, const typename Store<T>::C *h,
+                   typename Store<T>::C *r_out, double *out_r2, Scratch &s, cudaStream_t st) {
+    using C = typename Store<T>::C;
+    constexpr int R = Store<T>::R;
+    int nb = std::min(stream_blocks(n_pad, R), s.max_blocks);
+    size_t smem = (sizeof(C) + sizeof(T *)) * (size_t)std::max(m, 1);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_update<T><<<nb, kThreads, smem, st>>>(cols, m, n_pad, r, rec, h, r_out,
+                                             reinterpret_cast<double *>(s.partials),
+                                             s.tickets + kTicketUpdate, out_r2);
+}
+
+template <class T>
+void launch_normalize(typename Store<T>::C *r, long n_pad, const double *r2, double fixed,
+                      typename Store<T>::C *q, T *vcol, cudaStream_t st) {
+    k_normalize<T><<<elementwise_blocks(n_pad), kThreads, 0, st>>>(r, n_pad, r2, fixed, q, vcol);
+}
+
+template <class T>
+void launch_ritz(T *const *in_cols, int jml, long n_pad, const double *Y, int ldy, int kept,
+                 T *const *out_cols, cudaStream_t st) {
+    if (kept <= 0) return;
+    dim3 grid((unsigned)(n_pad / kBM), (unsigned)((kept + kBN - 1) / kBN));
+    k_ritz<T, T><<<grid, kThreads, 0, st>>>(in_cols, jml, Y, ldy, kept, out_cols, nullptr, 0, n_pad);
+}
+
+template <class T>
+void launch_ritz_out(T *const *in_cols, int jml, long n_pad, const double *Y, int ldy, int kept,
+                     typename Store<T>::C *out, long ldo, long n, cudaStream_t st) {
+    using C = typename Store<T>::C;
+    if (kept <= 0) return;
+    dim3 grid((unsigned)(n_pad / kBM), (unsigned)((kept + kBN - 1) / kBN));
+    k_ritz<T, C><<<grid, kThreads, 0, st>>>(in_cols, jml, Y, ldy, kept, nullptr, out, ldo, n);
+}
+
+template <class T>
+void launch_store(const typename Store<T>::C *src, long n_pad, T *dst, cudaStream_t st) {
+    k_store<T><<<elementwise_blocks(n_pad), kThreads, 0, st>>>(src, n_pad, dst);
+}
+template <class T>
+void launch_load(const T *src, long n, typename Store<T>::C *dst, cudaStream_t st) {
+    k_load<T><<<elementwise_blocks(n), kThreads, 0, st>>>(src, n, dst);
+}
+
+template <>
+void launch_random<double>(double *dst, long n, long n_pad, uint64_t seed, cudaStream_t st) {
+    k_random_real<<<elementwise_blocks(n_pad), kThreads, 0, st>>>(dst, n, n_pad, seed);
+}
+template <>
+void launch_random<zd>(zd *dst, long n, long n_pad, uint64_t seed, cudaStream_t st) {
+    k_random_cplx<<<elementwise_blocks(n_pad), kThreads, 0, st>>>(dst, n, n_pad, seed);
+}
+
+#define TRLB_INST(T)                                                                              \
+    template void launch_project<T>(T *const *, int, long, const Store<T>::C *, Recur<Store<T>::C>, \
+                                    Store<T>::C *, double *, Scratch &, cudaStream_t);            \
+    template void launch_update<T>(T *const *, int, long, const Store<T>::C *, Recur<Store<T>::C>,  \
+                                   const Store<T>::C *, Store<T>::C *, double *, Scratch &,        \
+                                   cudaStream_t);                                                 \
+    template void launch_normalize<T>(Store<T>::C *, long, const double *, double, Store<T>::C *,  \
+                                      T *, cudaStream_t);                                         \
+    template void launch_ritz<T>(T *const *, int, long, const double *, int, int, T *const *,     \
+                                 cudaStream_t);                                                   \
+    template void launch_ritz_out<T>(T *const *, int, long, const double *, int, int,             \
+                                     Store<T>::C *, long, long, cudaStream_t);                    \
+    template void launch_store<T>(const Store<T>::C *, long, T *, cudaStream_t);                  \
+    template void launch_load<T>(const T *, long, Store<T>::C *, cudaStream_t);
+
+TRLB_INST(double)
+TRLB_INST(float)
+TRLB_INST(zd)
+TRLB_INST(zf)
+template void launch_dot<double>(const double *, const double *, long, double *, Scratch &,
+                                 cudaStream_t);
+template void launch_dot<zd>(const zd *, const zd *, long, double *, Scratch &, cudaStream_t);
+
+}  // namespace trlb

@@ -1,0 +1,370 @@
+// Sparse matrix-vector kernels for the built-in operators.
+//
+// CSR: one row per group of 8 lanes (rows of the configured stencils have
+// 5-7 entries), so each group reads its row's values and column indices
+// coalesced and reduces with 3 shuffles.  SELL-C-32: one row per lane, the
+// slice stored column-major (entry k of the 32 rows contiguous), so every
+// value/index load of a warp is one 128/256-byte segment.  Both fuse the
+// Lanczos alpha = x^H y into the same pass.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "../../../include/trlx.h"
+#include "spmv.h"
+
+namespace trlb {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kGroup = 8;
+constexpr int kTicketSpmv = 3;
+
+template <class V>
+__device__ __forceinline__ V ld_val(const V *p) {
+    return *p;
+}
+__device__ __forceinline__ double mulx(double a, double x) { return a * x; }
+__device__ __forceinline__ zd mulx(zd a, zd x) { return zd{a.x * x.x - a.y * x.y, a.x * x.y + a.y * x.x}; }
+__device__ __forceinline__ double shfl_xor(double v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
+__device__ __forceinline__ zd shfl_xor(zd v, int o) {
+    return zd{__shfl_xor_sync(0xffffffffu, v.x, o), __shfl_xor_sync(0xffffffffu, v.y, o)};
+}
+__device__ __forceinline__ double ldg_c(const double *p) { return __ldg(p); }
+__device__ __forceinline__ zd ldg_c(const zd *p) {
+    double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+    return zd{v.x, v.y};
+}
+
+template <class V>
+__global__ void __launch_bounds__(kThreads)
+    k_csr(int nrow, long n_pad, const long long *__restrict__ rp, const int *__restrict__ ci,
+          const V *__restrict__ va, const V *__restrict__ x, V *__restrict__ y, double *part,
+          unsigned *ticket, double *alpha_out) {
+    const int g = threadIdx.x & (kGroup - 1);
+    const long groups = (long)gridDim.x * (kThreads / kGroup);
+    double aacc = 0.0;
+    // Rows are visited in rounds so that all lanes of a warp stay converged
+    // for the shuffles (bounds are uniform per round across the grid).
+    const long rounds = (n_pad + groups - 1) / groups;
+    for (long rd = 0; rd < rounds; ++rd) {
+        const long row = rd * groups + (long)blockIdx.x * (kThreads / kGroup) + (threadIdx.x / kGroup);
+        V acc = czero(V());
+        if (row < nrow) {
+            const long b = rp[row], e = rp[row + 1];
+            for (long k = b + g; k < e; k += kGroup) acc = acc + mulx(ld_val(va + k), ldg_c(x + ci[k]));
+        }
+#pragma unroll
+        for (int o = kGroup / 2; o > 0; o >>= 1) acc = acc + shfl_xor(acc, o);
+        if (g == 0 && row < n_pad) {
+            y[row] = acc;  // rows in [nrow, n_pad) get zero
+            if (alpha_out) {
+                V t = czero(V());
+                fma_conj(t, ldg_c(x + row), acc);
+                aacc += real_part(t);
+            }
+        }
+    }
+    if (!alpha_out) return;
+    __shared__ double red[32];
+    double s = block_sum(aacc, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+    if (last_block_arrived(ticket)) {
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (unsigned b = 0; b < gridDim.x; ++b) tot += __ldcg(part + b);
+            *alpha_out = tot;
+            *ticket = 0;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_sell(int nrow, long n_pad, int nslice, const long long *__restrict__ sp,
+           const int *__restrict__ ci, const double *__restrict__ va, const int *__restrict__ perm,
+           const double *__restrict__ x, double *__restrict__ y, double *part, unsigned *ticket,
+           double *alpha_out) {
+    const int lane = threadIdx.x & 31;
+    const long warps = (long)gridDim.x * (kThreads / 32);
+    double aacc = 0.0;
+    for (long s = (long)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); s < nslice; s += warps) {
+        const long b = sp[s];
+        const int w = (int)((sp[s + 1] - b) >> 5);
+        double acc = 0.0;
+        const double *v = va + b + lane;
+        const int *c = ci + b + lane;
+#pragma unroll 4
+        for (int k = 0; k < w; ++k) acc = fma(__ldg(v + (long)k * 32), __ldg(x + __ldg(c + (long)k * 32)), acc);
+        const long srow = s * 32 + lane;
+        if (srow < nrow) {
+            const int row = perm ? perm[srow] : (int)srow;
+            y[row] = acc;
+            if (alpha_out) aacc = fma(__ldg(x + row), acc, aacc);
+        }
+    }
+    // Zero the padding rows [nrow, n_pad).
+    for (long i = nrow + (long)blockIdx.x * kThreads + threadIdx.x; i < n_pad; i += (long)gridDim.x * kThreads)
+        y[i] = 0.0;
+    if (!alpha_out) return;
+    __shared__ double red[32];
+    double s2 = block_sum(aacc, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = s2;
+    if (last_block_arrived(ticket)) {
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (unsigned bb = 0; bb < gridDim.x; ++bb) tot += __ldcg(part + bb);
+            *alpha_out = tot;
+            *ticket = 0;
+        }
+    }
+}
+
+int spmv_blocks(long work_items, int per_block) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long need = (work_items + per_block - 1) / per_block;
+    return (int)std::max<long>(1, std::min<long>(need, (long)sms * 8));
+}
+
+}  // namespace
+
+void spmv_fused_real(const trlx_operator *A, const double *x, double *y, long n_pad,
+                     double *alpha_out, Scratch *s, cudaStream_t st) {
+    double *part = s ? reinterpret_cast<double *>(s->partials) : nullptr;
+    unsigned *tk = s ? s->tickets + kTicketSpmv : nullptr;
+    if (A->kind == 0) {
+        int nb = spmv_blocks(n_pad, kThreads / kGroup);
+        if (s) nb = std::min(nb, s->max_blocks);
+        k_csr<double><<<nb, kThreads, 0, st>>>(A->nrow, n_pad, A->row_ptr, A->col,
+                                               static_cast<const double *>(A->val), x, y, part, tk,
+                                               alpha_out);
+    } else {
+        int nb = spmv_blocks((long)A->nslice * 32, kThreads);
+        if (s) nb = std::min(nb, s->max_blocks);
+        k_sell<<<nb, kThreads, 0, st>>>(A->nrow, n_pad, A->nslice, A->slice_ptr, A->col,
+                                        static_cast<const double *>(A->val), A->perm, x, y, part, tk,
+                                        alpha_out);
+    }
+}
+
+void spmv_fused_cplx(const trlx_operator *A, const zd *x, zd *y, long n_pad, double *alpha_out,
+                     Scratch *s, cudaStream_t st) {
+    double *part = s ? reinterpret_cast<double *>(s->partials) : nullptr;
+    unsigned *tk = s ? s->tickets + kTicketSpmv : nullptr;
+    int nb = spmv_blocks(n_pad, kThreads / kGroup);
+    if (s) nb = std::min(nb, s->max_blocks);
+    k_csr<zd><<<nb, kThreads, 0, st>>>(A->nrow, n_pad, A->row_ptr, A->col,
+                                       static_cast<const zd *>(A->val), x, y, part, tk, alpha_out);
+}
+
+void spmv_plain(const trlx_operator *A, const void *x, void *y, cudaStream_t st) {
+    // n_pad == nrow: no padding rows written.
+    if (A->kind == 2)
+        spmv_fused_cplx(A, static_cast<const zd *>(x), static_cast<zd *>(y), A->nrow, nullptr, nullptr, st);
+    else
+        spmv_fused_real(A, static_cast<const double *>(x), static_cast<double *>(y), A->nrow, nullptr,
+                        nullptr, st);
+}
+
+double spmv_bytes(const trlx_operator *A) {
+    const double vs = A->kind == 2 ? 16.0 : 8.0;
+    double b = (double)A->nnz * (vs + 4.0) + 2.0 * vs * A->nrow;
+    if (A->kind == 1)
+        b += 8.0 * (A->nslice + 1) + (A->perm ? 4.0 * A->nrow : 0.0);
+    else
+        b += 8.0 * (A->nrow + 1.0);
+    return b;
+}
+
+}  // namespace trlb
+
+// ---------------------------------------------------------------------------
+// C API
+// ---------------------------------------------------------------------------
+namespace {
+
+template <class X>
+int to_device(const X *src, size_t count, int where, X **dst) {
+    if (count == 0) {
+        *dst = nullptr;
+        return 0;
+    }
+    if (cudaMalloc(reinterpret_cast<void **>(dst), count * sizeof(X)) != cudaSuccess) return -2;
+    cudaMemcpyKind kind = where == TRLX_DEVICE_ARRAYS ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (cudaMemcpy(*dst, src, count * sizeof(X), kind) != cudaSuccess) return -3;
+    return 0;
+}
+
+template <class X>
+std::vector<X> to_host(const X *src, size_t count, int where) {
+    std::vector<X> h(count);
+    if (count == 0) return h;
+    if (where == TRLX_DEVICE_ARRAYS)
+        cudaMemcpy(h.data(), src, count * sizeof(X), cudaMemcpyDeviceToHost);
+    else
+        std::memcpy(h.data(), src, count * sizeof(X));
+    return h;
+}
+
+int check_csr(int nrow, const long long *rp, const int *ci, const void *val) {
+    if (nrow <= 0 || !rp || !ci || !val) return -1;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int trlx_csr_create(int nrow, const long long *row_ptr, const int *col_idx,
+                               const double *val, int where, trlx_operator **out) {
+    if (!out || check_csr(nrow, row_ptr, col_idx, val)) return -1;
+    auto *A = new trlx_operator();
+    A->kind = 0;
+    A->nrow = nrow;
+    long long nnz = 0;
+    if (where == TRLX_DEVICE_ARRAYS)
+        cudaMemcpy(&nnz, row_ptr + nrow, sizeof(long long), cudaMemcpyDeviceToHost);
+    else
+        nnz = row_ptr[nrow];
+    A->nnz = nnz;
+    cudaGetDevice(&A->device);
+    int rc = to_device(row_ptr, (size_t)nrow + 1, where, &A->row_ptr);
+    if (!rc) rc = to_device(col_idx, (size_t)nnz, where, &A->col);
+    double *dv = nullptr;
+    if (!rc) rc = to_device(val, (size_t)nnz, where, &dv);
+    A->val = dv;
+    if (rc) {
+        trlx_operator_destroy(A);
+        return rc;
+    }
+    *out = A;
+    return 0;
+}
+
+extern "C" int trlx_zcsr_create(int nrow, const long long *row_ptr, const int *col_idx,
+                                const trl_dcomplex *val, int where, trlx_operator **out) {
+    if (!out || check_csr(nrow, row_ptr, col_idx, val)) return -1;
+    auto *A = new trlx_operator();
+    A->kind = 2;
+    A->nrow = nrow;
+    long long nnz = 0;
+    if (where == TRLX_DEVICE_ARRAYS)
+        cudaMemcpy(&nnz, row_ptr + nrow, sizeof(long long), cudaMemcpyDeviceToHost);
+    else
+        nnz = row_ptr[nrow];
+    A->nnz = nnz;
+    cudaGetDevice(&A->device);
+    int rc = to_device(row_ptr, (size_t)nrow + 1, where, &A->row_ptr);
+    if (!rc) rc = to_device(col_idx, (size_t)nnz, where, &A->col);
+    trlb::zd *dv = nullptr;
+    if (!rc) rc = to_device(reinterpret_cast<const trlb::zd *>(val), (size_t)nnz, where, &dv);
+    A->val = dv;
+    if (rc) {
+        trlx_operator_destroy(A);
+        return rc;
+    }
+    *out = A;
+    return 0;
+}
+
+extern "C" int trlx_sell_create(int nrow, const long long *row_ptr, const int *col_idx,
+                                const double *val, int sigma, int where, trlx_operator **out) {
+    if (!out || check_csr(nrow, row_ptr, col_idx, val)) return -1;
+    if (sigma < 1) sigma = 1;
+    std::vector<long long> rp = to_host(row_ptr, (size_t)nrow + 1, where);
+    const long long nnz = rp[nrow];
+    std::vector<int> ci = to_host(col_idx, (size_t)nnz, where);
+    std::vector<double> va = to_host(val, (size_t)nnz, where);
+    // Within windows of sigma rows, order rows by decreasing length.
+    std::vector<int> order(nrow);
+    std::iota(order.begin(), order.end(), 0);
+    if (sigma > 1) {
+        for (long w0 = 0; w0 < nrow; w0 += sigma) {
+            long w1 = std::min<long>(nrow, w0 + sigma);
+            std::stable_sort(order.begin() + w0, order.begin() + w1, [&](int a, int b) {
+                return (rp[a + 1] - rp[a]) > (rp[b + 1] - rp[b]);
+            });
+        }
+    }
+    const int nslice = (nrow + 31) / 32;
+    std::vector<long long> sp(nslice + 1, 0);
+    for (int s = 0; s < nslice; ++s) {
+        long long w = 0;
+        for (int l = 0; l < 32; ++l) {
+            long r = (long)s * 32 + l;
+            if (r < nrow) w = std::max(w, rp[order[r] + 1] - rp[order[r]]);
+        }
+        sp[s + 1] = sp[s] + w * 32;
+    }
+    const long long total = sp[nslice];
+    std::vector<int> sc(total, 0);
+    std::vector<double> sv(total, 0.0);
+    for (int s = 0; s < nslice; ++s) {
+        const long long w = (sp[s + 1] - sp[s]) / 32;
+        for (int l = 0; l < 32; ++l) {
+            long r = (long)s * 32 + l;
+            int orig = r < nrow ? order[r] : -1;
+            long long len = orig >= 0 ? rp[orig + 1] - rp[orig] : 0;
+            for (long long k = 0; k < w; ++k) {
+                long long dst = sp[s] + k * 32 + l;
+                if (k < len) {
+                    sc[dst] = ci[rp[orig] + k];
+                    sv[dst] = va[rp[orig] + k];
+                } else {
+                    // Padding: zero value, column of the row itself (always valid).
+                    sc[dst] = orig >= 0 ? orig : 0;
+                    sv[dst] = 0.0;
+                }
+            }
+        }
+    }
+    auto *A = new trlx_operator();
+    A->kind = 1;
+    A->nrow = nrow;
+    A->nnz = total;
+    A->nslice = nslice;
+    A->sigma = sigma;
+    cudaGetDevice(&A->device);
+    int rc = to_device(sp.data(), sp.size(), TRLX_HOST_ARRAYS, &A->slice_ptr);
+    if (!rc) rc = to_device(sc.data(), sc.size(), TRLX_HOST_ARRAYS, &A->col);
+    double *dv = nullptr;
+    if (!rc) rc = to_device(sv.data(), sv.size(), TRLX_HOST_ARRAYS, &dv);
+    A->val = dv;
+    bool identity = true;
+    for (int i = 0; i < nrow && identity; ++i) identity = (order[i] == i);
+    if (!rc && !identity) rc = to_device(order.data(), order.size(), TRLX_HOST_ARRAYS, &A->perm);
+    if (rc) {
+        trlx_operator_destroy(A);
+        return rc;
+    }
+    *out = A;
+    return 0;
+}
+
+extern "C" void trlx_operator_destroy(trlx_operator *A) {
+    if (!A) return;
+    cudaFree(A->row_ptr);
+    cudaFree(A->col);
+    cudaFree(A->val);
+    cudaFree(A->slice_ptr);
+    cudaFree(A->perm);
+    delete A;
+}
+
+extern "C" long long trlx_operator_nnz(const trlx_operator *A) { return A ? A->nnz : 0; }
+extern "C" int trlx_operator_nrow(const trlx_operator *A) { return A ? A->nrow : 0; }
+
+extern "C" void trlx_matvec(const int nrow, const int ncol, const double *x, const int ldx, double *y,
+                            const int ldy, void *mvparam) {
+    auto *A = static_cast<trlx_operator *>(mvparam);
+    if (!A || A->kind == 2 || nrow != A->nrow) return;
+    for (int j = 0; j < ncol; ++j) trlb::spmv_plain(A, x + (long)j * ldx, y + (long)j * ldy, 0);
+}
+
+extern "C" void trlx_zmatvec(const int nrow, const int ncol, const trl_dcomplex *x, const int ldx,
+                             trl_dcomplex *y, const int ldy, void *mvparam) {
+    auto *A = static_cast<trlx_operator *>(mvparam);
+    if (!A || A->kind != 2 || nrow != A->nrow) return;
+    for (int j = 0; j < ncol; ++j) trlb::spmv_plain(A, x + (long)j * ldx, y + (long)j * ldy, 0);
+}

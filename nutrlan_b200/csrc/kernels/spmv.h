@@ -1,0 +1,43 @@
+// Built-in sparse operators (CSR, SELL-C-sigma, complex CSR) and their
+// fused product kernels.  The engine calls spmv_fused() when the user's
+// `op` is trlx_matvec / trlx_zmatvec; the fused kernel produces y = A x and
+// alpha = Re(x^H y) in one pass over the matrix (the reference computes the
+// alpha dot separately after the callback, SRC/trlcore.c:1098-1108).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "lanczos_kernels.h"
+
+struct trlx_operator {
+    int kind = 0;  // 0 real CSR, 1 real SELL-C-32, 2 complex CSR
+    int nrow = 0;
+    long long nnz = 0;
+    // CSR
+    long long *row_ptr = nullptr;
+    int *col = nullptr;
+    void *val = nullptr;  // double or zd
+    // SELL-C-32
+    int nslice = 0;
+    int sigma = 1;
+    long long *slice_ptr = nullptr;  // offset of slice s (entries), nslice+1
+    int *perm = nullptr;             // stored row -> original row (nullptr = identity)
+    int device = -1;
+};
+
+namespace trlb {
+
+// y = A x and, if alpha_out != null, *alpha_out = Re(x^H y) (deterministic).
+// x, y are compute vectors of n_pad rows (padding rows of y are written 0).
+void spmv_fused_real(const trlx_operator *A, const double *x, double *y, long n_pad,
+                     double *alpha_out, Scratch *s, cudaStream_t st);
+void spmv_fused_cplx(const trlx_operator *A, const zd *x, zd *y, long n_pad,
+                     double *alpha_out, Scratch *s, cudaStream_t st);
+
+// Plain product with leading dimensions (used by trlx_matvec called directly).
+void spmv_plain(const trlx_operator *A, const void *x, void *y, cudaStream_t st);
+
+// Algorithmic bytes of one product (values + indices + row pointers + x + y).
+double spmv_bytes(const trlx_operator *A);
+
+}  // namespace trlb

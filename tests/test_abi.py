@@ -1,0 +1,71 @@
+"""The C-ABI library loads without a GPU and exports every declared symbol;
+trl_info keeps the reference's layout."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from nutrlan_b200 import TrlInfo, LIB_PATH
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in ("trlan.h", "ztrlan.h", "trlx.h"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b([a-z_][a-z0-9_]*)\s*\(", text):
+            name = m.group(1)
+            if name.startswith(("trl", "ztrl")) and name not in ("trl_matvec", "trl_uo", "ztrl_matvec"):
+                names.add(name)
+    return names
+
+
+def test_library_loads_and_exports_all_declared_symbols(lib):
+    names = declared_functions()
+    assert "trlan" in names and "ztrlan" in names and "trlx_trlan" in names
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB_PATH], capture_output=True, text=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    missing = sorted(n for n in names if n not in exported)
+    assert not missing, missing
+    for n in names:
+        getattr(lib, n)
+
+
+def test_trl_info_layout_matches_reference_header():
+    assert C.sizeof(TrlInfo) == 800
+    assert TrlInfo.mvparam.offset == 792
+    assert TrlInfo.clk_rate.offset == 112
+    assert TrlInfo.anrm.offset == 208
+    assert TrlInfo.log_file.offset == 392
+
+
+def test_header_compiles_and_layout_in_c(tmp_path):
+    src = tmp_path / "abi.c"
+    src.write_text(
+        "#include <stddef.h>\n#include <stdio.h>\n#include \"trlx.h\"\n"
+        "int main(){printf(\"%zu %zu\\n\", sizeof(trl_info), offsetof(trl_info, mvparam));"
+        "return 0;}\n")
+    exe = tmp_path / "abi"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    assert out == ["800", "792"]
+
+
+def test_init_info_defaults(lib):
+    info = TrlInfo()
+    lib.trl_init_info(C.byref(info), 1000, 50, -1, 5, 0.0, 0, 0, None)
+    assert info.tol == pytest.approx(1.4901161193847656e-08)
+    assert info.restart == 0 and info.maxlan == 50 and info.ned == 5
+    assert info.maxmv == 1000 and info.ntot == 1000 and info.nloc == 1000
+    assert info.trgt < -1e300 and info.tres == -1.0 and info.crat == 1.0 and info.tmv == -1
+    # tol > 1 is read as a reciprocal, tol tiny becomes eps
+    lib.trl_init_info(C.byref(info), 1000, 3, 1, 5, 50.0, 7, 100, None)
+    assert info.tol == pytest.approx(0.02) and info.maxlan == 11 and info.restart == 7
+
+
+def test_version_string(lib):
+    assert b"sm_100a" in lib.trlx_version()
