@@ -98,6 +98,7 @@ typedef struct {
     double kernel_seconds[8];
     double kernel_bytes[8];
     long long kernel_count[8];
+    double seconds_setup;     /* workspace acquisition and initialisation  */
 } trlx_stats;
 
 #define TRLX_K_SPMV 0      /* built-in operator (+ fused alpha)          */
@@ -109,6 +110,10 @@ typedef struct {
 #define TRLX_K_OTHER 6
 
 void trlx_get_last_stats(trlx_stats *stats);
+
+/* Device workspace (basis pool, reduction scratch) is kept per thread
+   between solves and reused when large enough; this frees it. */
+void trlx_release_workspace(void);
 
 /* Version string of the library. */
 const char *trlx_version(void);

@@ -22,7 +22,7 @@ class TrlxStats(C.Structure):
         ("kernel_launches", C.c_longlong), ("cgs_passes", c_int),
         ("host_syncs", c_int), ("max_true_residual", c_double),
         ("kernel_seconds", c_double * 8), ("kernel_bytes", c_double * 8),
-        ("kernel_count", C.c_longlong * 8),
+        ("kernel_count", C.c_longlong * 8), ("seconds_setup", c_double),
     ]
 
     KERNEL_CLASSES = ("spmv", "project", "update", "normalize", "ritz", "dot", "other")
@@ -50,6 +50,8 @@ def _declare(lib):
     lib.trlx_get_last_stats.argtypes = [P(TrlxStats)]
     lib.trlx_get_last_stats.restype = None
     lib.trlx_version.restype = C.c_char_p
+    lib.trlx_release_workspace.argtypes = []
+    lib.trlx_release_workspace.restype = None
     for name in ("trlx_csr_create", "trlx_zcsr_create"):
         f = getattr(lib, name)
         f.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_int, P(c_void_p)]

@@ -270,6 +270,8 @@ void trlx_get_last_stats(trlx_stats *s) {
     if (s) *s = trlb::last_stats();
 }
 
+void trlx_release_workspace(void) { trlb::release_workspace(); }
+
 const char *trlx_version(void) { return "trlan-b200 0.1 (sm_100a)"; }
 
 void trl_print_info(trl_info *info, int mvflop) {

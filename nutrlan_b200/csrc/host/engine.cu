@@ -45,6 +45,79 @@ trlx_stats &last_stats() {
     return s;
 }
 
+// Device workspace kept between solves on the calling thread, so repeated
+// solves (benchmark steps, batched or seeded workflows) do not pay for
+// allocating and freeing the basis pool every call.  Released by
+// trlx_release_workspace() or at thread exit.
+struct Workspace {
+    void *pool = nullptr;
+    size_t pool_bytes = 0;
+    void *fbuf = nullptr;
+    size_t fbuf_bytes = 0;
+    void *small = nullptr;  // coefficients, scalars, Ritz matrix, column table
+    size_t small_bytes = 0;
+    void *partials = nullptr;
+    size_t partial_bytes = 0;
+    void *out = nullptr;  // staging of final eigenvectors for host evec
+    size_t out_bytes = 0;
+    unsigned *tickets = nullptr;
+    double *h_scal = nullptr;
+    int device = -1;
+    ~Workspace() { release(); }
+    void release() {
+        cudaFree(pool);
+        cudaFree(fbuf);
+        cudaFree(small);
+        cudaFree(partials);
+        cudaFree(out);
+        cudaFree(tickets);
+        cudaFreeHost(h_scal);
+        pool = fbuf = small = partials = out = nullptr;
+        out_bytes = 0;
+        tickets = nullptr;
+        h_scal = nullptr;
+        pool_bytes = fbuf_bytes = small_bytes = partial_bytes = 0;
+        device = -1;
+    }
+    // Grows buf to at least `bytes`; returns false on allocation failure.
+    static bool ensure(void **buf, size_t *have, size_t bytes) {
+        if (*have >= bytes && *buf) return true;
+        cudaFree(*buf);
+        *buf = nullptr;
+        *have = 0;
+        if (bytes == 0) return true;
+        if (cudaMalloc(buf, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            *buf = nullptr;
+            return false;
+        }
+        *have = bytes;
+        return true;
+    }
+};
+
+Workspace &workspace() {
+    static thread_local Workspace w;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (w.device != dev) {
+        w.release();
+        w.device = dev;
+    }
+    return w;
+}
+
+void release_workspace() { workspace().release(); }
+
+__global__ void k_zero_padding(char *pool, int nslots, size_t slot_bytes, size_t from_byte) {
+    const size_t tail = slot_bytes - from_byte;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)nslots * tail;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const size_t s = i / tail, o = i - s * tail;
+        pool[s * slot_bytes + from_byte + o] = 0;
+    }
+}
+
 Options options_from(const trlx_options *o) {
     Options r;
     if (!o) return r;
@@ -190,6 +263,7 @@ class Engine {
     int syncs_ = 0;
     double t_op_ = 0, t_orth_ = 0, t_res_ = 0;
     double fl_ = 0, fl_h_ = 0, fl_r_ = 0;  // flop counts (excluding matvec)
+    double setup_seconds_ = 0;
     struct ProfRec {
         cudaEvent_t a, b;
         int cls;
@@ -269,38 +343,57 @@ int Engine<T>::setup() {
         CK(cudaStreamCreate(&st_));  // blocking: ordered with legacy-stream user work
         own_stream_ = true;
     }
-    size_t pool_bytes = (size_t)P_ * n_pad_ * sizeof(T);
-    if (cudaMalloc(&pool_, pool_bytes) != cudaSuccess) {
-        cudaGetLastError();
+    const double t_alloc0 = now_s();
+    Workspace &ws = workspace();
+    const size_t pool_bytes = (size_t)P_ * n_pad_ * sizeof(T);
+    if (!Workspace::ensure(&ws.pool, &ws.pool_bytes, pool_bytes)) {
+        ws.release();
         std::fprintf(stderr, "TRLAN-B200: cannot allocate %.2f GB basis pool.\n", pool_bytes / 1e9);
         return -5;
     }
-    CK(cudaMemsetAsync(pool_, 0, pool_bytes, st_));
-    lslot_.resize(P_);
-    for (int i = 0; i < P_; ++i) lslot_[i] = i;
-    CK(cudaMalloc(&d_cols_, sizeof(T *) * P_));
-    h_cols_.resize(P_);
-    if (!kWide) {
-        for (auto &b : fbuf_) {
-            CK(cudaMalloc(&b, sizeof(C) * n_pad_));
-            CK(cudaMemsetAsync(b, 0, sizeof(C) * n_pad_, st_));
+    pool_ = static_cast<T *>(ws.pool);
+    // Rows >= nrow of every column must read as zero (kernels run over n_pad).
+    {
+        const size_t slot = (size_t)n_pad_ * sizeof(T), from = (size_t)nrow_ * sizeof(T);
+        if (slot > from) {
+            k_zero_padding<<<1024, 256, 0, st_>>>(reinterpret_cast<char *>(pool_), P_, slot, from);
+            count_launch();
         }
     }
+    lslot_.resize(P_);
+    for (int i = 0; i < P_; ++i) lslot_[i] = i;
+    h_cols_.resize(P_);
     if (!kWide) {
+        if (!Workspace::ensure(&ws.fbuf, &ws.fbuf_bytes, 3 * sizeof(C) * n_pad_)) return -5;
+        for (int k = 0; k < 3; ++k) fbuf_[k] = static_cast<C *>(ws.fbuf) + (size_t)k * n_pad_;
+        CK(cudaMemsetAsync(ws.fbuf, 0, 3 * sizeof(C) * n_pad_, st_));
         qa64_ = fbuf_[0];
         qb64_ = fbuf_[1];
         r64_ = fbuf_[2];
     }
-    CK(cudaMalloc(&d_coef_, sizeof(C) * P_));
-    CK(cudaMalloc(&d_scal_, sizeof(double) * kNumScal));
+    // Small buffers carved from one allocation (256-byte aligned pieces).
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t b_coef = al(sizeof(C) * P_), b_scal = al(sizeof(double) * kNumScal),
+                 b_Y = al(sizeof(double) * (size_t)maxlan_ * maxlan_), b_cols = al(sizeof(T *) * P_);
+    if (!Workspace::ensure(&ws.small, &ws.small_bytes, b_coef + b_scal + b_Y + b_cols)) return -5;
+    char *sp = static_cast<char *>(ws.small);
+    d_coef_ = reinterpret_cast<C *>(sp);
+    d_scal_ = reinterpret_cast<double *>(sp + b_coef);
+    d_Y_ = reinterpret_cast<double *>(sp + b_coef + b_scal);
+    d_cols_ = reinterpret_cast<T **>(sp + b_coef + b_scal + b_Y);
     CK(cudaMemsetAsync(d_scal_, 0, sizeof(double) * kNumScal, st_));
-    CK(cudaMallocHost(&h_scal_, sizeof(double) * kNumScal));
-    CK(cudaMalloc(&d_Y_, sizeof(double) * (size_t)maxlan_ * maxlan_));
+    if (!ws.h_scal) CK(cudaMallocHost(&ws.h_scal, sizeof(double) * kNumScal));
+    h_scal_ = ws.h_scal;
     scratch_.max_blocks = 148 * 8;
     scratch_.max_cols = P_;
-    CK(cudaMalloc(&scratch_.partials, (size_t)scratch_.max_blocks * (P_ + 2) * sizeof(zd)));
-    CK(cudaMalloc(&scratch_.tickets, sizeof(unsigned) * kNumTickets));
+    if (!Workspace::ensure(&ws.partials, &ws.partial_bytes,
+                           (size_t)scratch_.max_blocks * (P_ + 2) * sizeof(zd)))
+        return -5;
+    scratch_.partials = ws.partials;
+    if (!ws.tickets) CK(cudaMalloc(&ws.tickets, sizeof(unsigned) * kNumTickets));
+    scratch_.tickets = ws.tickets;
     CK(cudaMemsetAsync(scratch_.tickets, 0, sizeof(unsigned) * kNumTickets, st_));
+    setup_seconds_ = now_s() - t_alloc0;
     if (host_op_) {
         CK(cudaMallocHost(&hx_, sizeof(User) * (size_t)nrow_));
         CK(cudaMallocHost(&hy_, sizeof(User) * (size_t)nrow_));
@@ -321,18 +414,11 @@ int Engine<T>::setup() {
 
 template <class T>
 void Engine<T>::release() {
+    // Device buffers belong to the thread's workspace and stay allocated.
     cudaStreamSynchronize(st_);
-    cudaFree(pool_);
-    cudaFree(d_cols_);
-    for (auto b : fbuf_) cudaFree(b);
-    cudaFree(d_coef_);
-    cudaFree(d_scal_);
-    cudaFreeHost(h_scal_);
-    cudaFree(d_Y_);
-    cudaFree(scratch_.partials);
-    cudaFree(scratch_.tickets);
     cudaFreeHost(hx_);
     cudaFreeHost(hy_);
+    hx_ = hy_ = nullptr;
     for (auto e : ev_)
         if (e) cudaEventDestroy(e);
     for (auto e : evpool_) cudaEventDestroy(e);
@@ -707,7 +793,10 @@ int Engine<T>::final_vectors(int jnd, int kept) {
     if (user_dev_) {
         out = reinterpret_cast<C *>(evec_);
     } else {
-        CK(cudaMalloc(&tmp, sizeof(C) * (size_t)n_pad_ * std::max(kept, 1)));
+        Workspace &ws = workspace();
+        if (!Workspace::ensure(&ws.out, &ws.out_bytes, sizeof(C) * (size_t)n_pad_ * std::max(kept, 1)))
+            return -5;
+        tmp = static_cast<C *>(ws.out);
         out = tmp;
         ldo = n_pad_;
     }
@@ -726,7 +815,6 @@ int Engine<T>::final_vectors(int jnd, int kept) {
                            user_dev_ ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st_));
     }
     CK(cudaStreamSynchronize(st_));
-    cudaFree(tmp);
     return 0;
 }
 
@@ -987,6 +1075,7 @@ void Engine<T>::run() {
         s.kernel_count[k] = kc_[k];
     }
     s.basis_bytes = kb_[TRLX_K_PROJECT] + kb_[TRLX_K_UPDATE] + kb_[TRLX_K_RITZ];
+    s.seconds_setup = setup_seconds_;
 }
 
 template <class T>

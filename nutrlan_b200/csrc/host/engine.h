@@ -32,4 +32,7 @@ void clear_counter(trl_info *info, int nrow, int mev, int lde);
 
 bool is_device_pointer(const void *p);
 
+// Frees the calling thread's cached device workspace.
+void release_workspace();
+
 }  // namespace trlb

@@ -32,7 +32,12 @@ int num_sms() {
 }
 
 constexpr int kThreads = 256;
-constexpr int kProjColsPerWarp = 16;  // 8 warps x 16 = 128 columns per sweep
+// Columns per warp in the projection: 8 warps x 16 = 128 real columns per
+// sweep (8 for complex types, which carry twice the accumulator registers).
+template <class T>
+constexpr int proj_cpw() {
+    return std::is_same<typename Store<T>::C, double>::value ? 16 : 8;
+}
 
 enum TicketSlot { kTicketDot = 0, kTicketProject = 1, kTicketUpdate = 2 };
 
@@ -63,10 +68,13 @@ __global__ void __launch_bounds__(kThreads) k_dot(const C *__restrict__ x, const
 }
 
 // ---------------------------------------------------------------------------
-// Projection h = V^H r.  Block b owns rows [b*chunk, (b+1)*chunk); warp w of a
-// sweep owns columns c0 + w*CPW .. +CPW and keeps one FP64 accumulator per
-// column per lane across all the block's rows, so each basis element is
-// read exactly once and reduced with a single warp shuffle tree at the end.
+// Projection h = V^H r.  Block b owns rows [b*chunk, (b+1)*chunk).  Columns
+// are cut into groups of CPW; a sweep gives each of the 8 warps one group
+// when there are at least 8 groups, otherwise the warps of a group split the
+// block's rows between them (so a short basis still keeps every warp
+// streaming).  Every lane keeps one FP64 accumulator per column across its
+// rows, each basis element is read once, and partial sums are combined in a
+// fixed order (lanes by shuffle tree, warps of a group in warp order).
 template <class T, int CPW>
 __global__ void __launch_bounds__(kThreads)
     k_project(T *const *__restrict__ cols, int m, long n_pad, long chunk,
@@ -76,40 +84,51 @@ __global__ void __launch_bounds__(kThreads)
     using S = Store<T>;
     using C = typename S::C;
     constexpr int R = S::R;
+    constexpr int W = kThreads / 32;
+    __shared__ C red_c[W][CPW];
+    __shared__ double red_r2[W];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long row0 = (long)blockIdx.x * chunk;
     const long row1 = min(n_pad, row0 + chunk);
     const double alpha = rec.on ? *rec.alpha : 0.0;
+    const int ngroups = (m + CPW - 1) / CPW;
     double r2acc = 0.0;
-    for (int c0 = 0; c0 < m; c0 += (kThreads / 32) * CPW) {
-        const int cb = c0 + warp * CPW;
+    for (int g0 = 0; g0 < ngroups; g0 += W) {
+        const int G = min(W, ngroups - g0);
+        const int wpg = W / G;
+        const int grp = warp / wpg, slice = warp - grp * wpg;
+        const bool active = grp < G;
+        const int cb = (g0 + grp) * CPW;
         const T *p[CPW];
 #pragma unroll
-        for (int k = 0; k < CPW; ++k) p[k] = (cb + k < m) ? cols[cb + k] : nullptr;
+        for (int k = 0; k < CPW; ++k) p[k] = (active && cb + k < m) ? cols[cb + k] : nullptr;
         C acc[CPW];
 #pragma unroll
         for (int k = 0; k < CPW; ++k) acc[k] = czero(C());
-        for (long i = row0 + lane * R; i < row1; i += 32 * R) {
-            C rv[R];
-            load_c<R>(r + i, rv);
-            if (rec.on) {
-                C xv[R], xpv[R];
-                load_c<R>(rec.x + i, xv);
-                load_c<R>(rec.xp + i, xpv);
+        const bool count_r2 = (g0 == 0 && grp == 0);
+        if (active) {
+            for (long i = row0 + (long)(slice * 32 + lane) * R; i < row1; i += (long)wpg * 32 * R) {
+                C rv[R];
+                load_c<R>(r + i, rv);
+                if (rec.on) {
+                    C xv[R], xpv[R];
+                    load_c<R>(rec.x + i, xv);
+                    load_c<R>(rec.xp + i, xpv);
 #pragma unroll
-                for (int q = 0; q < R; ++q) rv[q] = rv[q] - alpha * xv[q] - rec.beta * xpv[q];
-            }
-            if (c0 == 0 && warp == 0) {
+                    for (int q = 0; q < R; ++q) rv[q] = rv[q] - alpha * xv[q] - rec.beta * xpv[q];
+                }
+                if (count_r2) {
 #pragma unroll
-                for (int q = 0; q < R; ++q) r2acc += abs2(rv[q]);
-            }
+                    for (int q = 0; q < R; ++q) r2acc += abs2(rv[q]);
+                }
 #pragma unroll
-            for (int k = 0; k < CPW; ++k) {
-                if (p[k]) {
-                    C v[R];
-                    S::load(p[k] + i, v);
+                for (int k = 0; k < CPW; ++k) {
+                    if (p[k]) {
+                        C v[R];
+                        S::load(p[k] + i, v);
 #pragma unroll
-                    for (int q = 0; q < R; ++q) fma_conj(acc[k], v[q], rv[q]);
+                        for (int q = 0; q < R; ++q) fma_conj(acc[k], v[q], rv[q]);
+                    }
                 }
             }
         }
@@ -117,13 +136,28 @@ __global__ void __launch_bounds__(kThreads)
         for (int k = 0; k < CPW; ++k) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) acc[k] = acc[k] + shfl_down(acc[k], o);
-            if (lane == 0 && cb + k < m) part[(long)blockIdx.x * m + cb + k] = acc[k];
+            if (lane == 0) red_c[warp][k] = acc[k];
         }
+        __syncthreads();
+        if (threadIdx.x < G * CPW) {
+            const int gg = threadIdx.x / CPW, k = threadIdx.x - gg * CPW;
+            const int c = (g0 + gg) * CPW + k;
+            if (c < m) {
+                C s = czero(C());
+                for (int sl = 0; sl < wpg; ++sl) s = s + red_c[gg * wpg + sl][k];
+                part[(long)blockIdx.x * m + c] = s;
+            }
+        }
+        __syncthreads();
     }
-    if (warp == 0) {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) r2acc += __shfl_down_sync(0xffffffffu, r2acc, o);
-        if (lane == 0) part_r2[blockIdx.x] = r2acc;
+    for (int o = 16; o > 0; o >>= 1) r2acc += __shfl_down_sync(0xffffffffu, r2acc, o);
+    if (lane == 0) red_r2[warp] = r2acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < W; ++w) s += red_r2[w];
+        part_r2[blockIdx.x] = s;
     }
     if (last_block_arrived(ticket)) {
         __shared__ double red[32];
@@ -381,7 +415,7 @@ void launch_project(T *const *cols, int m, long n_pad, const typename Store<T>::
     nb = (int)((n_pad + chunk - 1) / chunk);
     C *part = reinterpret_cast<C *>(s.partials);
     double *part_r2 = reinterpret_cast<double *>(part + (long)nb * m);
-    k_project<T, kProjColsPerWarp><<<nb, kThreads, 0, st>>>(
+    k_project<T, proj_cpw<T>()><<<nb, kThreads, 0, st>>>(
         cols, m, n_pad, chunk, r, rec, part, part_r2, s.tickets + kTicketProject, h, out2);
 }
 

@@ -81,6 +81,59 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+// CSR in row tiles of kThreads rows: the tile's entries are processed in
+// chunks of kChunk; all threads compute val*x[col] products with coalesced
+// loads (kChunk/kThreads independent loads in flight per thread) into shared
+// memory, then each thread sums its own row's products in index order.
+constexpr int kChunk = 2048;
+
+template <class V>
+__global__ void __launch_bounds__(kThreads)
+    k_csr_stream(int nrow, long n_pad, const long long *__restrict__ rp, const int *__restrict__ ci,
+                 const V *__restrict__ va, const V *__restrict__ x, V *__restrict__ y, double *part,
+                 unsigned *ticket, double *alpha_out) {
+    __shared__ V prod[kChunk];
+    __shared__ long long rps[kThreads + 1];
+    const int t = threadIdx.x;
+    double aacc = 0.0;
+    const long ntiles = n_pad / kThreads;
+    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long r0 = tile * kThreads;
+        for (int k = t; k <= kThreads; k += kThreads) rps[k] = rp[(r0 + k < nrow) ? (r0 + k) : (long)nrow];
+        __syncthreads();
+        const long long eb = rps[0], ee = rps[kThreads];
+        const long long mb = rps[t], me = rps[t + 1];
+        V acc = czero(V());
+        for (long long c0 = eb; c0 < ee; c0 += kChunk) {
+            const long long c1 = min(ee, c0 + (long long)kChunk);
+            for (long long e = c0 + t; e < c1; e += kThreads) prod[e - c0] = mulx(ld_val(va + e), ldg_c(x + ci[e]));
+            __syncthreads();
+            const long long lo = max(mb, c0), hi = min(me, c1);
+            for (long long e = lo; e < hi; ++e) acc = acc + prod[e - c0];
+            __syncthreads();
+        }
+        const long row = r0 + t;
+        y[row] = acc;  // rows in [nrow, n_pad) have no entries: zero
+        if (alpha_out) {
+            V tt = czero(V());
+            fma_conj(tt, ldg_c(x + row), acc);
+            aacc += real_part(tt);
+        }
+    }
+    if (!alpha_out) return;
+    __shared__ double red[32];
+    double s = block_sum(aacc, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+    if (last_block_arrived(ticket)) {
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (unsigned b = 0; b < gridDim.x; ++b) tot += __ldcg(part + b);
+            *alpha_out = tot;
+            *ticket = 0;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kThreads)
     k_sell(int nrow, long n_pad, int nslice, const long long *__restrict__ sp,
            const int *__restrict__ ci, const double *__restrict__ va, const int *__restrict__ perm,
@@ -122,9 +175,13 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 int spmv_blocks(long work_items, int per_block) {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
     long need = (work_items + per_block - 1) / per_block;
     return (int)std::max<long>(1, std::min<long>(need, (long)sms * 8));
 }
@@ -136,6 +193,14 @@ void spmv_fused_real(const trlx_operator *A, const double *x, double *y, long n_
     double *part = s ? reinterpret_cast<double *>(s->partials) : nullptr;
     unsigned *tk = s ? s->tickets + kTicketSpmv : nullptr;
     if (A->kind == 0) {
+        if (n_pad % kThreads == 0) {
+            int nb = spmv_blocks(n_pad, kThreads);
+            if (s) nb = std::min(nb, s->max_blocks);
+            k_csr_stream<double><<<nb, kThreads, 0, st>>>(A->nrow, n_pad, A->row_ptr, A->col,
+                                                          static_cast<const double *>(A->val), x, y, part, tk,
+                                                          alpha_out);
+            return;
+        }
         int nb = spmv_blocks(n_pad, kThreads / kGroup);
         if (s) nb = std::min(nb, s->max_blocks);
         k_csr<double><<<nb, kThreads, 0, st>>>(A->nrow, n_pad, A->row_ptr, A->col,
@@ -154,6 +219,13 @@ void spmv_fused_cplx(const trlx_operator *A, const zd *x, zd *y, long n_pad, dou
                      Scratch *s, cudaStream_t st) {
     double *part = s ? reinterpret_cast<double *>(s->partials) : nullptr;
     unsigned *tk = s ? s->tickets + kTicketSpmv : nullptr;
+    if (n_pad % kThreads == 0) {
+        int nb = spmv_blocks(n_pad, kThreads);
+        if (s) nb = std::min(nb, s->max_blocks);
+        k_csr_stream<zd><<<nb, kThreads, 0, st>>>(A->nrow, n_pad, A->row_ptr, A->col,
+                                                  static_cast<const zd *>(A->val), x, y, part, tk, alpha_out);
+        return;
+    }
     int nb = spmv_blocks(n_pad, kThreads / kGroup);
     if (s) nb = std::min(nb, s->max_blocks);
     k_csr<zd><<<nb, kThreads, 0, st>>>(A->nrow, n_pad, A->row_ptr, A->col,

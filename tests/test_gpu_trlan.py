@@ -68,13 +68,58 @@ def test_laplace_128_builtin_operator_matches_oracle(lap128, fmt):
     if o is not None:
         assert o["info"].stat == 0
         ref_vals = o["eval"][: o["info"].nec]
-        _match(got, ref_vals)
-        np.testing.assert_allclose(_distinct(got)[:5], _distinct(ref_vals)[:5], rtol=REL)
-        # Same algorithm: matvec counts within a few percent of the reference.
-        assert abs(r.info.matvec - o["info"].matvec) <= 0.1 * o["info"].matvec + 16
+        # The 128^2 Laplacian has exact degeneracies lambda(i,j) = lambda(j,i):
+        # whether single-vector Lanczos also converges the partner copies
+        # depends on rounding (the reference finds them with multi-threaded
+        # BLAS and misses them single-threaded), so compare distinct values.
+        dg, dr = _distinct(got), _distinct(ref_vals)
+        k = min(len(dg), len(dr))
+        np.testing.assert_allclose(dg[:k], dr[:k], rtol=REL)
+        _match(dg[:k], exact)
 
 
-@pytest.mark.parametrize("restart", [1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.fixture(scope="module")
+def anderson16():
+    A = ops.anderson_3d(16, W=4.0, seed=11)
+    return A, ops.start_vector(A.n), np.linalg.eigvalsh(A.to_scipy().toarray())
+
+
+@pytest.mark.parametrize("restart", [1, 7])
+@pytest.mark.parametrize("fmt", ["csr", "sell"])
+def test_nondegenerate_matvec_count_parity(anderson16, restart, fmt):
+    """Without exact degeneracy the engine takes the reference's path: same
+    converged set, matvec and restart counts within a few percent (rounding
+    differs between the GPU reductions and BLAS)."""
+    A, x0, dense = anderson16
+    with DeviceOperator(A, fmt=fmt) as op:
+        r = solve(op, ned=8, maxlan=40, restart=restart, maxmv=100000, start=x0)
+    assert r.stat == 0 and r.nec >= 8
+    np.testing.assert_allclose(r.eval[:8], dense[:8], rtol=REL, atol=REL)
+    o = _ref_run(A, x0, 8, 40, restart)
+    if o is not None:
+        np.testing.assert_allclose(r.eval[:8], o["eval"][:8], rtol=REL, atol=REL)
+        assert abs(r.info.matvec - o["info"].matvec) <= 0.05 * o["info"].matvec + 8
+        assert abs(r.info.nloop - o["info"].nloop) <= 0.1 * o["info"].nloop + 2
+
+
+def test_scheme8_trajectory_matches_oracle(lap128):
+    """Scheme 8 with the default rfact shrinks the basis to ned (klan = 10)
+    and then crawls, in the reference as here; over a bounded run the two
+    trajectories coincide: same restarts, basis size, converged count and
+    Ritz values."""
+    A, x0, exact = lap128
+    with DeviceOperator(A) as op:
+        r = solve(op, ned=10, maxlan=64, restart=8, maxmv=1600, start=x0)
+    assert r.stat == 0
+    if ref.available():
+        o = ref.trlan(A.matvec, A.n, ned=10, maxlan=64, restart=8, start=x0, maxmv=1600)
+        i, j = r.info, o["info"]
+        assert (i.nloop, i.klan, i.nec, i.locked) == (j.nloop, j.klan, j.nec, j.locked)
+        assert abs(i.matvec - j.matvec) <= 2
+        np.testing.assert_allclose(r.eval[:4], o["eval"][:4], rtol=1e-9)
+
+
+@pytest.mark.parametrize("restart", [1, 2, 3, 4, 5, 6, 7])
 def test_restart_schemes_match_oracle(lap128, restart):
     A, x0, exact = lap128
     with DeviceOperator(A) as op:
@@ -83,7 +128,9 @@ def test_restart_schemes_match_oracle(lap128, restart):
     _match(r.eval[: r.nec], exact)
     o = _ref_run(A, x0, 10, 64, restart)
     if o is not None:
-        _match(r.eval[: r.nec], o["eval"][: o["info"].nec])
+        dg, dr = _distinct(r.eval[: r.nec]), _distinct(o["eval"][: o["info"].nec])
+        k = min(len(dg), len(dr))
+        np.testing.assert_allclose(dg[:k], dr[:k], rtol=REL)
 
 
 def test_largest_eigenvalues(lap128):
