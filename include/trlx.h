@@ -56,6 +56,25 @@ void trlx_zmatvec(const int nrow, const int ncol, const trl_dcomplex *x,
                   void *mvparam);
 
 /* ---------------------------------------------------------------------------
+ * Kernel-level entry points (device pointers, column-major blocks).
+ * ------------------------------------------------------------------------- */
+/* Gram-Schmidt projection wrk = [v1 v2]^T rr over two blocks of basis
+   columns (v1: m1 columns, leading dimension ld1; v2: m2 columns, ld2):
+   the counterpart of the reference's trl_g_dot_ (SRC/trl_comm_none.c:238),
+   which the MPI build also uses as the allreduce point.  All pointers are
+   device memory; the work is queued on `stream` (a cudaStream_t, NULL for
+   the legacy default stream) and wrk is valid once that stream reaches it.
+   Deterministic (fixed summation order).  Returns 0, -201 if ld1 or ld2 is
+   smaller than nrow (the reference aborts there), -1 on invalid arguments,
+   -5 if the reduction scratch cannot be allocated. */
+int trlx_g_dot(int nrow, const double *v1, int ld1, int m1, const double *v2,
+               int ld2, int m2, const double *rr, double *wrk, void *stream);
+/* Complex twin: wrk = [v1 v2]^H rr (ztrl_g_dot_, SRC/ztrl_comm_none.c:16). */
+int trlx_zg_dot(int nrow, const trl_dcomplex *v1, int ld1, int m1,
+                const trl_dcomplex *v2, int ld2, int m2,
+                const trl_dcomplex *rr, trl_dcomplex *wrk, void *stream);
+
+/* ---------------------------------------------------------------------------
  * Solver options.
  * ------------------------------------------------------------------------- */
 typedef struct {

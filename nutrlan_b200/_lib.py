@@ -50,6 +50,11 @@ def _declare(lib):
     lib.trlx_get_last_stats.argtypes = [P(TrlxStats)]
     lib.trlx_get_last_stats.restype = None
     lib.trlx_version.restype = C.c_char_p
+    for name in ("trlx_g_dot", "trlx_zg_dot"):
+        f = getattr(lib, name)
+        f.argtypes = [c_int, c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p, c_void_p,
+                      c_void_p]
+        f.restype = c_int
     lib.trlx_release_workspace.argtypes = []
     lib.trlx_release_workspace.restype = None
     for name in ("trlx_csr_create", "trlx_zcsr_create"):

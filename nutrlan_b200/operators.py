@@ -54,8 +54,11 @@ class CSR:
 
     def matvec(self, x):
         """y = A x (numpy, for the CPU checks)."""
-        prod = self.val * x[self.col]
-        return np.add.reduceat(prod, self.row_ptr[:-1]) if self.nnz else np.zeros_like(x)
+        out = np.zeros(self.n, dtype=np.result_type(self.val, x))
+        nz = np.diff(self.row_ptr) > 0
+        if nz.any():
+            out[nz] = np.add.reduceat(self.val * x[self.col], self.row_ptr[:-1][nz])
+        return out
 
     def to_scipy(self):
         import scipy.sparse as sp
