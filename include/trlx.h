@@ -74,6 +74,24 @@ int trlx_zg_dot(int nrow, const trl_dcomplex *v1, int ld1, int m1,
                 const trl_dcomplex *v2, int ld2, int m2,
                 const trl_dcomplex *rr, trl_dcomplex *wrk, void *stream);
 
+/* Allocation-free variant of trlx_g_dot, for callers that must not allocate
+   device memory (an application-wide memory budget or caching allocator
+   owns the GPU, or the call happens inside an operator callback or another
+   hot loop where cudaMalloc could synchronize the device).  No counterpart
+   in the reference.  Same arguments, result and error codes as trlx_g_dot;
+   it calls no cudaMalloc/cudaFree.  Its reduction scratch is a fixed
+   592 KiB array inside the library, held by every GPU that loads the library
+   until the process exits; at most TRLX_G_DOT_NOALLOC_MAX_COLS columns
+   (m1 + m2), larger requests return -7.  The first call on a device looks
+   up that array's device address (cudaGetSymbolAddress) and caches it, so
+   make the first call on each device before any stream capture.  All calls
+   share the array: calls whose work overlaps on the GPU (different streams
+   or threads on one device) race and must be serialised. */
+#define TRLX_G_DOT_NOALLOC_MAX_COLS 512
+int trlx_g_dot_noalloc(int nrow, const double *v1, int ld1, int m1,
+                       const double *v2, int ld2, int m2, const double *rr,
+                       double *wrk, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Solver options.
  * ------------------------------------------------------------------------- */

@@ -50,7 +50,7 @@ def _declare(lib):
     lib.trlx_get_last_stats.argtypes = [P(TrlxStats)]
     lib.trlx_get_last_stats.restype = None
     lib.trlx_version.restype = C.c_char_p
-    for name in ("trlx_g_dot", "trlx_zg_dot"):
+    for name in ("trlx_g_dot", "trlx_zg_dot", "trlx_g_dot_noalloc"):
         f = getattr(lib, name)
         f.argtypes = [c_int, c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p, c_void_p,
                       c_void_p]
