@@ -170,11 +170,16 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="anderson256")
     ap.add_argument("--basis-bits", type=int, choices=[64, 32], default=64)
-    ap.add_argument("--format", choices=["csr", "sell"], default="csr")
+    ap.add_argument("--format", choices=["csr", "sell"], default="sell")
     ap.add_argument("--cpu-sample", type=int, default=32,
                     help="Lanczos steps in the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the secondary timings (other format, 32-bit basis)")
+    ap.add_argument("--full-solve", action="store_true",
+                    help="also run one solve to convergence (time to solution)")
+    ap.add_argument("--solve-maxmv", type=int, default=20000)
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world, rank, local, pg = dist_setup(args)
@@ -348,6 +353,78 @@ def main():
                "h2d_bytes_per_step": int(op_obj_bytes + 8 * n),
                "d2h_bytes_per_step": int(8 * n * mev + 8 * mev)}
 
+    # ---- secondary timings: the other configured format, 32-bit basis -----
+    variants = {}
+    if not args.no_variants:
+        def time_variant(fmt, bits):
+            vop = op if fmt == args.format else DeviceOperator(A, fmt=fmt)
+            vopts = TrlxOptions()
+            lib.trlx_default_options(C.byref(vopts))
+            vopts.basis_bits = bits
+            inf = TrlInfo()
+
+            def call():
+                lib.trl_init_info(C.byref(inf), n, maxlan, -1, ned, tol, 1, steps_per_call, None)
+                inf.mvparam = vop.handle.value
+                lib.trl_set_iguess(C.byref(inf), 0, 1, 0, None)
+                evec[0].copy_(x0_dev)
+                lib.trlx_trlan(vop.applier, None, C.byref(inf), n, mev, eval_.ctypes.data, evec.data_ptr(), n,
+                               mev, wrk.ctypes.data, C.byref(vopts))
+                return inf.matvec
+
+            call()
+            torch.cuda.synchronize()
+            barrier(pg)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            mv = sum(call() for _ in range(args.steps))
+            e1.record()
+            torch.cuda.synchronize()
+            dt = reduce_max(pg, e0.elapsed_time(e1) * 1e-3, dev)
+            if vop is not op:
+                vop.close()
+            return reduce_max(pg, mv, dev) * world / dt
+
+        other = "csr" if args.format == "sell" else "sell"
+        variants[f"{other}_fp{args.basis_bits}"] = time_variant(other, args.basis_bits)
+        alt_bits = 32 if args.basis_bits == 64 else 64
+        variants[f"{args.format}_fp{alt_bits}"] = time_variant(args.format, alt_bits)
+
+    solve_rec = None
+    if args.full_solve and rank == 0:
+        from nutrlan_b200 import residual_norms
+        solve_rec = {}
+        for bits in (64, 32):
+            inf = TrlInfo()
+            lib.trl_init_info(C.byref(inf), n, maxlan, -1, ned, tol, 1, args.solve_maxmv, None)
+            inf.mvparam = op.handle.value
+            lib.trl_set_iguess(C.byref(inf), 0, 1, 0, None)
+            evec[0].copy_(x0_dev)
+            sopts = TrlxOptions()
+            lib.trlx_default_options(C.byref(sopts))
+            sopts.basis_bits = bits
+            torch.cuda.synchronize()
+            ts = time.perf_counter()
+            lib.trlx_trlan(op.applier, None, C.byref(inf), n, mev, eval_.ctypes.data, evec.data_ptr(), n, mev,
+                           wrk.ctypes.data, C.byref(sopts))
+            torch.cuda.synchronize()
+            ts = time.perf_counter() - ts
+            k = max(inf.nec, 1)
+            res = residual_norms(op, eval_[:k], evec[:k])
+            anrm = inf.anrm
+            solve_rec[f"fp{bits}"] = {
+                "seconds": ts, "matvecs": inf.matvec, "restarts": inf.nloop, "nec": inf.nec,
+                "stat": inf.stat, "restart_scheme": 1,
+                "max_residual_estimate": float(np.max(wrk[:k])),
+                "max_true_residual": float(res.max()), "anrm": anrm,
+                "max_true_residual_rel": float(res.max() / anrm),
+                "eval_min": float(eval_[0]), "eval_max_converged": float(eval_[k - 1]),
+                "evals": [float(v) for v in eval_[:k]]}
+        if "fp64" in solve_rec and "fp32" in solve_rec:
+            a, b = np.array(solve_rec["fp64"]["evals"]), np.array(solve_rec["fp32"]["evals"])
+            kk = min(len(a), len(b))
+            solve_rec["fp32_vs_fp64_max_rel_eval_diff"] = float(np.max(np.abs(a[:kk] - b[:kk]) / np.abs(a[:kk])))
+
     op.close()
     del evec
     torch.cuda.empty_cache()
@@ -371,7 +448,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded Anderson potential and start vector)", "config": config,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-                "clocks": clocks, "host_wall_s": wall,
+                "clocks": clocks, "host_wall_s": wall, "variants": variants, "solve": solve_rec,
                 "matvecs_per_call": int(matvecs // max(args.steps, 1))}
         print(json.dumps(line), flush=True)
     if pg is not None:

@@ -8,6 +8,6 @@ device operator with the basis resident in GPU memory, and
 """
 from ._abi import TrlInfo, TrlDComplex, MATVEC, USER_ORTHO  # noqa: F401
 from ._lib import load, LIB_PATH, TrlxStats, TrlxOptions  # noqa: F401
-from .solver import DeviceOperator, solve, SolveResult  # noqa: F401
+from .solver import DeviceOperator, solve, SolveResult, residual_norms  # noqa: F401
 
 __version__ = "0.1.0"

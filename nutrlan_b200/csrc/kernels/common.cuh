@@ -185,6 +185,49 @@ __device__ __forceinline__ bool last_block_arrived(unsigned *ticket) {
     return is_last;
 }
 
+// Final step of a grid reduction, run by the last block: out[c] =
+// sum_b part[b * m + c] for c < m, in a fixed order.  Each column gets
+// tpc = max(1, blockDim / m) threads (power of two); thread j of a column
+// sums blocks b = j, j + tpc, ... with 8 independent accumulators (8 loads
+// in flight), and the tpc partial sums are then added in thread order.
+// Returns, in thread 0, sum_c |out[c]|^2.  smem must hold blockDim.x values.
+template <class C>
+__device__ inline double reduce_columns(const C *part, int nb, int m, C *out, C *smem) {
+    int tpc = 1;
+    while (tpc * 2 * m <= (int)blockDim.x) tpc *= 2;
+    const int groups = blockDim.x / tpc;  // columns handled per round
+    double norm2 = 0.0;
+    for (int c0 = 0; c0 < m; c0 += groups) {
+        const int c = c0 + (int)threadIdx.x / tpc;
+        const int j = threadIdx.x % tpc;
+        C acc[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) acc[u] = czero(C());
+        if (c < m) {
+            int b = j;
+            for (; b + 7 * tpc < nb; b += 8 * tpc) {
+#pragma unroll
+                for (int u = 0; u < 8; ++u) acc[u] = acc[u] + ldcg(part + (long)(b + u * tpc) * m + c);
+            }
+            for (; b < nb; b += tpc) acc[0] = acc[0] + ldcg(part + (long)b * m + c);
+        }
+        smem[threadIdx.x] = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+        __syncthreads();
+        if (j == 0 && c < m) {
+            C s = smem[threadIdx.x];
+            for (int q = 1; q < tpc; ++q) s = s + smem[threadIdx.x + q];
+            out[c] = s;
+            smem[threadIdx.x] = s;  // keep for the norm below
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int g = 0; g < groups && c0 + g < m; ++g) norm2 += abs2(smem[g * tpc]);
+        }
+        __syncthreads();
+    }
+    return norm2;
+}
+
 // Counter-based uniform [0,1) generator (splitmix64 finaliser).
 __host__ __device__ inline double uniform01(uint64_t seed, uint64_t i) {
     uint64_t z = seed + 0x9E3779B97F4A7C15ull * (i + 1);

@@ -89,12 +89,8 @@ __global__ void __launch_bounds__(kThreads)
         __syncthreads();
     }
     if (last_block_arrived(ticket)) {
-        const int nb = gridDim.x;
-        for (int c = threadIdx.x; c < m; c += blockDim.x) {
-            C s = czero(C());
-            for (int b = 0; b < nb; ++b) s = s + ldcg(part + (long)b * m + c);
-            wrk[c] = s;
-        }
+        __shared__ C red_cols[kThreads];
+        reduce_columns(part, (int)gridDim.x, m, wrk, red_cols);
         if (threadIdx.x == 0) *ticket = 0;
     }
 }

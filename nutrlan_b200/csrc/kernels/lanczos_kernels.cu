@@ -11,6 +11,7 @@
 // bitwise reproducible run to run.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <type_traits>
 
 #include "lanczos_kernels.h"
@@ -75,8 +76,18 @@ __global__ void __launch_bounds__(kThreads) k_dot(const C *__restrict__ x, const
 // streaming).  Every lane keeps one FP64 accumulator per column across its
 // rows, each basis element is read once, and partial sums are combined in a
 // fixed order (lanes by shuffle tree, warps of a group in warp order).
+// Resident blocks per SM the projection is compiled for: as many as the
+// accumulators (CPW per lane, complex counts double) and the per-lane loads
+// (R elements per column) leave registers for, without spilling.
 template <class T, int CPW>
-__global__ void __launch_bounds__(kThreads)
+constexpr int proj_min_blocks() {
+    return !std::is_same<typename Store<T>::C, double>::value
+               ? 2
+               : (Store<T>::R == 4 ? (CPW >= 12 ? 2 : 3) : (CPW >= 16 ? 2 : (CPW >= 12 ? 3 : 4)));
+}
+
+template <class T, int CPW>
+__global__ void __launch_bounds__(kThreads, (proj_min_blocks<T, CPW>()))
     k_project(T *const *__restrict__ cols, int m, long n_pad, long chunk,
               const typename Store<T>::C *__restrict__ r, Recur<typename Store<T>::C> rec,
               typename Store<T>::C *part, double *part_r2, unsigned *ticket,
@@ -160,16 +171,9 @@ __global__ void __launch_bounds__(kThreads)
         part_r2[blockIdx.x] = s;
     }
     if (last_block_arrived(ticket)) {
-        __shared__ double red[32];
+        __shared__ C red_cols[kThreads];
         const int nb = gridDim.x;
-        double h2loc = 0.0;
-        for (int c = threadIdx.x; c < m; c += blockDim.x) {
-            C s = czero(C());
-            for (int b = 0; b < nb; ++b) s = s + ldcg(part + (long)b * m + c);
-            h[c] = s;
-            h2loc += abs2(s);
-        }
-        double h2 = block_sum(h2loc, red);
+        const double h2 = reduce_columns(part, nb, m, h, red_cols);
         if (threadIdx.x == 0) {
             double r2 = 0.0;
             for (int b = 0; b < nb; ++b) r2 += __ldcg(part_r2 + b);
@@ -269,70 +273,96 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------
-// out[:,k] = sum_c in[:,c] Y[c,k]: 64x64 output tiles, K in steps of 16,
-// each thread a 4x4 register tile (rows ty+16q, columns tx+16p).
-constexpr int kBM = 64, kBN = 64, kBK = 16;
+// out[:,k] = sum_c in[:,c] Y[c,k] (FP64 accumulate): output tiles of
+// 128 rows x BN columns, K in steps of 16 staged through shared memory with
+// the next K-slice prefetched into registers while the current one is used.
+// Thread (tx, ty) owns rows ty + 16 q (q < 8) and columns tx + TX p
+// (p < BN / TX), TX = 16 for BN = 64 and 8 for BN = 32, so a restart that
+// keeps <= 32 vectors does not compute a half-empty tile.
+constexpr int kBM = 128, kBK = 16;
 
-template <class T, class OutT>
+template <int BN>
+struct RitzShape {
+    static constexpr int TX = BN == 64 ? 16 : 8;      // threads along columns
+    static constexpr int TY = kThreads / TX;          // threads along rows
+    static constexpr int QR = kBM / TY;               // rows per thread
+    static constexpr int PC = BN / TX;                // columns per thread
+};
+
+template <class T, class OutT, int BN>
 __global__ void __launch_bounds__(kThreads)
     k_ritz(T *const *__restrict__ in_cols, int jml, const double *__restrict__ Y, int ldy, int kept,
            OutT *const *out_cols, OutT *out, long ldo, long n_valid) {
     using S = Store<T>;
     using C = typename S::C;
+    using Sh = RitzShape<BN>;
     __shared__ C As[kBK][kBM + 1];
-    __shared__ double Bs[kBK][kBN + 1];
-    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+    __shared__ double Bs[kBK][BN + 1];
+    const int t = threadIdx.x, tx = t % Sh::TX, ty = t / Sh::TX;
     const long i0 = (long)blockIdx.x * kBM;
-    const int k0 = blockIdx.y * kBN;
-    C acc[4][4];
+    const int k0 = blockIdx.y * BN;
+    // A loads: 16 columns x 128 rows = 2048 elements, 8 per thread:
+    // column kk = t / 16, rows (t % 16) * 8 .. +8.
+    const int a_kk = t >> 4, a_rr = (t & 15) * 8;
+    C areg[8];
+    double breg[BN * kBK / kThreads];
+    auto load_tiles = [&](int c0) {
+        const int c = c0 + a_kk;
+        if (c < jml) {
+            const T *col = in_cols[c] + i0 + a_rr;
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+            for (int q = 0; q < 8; ++q) areg[q] = S::to_c(col[q]);
+        } else {
 #pragma unroll
-        for (int p = 0; p < 4; ++p) acc[q][p] = czero(C());
-    for (int c0 = 0; c0 < jml; c0 += kBK) {
-        {  // A tile: column kk = t/16, rows (t%16)*4 .. +4
-            const int kk = t >> 4, rr = (t & 15) * 4;
-            const int c = c0 + kk;
-            if (c < jml) {
-                const T *col = in_cols[c] + i0 + rr;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) As[kk][rr + q] = S::to_c(col[q]);
-            } else {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) As[kk][rr + q] = czero(C());
-            }
+            for (int q = 0; q < 8; ++q) areg[q] = czero(C());
         }
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {  // B tile
+        for (int e = 0; e < BN * kBK / kThreads; ++e) {
             const int idx = t + e * kThreads;
-            const int kk = idx / kBN, kc = idx % kBN;
-            const int c = c0 + kk, k = k0 + kc;
-            Bs[kk][kc] = (c < jml && k < kept) ? Y[(long)c + (long)k * ldy] : 0.0;
+            const int kk = idx / BN, kc = idx % BN;
+            const int cc = c0 + kk, k = k0 + kc;
+            breg[e] = (cc < jml && k < kept) ? Y[(long)cc + (long)k * ldy] : 0.0;
+        }
+    };
+    C acc[Sh::QR][Sh::PC];
+#pragma unroll
+    for (int q = 0; q < Sh::QR; ++q)
+#pragma unroll
+        for (int p = 0; p < Sh::PC; ++p) acc[q][p] = czero(C());
+    load_tiles(0);
+    for (int c0 = 0; c0 < jml; c0 += kBK) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) As[a_kk][a_rr + q] = areg[q];
+#pragma unroll
+        for (int e = 0; e < BN * kBK / kThreads; ++e) {
+            const int idx = t + e * kThreads;
+            Bs[idx / BN][idx % BN] = breg[e];
         }
         __syncthreads();
+        if (c0 + kBK < jml) load_tiles(c0 + kBK);
 #pragma unroll
         for (int kk = 0; kk < kBK; ++kk) {
-            C a[4];
-            double b[4];
+            C a[Sh::QR];
+            double b[Sh::PC];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) a[q] = As[kk][ty + 16 * q];
+            for (int q = 0; q < Sh::QR; ++q) a[q] = As[kk][ty + Sh::TY * q];
 #pragma unroll
-            for (int p = 0; p < 4; ++p) b[p] = Bs[kk][tx + 16 * p];
+            for (int p = 0; p < Sh::PC; ++p) b[p] = Bs[kk][tx + Sh::TX * p];
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
+            for (int q = 0; q < Sh::QR; ++q)
 #pragma unroll
-                for (int p = 0; p < 4; ++p) fma_real(acc[q][p], a[q], b[p]);
+                for (int p = 0; p < Sh::PC; ++p) fma_real(acc[q][p], a[q], b[p]);
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int p = 0; p < 4; ++p) {
-        const int k = k0 + tx + 16 * p;
+    for (int p = 0; p < Sh::PC; ++p) {
+        const int k = k0 + tx + Sh::TX * p;
         if (k >= kept) continue;
         OutT *dst = out_cols ? out_cols[k] : out + (long)k * ldo;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const long row = i0 + ty + 16 * q;
+        for (int q = 0; q < Sh::QR; ++q) {
+            const long row = i0 + ty + Sh::TY * q;
             if (row < n_valid) {
                 if constexpr (std::is_same<OutT, C>::value) {
                     dst[row] = acc[q][p];
@@ -415,8 +445,28 @@ void launch_project(T *const *cols, int m, long n_pad, const typename Store<T>::
     nb = (int)((n_pad + chunk - 1) / chunk);
     C *part = reinterpret_cast<C *>(s.partials);
     double *part_r2 = reinterpret_cast<double *>(part + (long)nb * m);
-    k_project<T, proj_cpw<T>()><<<nb, kThreads, 0, st>>>(
-        cols, m, n_pad, chunk, r, rec, part, part_r2, s.tickets + kTicketProject, h, out2);
+    auto args = [&](auto kern) {
+        kern<<<nb, kThreads, 0, st>>>(cols, m, n_pad, chunk, r, rec, part, part_r2, s.tickets + kTicketProject, h,
+                                      out2);
+    };
+    if constexpr (std::is_same<C, double>::value) {
+        // Columns per warp: 16 keeps one accumulator per column for 128
+        // columns per sweep (2 blocks/SM); 12 and 8 trade a second sweep for
+        // 3-4 resident blocks.  TRLX_PROJECT_CPW selects (tuning only).
+        static const int cpw = [] {
+            const char *e = std::getenv("TRLX_PROJECT_CPW");
+            int v = e ? std::atoi(e) : 16;
+            return (v == 8 || v == 12) ? v : 16;
+        }();
+        if (cpw == 8)
+            args(k_project<T, 8>);
+        else if (cpw == 12)
+            args(k_project<T, 12>);
+        else
+            args(k_project<T, 16>);
+    } else {
+        args(k_project<T, proj_cpw<T>()>);
+    }
 }
 
 template <class T>
@@ -440,21 +490,30 @@ void launch_normalize(typename Store<T>::C *r, long n_pad, const double *r2, dou
     k_normalize<T><<<elementwise_blocks(n_pad), kThreads, 0, st>>>(r, n_pad, r2, fixed, q, vcol);
 }
 
-template <class T>
-void launch_ritz(T *const *in_cols, int jml, long n_pad, const double *Y, int ldy, int kept,
-                 T *const *out_cols, cudaStream_t st) {
+template <class T, class OutT>
+void ritz_dispatch(T *const *in_cols, int jml, long n_pad, const double *Y, int ldy, int kept, OutT *const *out_cols,
+                   OutT *out, long ldo, long n_valid, cudaStream_t st) {
     if (kept <= 0) return;
-    dim3 grid((unsigned)(n_pad / kBM), (unsigned)((kept + kBN - 1) / kBN));
-    k_ritz<T, T><<<grid, kThreads, 0, st>>>(in_cols, jml, Y, ldy, kept, out_cols, nullptr, 0, n_pad);
+    const unsigned gx = (unsigned)(n_pad / kBM);
+    if (kept <= 32) {
+        k_ritz<T, OutT, 32><<<dim3(gx, 1), kThreads, 0, st>>>(in_cols, jml, Y, ldy, kept, out_cols, out, ldo, n_valid);
+    } else {
+        dim3 grid(gx, (unsigned)((kept + 63) / 64));
+        k_ritz<T, OutT, 64><<<grid, kThreads, 0, st>>>(in_cols, jml, Y, ldy, kept, out_cols, out, ldo, n_valid);
+    }
+}
+
+template <class T>
+void launch_ritz(T *const *in_cols, int jml, long n_pad, const double *Y, int ldy, int kept, T *const *out_cols,
+                 cudaStream_t st) {
+    ritz_dispatch<T, T>(in_cols, jml, n_pad, Y, ldy, kept, out_cols, nullptr, 0, n_pad, st);
 }
 
 template <class T>
 void launch_ritz_out(T *const *in_cols, int jml, long n_pad, const double *Y, int ldy, int kept,
                      typename Store<T>::C *out, long ldo, long n, cudaStream_t st) {
     using C = typename Store<T>::C;
-    if (kept <= 0) return;
-    dim3 grid((unsigned)(n_pad / kBM), (unsigned)((kept + kBN - 1) / kBN));
-    k_ritz<T, C><<<grid, kThreads, 0, st>>>(in_cols, jml, Y, ldy, kept, nullptr, out, ldo, n);
+    ritz_dispatch<T, C>(in_cols, jml, n_pad, Y, ldy, kept, nullptr, out, ldo, n, st);
 }
 
 template <class T>

@@ -71,6 +71,25 @@ class DeviceOperator:
             pass
 
 
+def residual_norms(op, evals, evecs):
+    """||A z_i - lambda_i z_i|| / ||z_i|| for device eigenvectors (rows of a
+    torch CUDA tensor), recomputed in FP64 with the built-in operator."""
+    import torch
+    lib = op.lib
+    name = "trlx_zmatvec" if op.complex else "trlx_matvec"
+    f = getattr(lib, name)
+    f.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+    f.restype = None
+    out = []
+    y = torch.empty_like(evecs[0])
+    for lam, z in zip(evals, evecs):
+        z = z.contiguous()
+        f(op.n, 1, z.data_ptr(), op.n, y.data_ptr(), op.n, op.handle)
+        torch.cuda.synchronize()
+        out.append(float(torch.linalg.vector_norm(y - float(lam) * z) / torch.linalg.vector_norm(z)))
+    return np.array(out)
+
+
 @dataclass
 class SolveResult:
     eval: np.ndarray
