@@ -1,4 +1,6 @@
-// Small dense FP64 host routines of the thick-restart Lanczos engine.
+// Host entry points of the small dense FP64 routines of the thick-restart
+// Lanczos engine (implementations shared with the device-side batched solver
+// live in dense_core.h and restart_core.h).
 //
 // Everything here operates on the projected problem (size <= maxlan), never
 // on length-n vectors, so it stays on the host in FP64.  The algorithms are

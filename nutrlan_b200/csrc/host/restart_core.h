@@ -1,36 +1,36 @@
 // Thick-restart policy: how many Ritz pairs to keep at a restart and (for
-// schemes 7/8) the next basis size.  The decision rules are those of the
-// reference's SRC/restart.c (trl_shuffle_eig and the scheme helpers at
-// :29-1408); they are restated here because `info->restart` must select the
-// same behaviour, and hence the same matvec counts, as the reference.
-#include <algorithm>
-#include <cfloat>
-#include <cmath>
-#include <cstdlib>
+// schemes 7/8) the next basis size, shared by the host engine and the
+// device-side batched solver (__host__ __device__ under nvcc).  The decision
+// rules are those of the reference's SRC/restart.c (trl_shuffle_eig and the
+// scheme helpers at :29-1408); they are restated here because
+// info->restart must select the same behaviour, and hence the same matvec
+// counts, as the reference.
+#pragma once
 
-#include "../../../include/trlan.h"
-#include "dense.h"
+#include "dense_core.h"
 
 namespace trlb {
-namespace {
+namespace core {
 
-inline int round_half_up(double x) { return (int)(x + 0.5); }
+namespace restart_detail {
+
+TRLB_HD inline int round_half_up(double x) { return (int)(x + 0.5); }
 
 // Search window [klm, krm] for the brute-force schemes (restart.c:29-81).
 // For lohi == 0 it also chooses a side and writes it to *lohi_out.
-void search_range(int nd, const double *res, trl_info *info, int ncl, int ncr,
+TRLB_HD inline void search_range(int nd, const double *res, trl_info *info, int ncl, int ncr,
                   int *lohi_out, int tind, int *klm, int *krm) {
-    int kl = std::max(ncl, 0);
-    int kr = std::min(ncr, nd - 1);
+    int kl = hmax(ncl, 0);
+    int kr = hmin(ncr, nd - 1);
     double bnd = info->tol * info->anrm;
     *lohi_out = info->lohi;
     if (info->lohi > 0) {
-        kr = std::min(std::max(info->maxlan - info->ned, (info->maxlan + info->nec) / 2) - 1,
-                      std::min(kr, tind - 1));
+        kr = hmin(hmax(info->maxlan - info->ned, (info->maxlan + info->nec) / 2) - 1,
+                      hmin(kr, tind - 1));
         while (kr + kr > ncl + ncr && res[kr] < bnd) --kr;
     } else if (info->lohi < 0) {
-        kl = std::max(std::min(info->ned, (info->maxlan + info->nec) / 2) - 1,
-                      std::max(tind + 1, kl));
+        kl = hmax(hmin(info->ned, (info->maxlan + info->nec) / 2) - 1,
+                      hmax(tind + 1, kl));
         while (kl + kl < ncl + ncr && res[kl] < bnd) ++kl;
     } else {
         if (tind - kl < kr - tind) {
@@ -43,8 +43,8 @@ void search_range(int nd, const double *res, trl_info *info, int ncl, int ncr,
         int j = info->locked + kl + nd - kr + 1;
         if (j > 0) {
             j /= 2;
-            kl = std::max(0, kl - j);
-            kr = std::min(kr + j, nd - 1);
+            kl = hmax(0, kl - j);
+            kr = hmin(kr + j, nd - 1);
         }
     }
     *klm = kl;
@@ -52,21 +52,21 @@ void search_range(int nd, const double *res, trl_info *info, int ncl, int ncr,
 }
 
 // Smallest gap ratio that still converges all wanted pairs within maxmv.
-double min_gap_ratio(const trl_info *info, int nd, int tind, const double *res) {
+TRLB_HD inline double min_gap_ratio(const trl_info *info, int nd, int tind, const double *res) {
     (void)nd;
     double gamma = info->maxmv * (info->nec + 1.0) / info->ned - info->matvec;
     if (gamma < info->klan)
-        gamma = std::max((info->maxmv - info->matvec) / ((double)(info->ned - info->nec)), 2.0);
-    return std::min(std::log(res[tind] / (info->tol * info->anrm)) / gamma, 0.5);
+        gamma = hmax((info->maxmv - info->matvec) / ((double)(info->ned - info->nec)), 2.0);
+    return hmin(log(res[tind] / (info->tol * info->anrm)) / gamma, 0.5);
 }
 
-inline double gap_ratio(int i, int j, int tind, const double *lambda) {
+TRLB_HD inline double gap_ratio(int i, int j, int tind, const double *lambda) {
     return (lambda[i] - lambda[tind]) / (lambda[j] - lambda[tind]);
 }
 
 // Shared by the dynamic schemes 5 and 7: fraction of the search window that
 // must separate the kept ends, from the observed vs predicted convergence.
-double dynamic_gap_fraction(trl_info *info) {
+TRLB_HD inline double dynamic_gap_fraction(trl_info *info) {
     const double kPi = 3.141592654;
     const double up = 1.0, dw = 0.7;
     info->avgm = (info->avgm * ((double)info->nloop - 1) + (double)(info->klan - info->k + 1)) /
@@ -75,31 +75,31 @@ double dynamic_gap_fraction(trl_info *info) {
     double z2 = 1.0 / info->cfac;
     if (z2 < 1.0) return 0.7;
     if (z1 < 1.0) return 1.0;
-    double observed = std::log(z1 + std::sqrt(z1 - 1.0) * std::sqrt(z1 + 1.0)) / (2.0 * info->avgm);
-    double achieved = std::log(z2 + std::sqrt(z2 - 1.0) * std::sqrt(z2 + 1.0)) /
+    double observed = log(z1 + sqrt(z1 - 1.0) * sqrt(z1 + 1.0)) / (2.0 * info->avgm);
+    double achieved = log(z2 + sqrt(z2 - 1.0) * sqrt(z2 + 1.0)) /
                       (info->klan - info->k + 1);
-    double t = std::pow(achieved / observed, 2.0);
-    t = std::atan(t) * (2.0 / kPi);
+    double t = pow(achieved / observed, 2.0);
+    t = atan(t) * (2.0 / kPi);
     return dw + (up - dw) * t;
 }
 
 // Scheme 7: minimise (reorthogonalisation cost) / (expected residual
 // reduction) over the kept ends (i, j) and the next basis size k.
-void scheme_gap_cost(int n, int tind, trl_info *info, const double *lambda,
+TRLB_HD inline void scheme_gap_cost(int n, int tind, trl_info *info, const double *lambda,
                      const double *res, int *kl, int *kr) {
     int nd = info->ned, mn = info->maxlan, k1, k2;
     search_range(n, res, info, *kl, *kr, &info->lohi, tind, &k1, &k2);
     double frac = dynamic_gap_fraction(info);
-    int t = (int)(std::abs(k2 - k1) * frac);
+    int t = (int)(abs(k2 - k1) * frac);
     double best = 0.0, best_gamma = 0.0, best_gamma0 = 0.0;
     int bk1 = k1, bk2 = k2, bm = info->klan, bl = 0;
     for (int i = k1; i <= k2 - t; ++i) {
         for (int j = i + t; j <= k2; ++j) {
             double gamma0 =
-                std::sqrt((lambda[i + 1] - lambda[tind]) / (lambda[j - 1] - lambda[i + 1]));
+                sqrt((lambda[i + 1] - lambda[tind]) / (lambda[j - 1] - lambda[i + 1]));
             int l1 = (i + 1) + (n - j);
             int l2 = l1 + info->locked;
-            int lo = std::max(std::min(l2 + 1, mn), nd);
+            int lo = hmax(hmin(l2 + 1, mn), nd);
             for (int k = lo; k <= mn; ++k) {
                 double gamma = (k - l2) * gamma0;
                 double val = ((k - l2) * (k + l2 - 1) + k * l1) / gamma;
@@ -121,7 +121,7 @@ void scheme_gap_cost(int n, int tind, trl_info *info, const double *lambda,
     info->k1 = bk1;
     info->k2 = bk2;
     info->k = bl;
-    info->predicted_crate = std::exp(-best_gamma);
+    info->predicted_crate = exp(-best_gamma);
     info->mgamma = best_gamma;
     info->gamma0 = best_gamma0;
     info->old_target = lambda[tind];
@@ -130,23 +130,23 @@ void scheme_gap_cost(int n, int tind, trl_info *info, const double *lambda,
 }
 
 // Scheme 8: as scheme 7 but the next basis size is fixed by rfact.
-void scheme_gap_cost_static(int n, int tind, trl_info *info, const double *lambda,
+TRLB_HD inline void scheme_gap_cost_static(int n, int tind, trl_info *info, const double *lambda,
                             const double *res, int *kl, int *kr) {
     const double kPi = 3.141592654;
     int nd = info->ned, mn = info->maxlan, k1, k2, t;
     search_range(n, res, info, *kl, *kr, &info->lohi, tind, &k1, &k2);
     if (info->crat > 0.0) {
-        double rate = -std::log(info->crat);
-        double need = -(rate * info->maxlan) / std::log(info->tol * info->anrm);
+        double rate = -log(info->crat);
+        double need = -(rate * info->maxlan) / log(info->tol * info->anrm);
         if (need >= 0.5 || info->klan < info->maxlan) {
-            t = (int)(std::abs(k2 - k1) * 0.8);
+            t = (int)(abs(k2 - k1) * 0.8);
         } else {
             double f = rate / min_gap_ratio(info, nd, tind, res);
-            f = std::atan(std::pow(f, 0.25)) * (4.0 / kPi);
-            t = (int)(std::abs(k2 - k1) * f);
+            f = atan(pow(f, 0.25)) * (4.0 / kPi);
+            t = (int)(abs(k2 - k1) * f);
         }
     } else {
-        t = (int)(std::abs(k2 - k1) * 0.8);
+        t = (int)(abs(k2 - k1) * 0.8);
     }
     int mn1 = round_half_up(2.0 * info->klan / 5.0);
     double best = 0.0;
@@ -154,12 +154,12 @@ void scheme_gap_cost_static(int n, int tind, trl_info *info, const double *lambd
     for (int i = k1; i <= k2 - t; ++i) {
         for (int j = i + t; j <= k2; ++j) {
             double gamma0 =
-                std::sqrt((lambda[i + 1] - lambda[tind]) / (lambda[j - 1] - lambda[i + 1]));
+                sqrt((lambda[i + 1] - lambda[tind]) / (lambda[j - 1] - lambda[i + 1]));
             int l1 = (i + 1) + (n - j);
             int l2 = l1 + info->locked;
             int m2 = mn1;
             if (mn1 < info->rfact * l2) m2 = (int)(info->rfact * l2);
-            m2 = std::max(std::min(m2, mn), nd);
+            m2 = hmax(hmin(m2, mn), nd);
             double gamma = (m2 - l2 + 1) * gamma0;
             double val = (m2 * m2 - l2 * l2 + 2 * m2 * l1) / gamma;
             if (best == 0.0 || val < best) {
@@ -176,17 +176,17 @@ void scheme_gap_cost_static(int n, int tind, trl_info *info, const double *lambd
 }
 
 // Number of extra pairs kept beyond the converged ones (schemes 1/2).
-int extra_pairs(int mnd, const trl_info *info) {
+TRLB_HD inline int extra_pairs(int mnd, const trl_info *info) {
     int extra = round_half_up((mnd - info->nec) * (0.4 + 0.1 * info->ned / (double)mnd));
     if (extra > info->ned + info->ned && extra > 5) {
         double g = ((double)mnd) / ((double)info->ned);
-        extra = round_half_up((extra + (std::log(g) * info->ned) * g) / (1.0 + g));
+        extra = round_half_up((extra + (log(g) * info->ned) * g) / (1.0 + g));
     }
     return extra;
 }
 
 // For lohi == 0: shift the window toward the end that converges faster.
-void balance_ends(const double *res, int kl0, int kr0, int *kl, int *kr) {
+TRLB_HD inline void balance_ends(const double *res, int kl0, int kr0, int *kl, int *kr) {
     while (*kl > kl0 && *kr < kr0) {
         if (10.0 * res[*kl] < res[*kr]) {
             if (res[*kl + 1] < res[*kr + 1]) {
@@ -209,17 +209,17 @@ void balance_ends(const double *res, int kl0, int kr0, int *kl, int *kr) {
 }
 
 // Scheme 1 (and 0): fixed number of extra pairs plus a minimum gap ratio.
-void scheme_fixed(int nd, int mnd, int tind, const double *lambda, const double *res,
+TRLB_HD inline void scheme_fixed(int nd, int mnd, int tind, const double *lambda, const double *res,
                   trl_info *info, int *kl, int *kr) {
     int kli = *kl, kri = *kr, kl0 = kli, kr0 = kri;
     int extra = extra_pairs(mnd, info);
-    int minsep = std::max(3, std::max(nd / 5, nd - 4 * info->ned));
+    int minsep = hmax(3, hmax(nd / 5, nd - 4 * info->ned));
     double gmin = min_gap_ratio(info, nd, tind, res);
     if (info->lohi > 0) {
-        kri = std::min(tind - 1, kri) - extra;
+        kri = hmin(tind - 1, kri) - extra;
         kli = -1;
     } else if (info->lohi < 0) {
-        kli = std::max(tind + 1, kli) + extra;
+        kli = hmax(tind + 1, kli) + extra;
         kri = nd;
     } else {
         ++extra;
@@ -228,7 +228,7 @@ void scheme_fixed(int nd, int mnd, int tind, const double *lambda, const double 
         balance_ends(res, kl0, kr0, &kli, &kri);
     }
     while (kli + minsep < kri &&
-           gap_ratio(std::max(0, kli), std::min(kri, nd - 1), tind, lambda) < gmin) {
+           gap_ratio(hmax(0, kli), hmin(kri, nd - 1), tind, lambda) < gmin) {
         if (info->lohi < 0)
             ++kli;
         else if (info->lohi > 0)
@@ -257,44 +257,44 @@ void scheme_fixed(int nd, int mnd, int tind, const double *lambda, const double 
 }
 
 // Scheme 6: progressively vary the thickness.
-void scheme_scan(int nd, const double *res, trl_info *info, int kept, int *kl, int *kr) {
+TRLB_HD inline void scheme_scan(int nd, const double *res, trl_info *info, int kept, int *kl, int *kr) {
     int kli = *kl, kri = *kr;
     if (info->lohi < 0) {
         kri = nd;
-        kli = kept + std::min(std::max(info->nec, 1), (nd - kept) / 2) - 1;
+        kli = kept + hmin(hmax(info->nec, 1), (nd - kept) / 2) - 1;
         if (kli <= 0) {
             if (nd > 6)
                 kli = nd / 2 - 1;
             else if (nd > 2)
                 kli = 1;
         } else if (kli + 3 > nd) {
-            kli = info->nec + std::min(info->ned, std::min(10, (nd - info->ned) / 2)) - 1;
+            kli = info->nec + hmin(info->ned, hmin(10, (nd - info->ned) / 2)) - 1;
         }
     } else if (info->lohi > 0) {
         kli = -1;
-        kri = kept + std::min(std::max(info->nec, 1), (nd - kept) / 2) - 1;
+        kri = kept + hmin(hmax(info->nec, 1), (nd - kept) / 2) - 1;
         if (kri <= 0) {
             if (nd > 6)
                 kri = nd / 2 - 1;
             else if (nd > 2)
                 kri = 1;
         } else if (kri + 4 > nd) {
-            kri = info->nec + std::min(info->ned, std::min(10, (nd - info->ned) / 2));
+            kri = info->nec + hmin(info->ned, hmin(10, (nd - info->ned) / 2));
         }
         kri = nd - kri - 1;
     } else {
         int kl0 = kli, kr0 = kri;
-        int extra = kept + std::min(info->nec, (nd - kept) / 2) + 1;
+        int extra = kept + hmin(info->nec, (nd - kept) / 2) + 1;
         if (extra <= 0) {
             if (nd > 6)
                 extra = nd / 2;
             else if (nd > 2)
                 extra = 2;
         } else if (extra + 3 > nd) {
-            extra = info->nec + std::min(info->ned, std::min(10, (nd - info->ned) / 2));
+            extra = info->nec + hmin(info->ned, hmin(10, (nd - info->ned) / 2));
         }
-        kli = std::max(kli, extra / 2 - 1);
-        kri = std::min(kri, nd - extra / 2 - 1);
+        kli = hmax(kli, extra / 2 - 1);
+        kri = hmin(kri, nd - extra / 2 - 1);
         balance_ends(res, kl0, kr0, &kli, &kri);
     }
     *kl = kli;
@@ -302,37 +302,37 @@ void scheme_scan(int nd, const double *res, trl_info *info, int kept, int *kl, i
 }
 
 // Scheme 2: keep the pairs whose residuals are close to the target's.
-void scheme_small_res(int nd, int mnd, int tind, const double *lambda, const double *res,
+TRLB_HD inline void scheme_small_res(int nd, int mnd, int tind, const double *lambda, const double *res,
                       trl_info *info, int *kl, int *kr) {
-    int minsep = std::max(3, std::max(nd / 5, nd - 4 * info->ned));
+    int minsep = hmax(3, hmax(nd / 5, nd - 4 * info->ned));
     int extra = extra_pairs(mnd, info);
     int kli = *kl, kri = *kr, kl0 = kli, kr0 = kri;
     double resmax = res[0];
-    for (int i = 1; i < nd; ++i) resmax = std::max(resmax, res[i]);
+    for (int i = 1; i < nd; ++i) resmax = hmax(resmax, res[i]);
     if (nd <= 0) resmax = 0.0;
     double acpt = resmax / res[tind];
     if (info->lohi > 0) {
         if (acpt < 0.999 && acpt >= 0.0) {
             int ii = tind - 1;
-            acpt = std::min(std::max(std::sqrt(acpt) * res[tind], res[ii] + res[ii]), resmax);
+            acpt = hmin(hmax(sqrt(acpt) * res[tind], res[ii] + res[ii]), resmax);
             kri = ii - 1;
             while (res[kri] < acpt && kri > kli + 3) --kri;
         } else {
             kri = kr0 - extra;
         }
-        kri = std::max(2, kri);
-        kli = std::min(kli, kri - 2);
+        kri = hmax(2, kri);
+        kli = hmin(kli, kri - 2);
     } else if (info->lohi < 0) {
         if (acpt < 0.999 && acpt >= 0.0) {
             int ii = tind + 1;
-            acpt = std::min(std::max(std::sqrt(acpt) * res[tind], res[ii] + res[ii]), resmax);
+            acpt = hmin(hmax(sqrt(acpt) * res[tind], res[ii] + res[ii]), resmax);
             kli = ii + 1;
             while (res[kli] < acpt && kli < kri - 3) ++kli;
         } else {
             kli = kl0 + extra;
         }
-        kli = std::min(nd - 4, kli);
-        kri = std::max(kri, kli + 2);
+        kli = hmin(nd - 4, kli);
+        kri = hmax(kri, kli + 2);
     } else {
         int i = kli + 1, j = kri - 1;
         for (int c = 1; c <= extra; ++c) {
@@ -352,7 +352,7 @@ void scheme_small_res(int nd, int mnd, int tind, const double *lambda, const dou
     double gmin = min_gap_ratio(info, nd, tind, res);
     bool stuck = false;
     while (kli + minsep < kri &&
-           gap_ratio(std::max(0, kli), std::min(nd - 1, kri), tind, lambda) < gmin && !stuck) {
+           gap_ratio(hmax(0, kli), hmin(nd - 1, kri), tind, lambda) < gmin && !stuck) {
         if (info->lohi < 0)
             ++kli;
         else if (info->lohi > 0)
@@ -369,20 +369,20 @@ void scheme_small_res(int nd, int mnd, int tind, const double *lambda, const dou
         while (i > kli + minsep && lambda[kri] - res[kri] < lambda[i] &&
                lambda[kri] + res[kri] < lambda[i] + res[i])
             --i;
-        kri = std::min(kri, i + 1);
+        kri = hmin(kri, i + 1);
     } else {
         int i = kl0 + 1;
         while (i < kri - minsep && lambda[kli] + res[kli] > lambda[i] &&
                lambda[kli] - res[kli] > lambda[i] - res[i])
             ++i;
-        kli = std::max(kli, i - 1);
+        kli = hmax(kli, i - 1);
     }
     *kl = kli;
     *kr = kri;
 }
 
 // Scheme 3: maximise the gap ratio of the target for a fixed window width.
-void scheme_max_gap(int nd, int tind, int kept, const double *lambda, const double *res,
+TRLB_HD inline void scheme_max_gap(int nd, int tind, int kept, const double *lambda, const double *res,
                     trl_info *info, int *kl, int *kr) {
     auto gratio = [&](int i, int j) {
         return lambda[j] == info->trgt ? DBL_MAX
@@ -391,16 +391,16 @@ void scheme_max_gap(int nd, int tind, int kept, const double *lambda, const doub
     int lohi, klm, krm;
     search_range(nd, res, info, *kl, *kr, &lohi, tind, &klm, &krm);
     int kli = klm, kri = krm;
-    int igap = std::max(std::min(nd - info->ned, round_half_up((krm - klm) * 0.4)), 2);
+    int igap = hmax(hmin(nd - info->ned, round_half_up((krm - klm) * 0.4)), 2);
     if (igap > 2 && info->matvec > info->maxlan) {
         // The reference weighs operator time against the rest using its own
         // timers; the same fields are filled by this engine.
         if (info->clk_op + info->tick_o >
             10.0 * (info->clk_orth + info->tick_h + info->clk_res + info->tick_r)) {
-            igap = std::max(2, nd - kept - 1);
+            igap = hmax(2, nd - kept - 1);
         } else {
             double bnd = min_gap_ratio(info, nd, tind, res);
-            if (info->crat < bnd) igap = std::max(2, nd - kept - 1);
+            if (info->crat < bnd) igap = hmax(2, nd - kept - 1);
         }
     }
     if (kli + igap > kri) {
@@ -437,7 +437,7 @@ void scheme_max_gap(int nd, int tind, int kept, const double *lambda, const doub
 
 // Schemes 4 and 5: brute-force search of a merit function over (i, j).
 template <class Merit>
-void brute_force(int lohi, int klm, int krm, int igap, Merit merit, double init, int *kl,
+TRLB_HD inline void brute_force(int lohi, int klm, int krm, int igap, Merit merit, double init, int *kl,
                  int *kr) {
     int kli = klm, kri = krm;
     double ss = init;
@@ -455,43 +455,44 @@ void brute_force(int lohi, int klm, int krm, int igap, Merit merit, double init,
     *kr = kri;
 }
 
-void scheme_max_progress(int nd, int tind, int kept, const double *lambda, const double *res,
+TRLB_HD inline void scheme_max_progress(int nd, int tind, int kept, const double *lambda, const double *res,
                          trl_info *info, int *kl, int *kr) {
     auto merit = [&](int i, int j) {
-        return (lambda[i] - info->trgt) * std::abs(j - i) / (lambda[j] - info->trgt);
+        return (lambda[i] - info->trgt) * abs(j - i) / (lambda[j] - info->trgt);
     };
     int lohi, klm, krm;
     search_range(nd, res, info, *kl, *kr, &lohi, tind, &klm, &krm);
-    int igap = std::max(std::min(nd - info->ned, round_half_up((krm - klm) * 0.4)), 2);
+    int igap = hmax(hmin(nd - info->ned, round_half_up((krm - klm) * 0.4)), 2);
     if (igap > 2 && igap + kept > nd && info->crat > 0.0) {
         double ss = min_gap_ratio(info, nd, tind, res);
-        if (ss > info->crat) igap = std::max(2, nd - kept - 1);
+        if (ss > info->crat) igap = hmax(2, nd - kept - 1);
     }
     double init = lohi > 0 ? merit(krm, klm) : merit(klm, krm);
     brute_force(lohi, klm, krm, igap, merit, init, kl, kr);
 }
 
-void scheme_max_reduction(int nd, int tind, int kept, const double *lambda,
+TRLB_HD inline void scheme_max_reduction(int nd, int tind, int kept, const double *lambda,
                           const double *res, trl_info *info, int *kl, int *kr) {
     auto merit = [&](int i, int j) {
-        return std::sqrt((lambda[i] - info->trgt) / (lambda[j] - lambda[i])) * std::abs(j - i);
+        return sqrt((lambda[i] - info->trgt) / (lambda[j] - lambda[i])) * abs(j - i);
     };
     int lohi, klm, krm;
     search_range(nd, res, info, *kl, *kr, &lohi, tind, &klm, &krm);
     double frac = dynamic_gap_fraction(info);
-    int igap = (int)(std::abs(krm - klm) * frac);
+    int igap = (int)(abs(krm - klm) * frac);
     if (igap > 2 && igap + kept > nd && info->crat > 0.0) {
         double ss = min_gap_ratio(info, nd, tind, res);
-        if (ss > info->crat) igap = std::max(2, nd - kept - 1);
+        if (ss > info->crat) igap = hmax(2, nd - kept - 1);
     }
     double init = lohi > 0 ? merit(krm, klm) : merit(klm, krm);
     brute_force(lohi, klm, krm, igap, merit, init, kl, kr);
 }
 
-}  // namespace
+}  // namespace restart_detail
 
-void shuffle_eig(int nd, int mnd, double *lambda, double *res, trl_info *info, int *kept,
+TRLB_HD inline void shuffle_eig(int nd, int mnd, double *lambda, double *res, trl_info *info, int *kept,
                  int locked) {
+    using namespace restart_detail;
     (void)locked;
     if (nd <= 5) {
         // Tiny basis: keep the pairs with the smallest residuals.
@@ -502,7 +503,7 @@ void shuffle_eig(int nd, int mnd, double *lambda, double *res, trl_info *info, i
     }
     // Converged prefix/suffix (ncl: last converged from the left, ncr: first
     // converged from the right).
-    double bnd = std::min(info->tol, DBL_EPSILON * info->anrm);
+    double bnd = hmin(info->tol, DBL_EPSILON * info->anrm);
     int ncr = 0, ncl = nd - 1;
     for (int i = nd - 1; i >= 0; --i) {
         if (!(res[i] <= bnd)) {
@@ -542,16 +543,16 @@ void shuffle_eig(int nd, int mnd, double *lambda, double *res, trl_info *info, i
         }
         if (info->lohi > 0) {
             kr = kl;
-            kl = std::min(ncl, std::max(0, nd - info->ned) - 1);
+            kl = hmin(ncl, hmax(0, nd - info->ned) - 1);
         } else if (info->lohi < 0) {
             kl = kr;
-            kr = std::max(ncr, std::min(nd - info->nec, info->ned + 1) - 1);
+            kr = hmax(ncr, hmin(nd - info->nec, info->ned + 1) - 1);
         } else if (ncr - tind > tind - ncl) {
             kl = kr;
-            kr = std::max(ncr, std::min(nd - info->nec, info->ned + 1) - 1);
+            kr = hmax(ncr, hmin(nd - info->nec, info->ned + 1) - 1);
         } else {
             kr = kl;
-            kl = std::min(ncl, std::max(0, nd - info->ned) - 1);
+            kl = hmin(ncl, hmax(0, nd - info->ned) - 1);
         }
     } else {
         *kept = nd;
@@ -563,9 +564,9 @@ void shuffle_eig(int nd, int mnd, double *lambda, double *res, trl_info *info, i
             if (info->restart <= -info->ned) {
                 if (info->lohi >= 0) {
                     kl = -1;
-                    kr = std::max(2, nd + info->restart);
+                    kr = hmax(2, nd + info->restart);
                 } else {
-                    kl = std::min(-info->restart, nd - 3) - 1;
+                    kl = hmin(-info->restart, nd - 3) - 1;
                     kr = nd;
                 }
             } else {
@@ -615,16 +616,16 @@ void shuffle_eig(int nd, int mnd, double *lambda, double *res, trl_info *info, i
     }
 
     // Enforce a minimum separation between the two kept ends.
-    int minsep = std::max(3, std::max(nd / 6, nd - 6 * info->ned));
+    int minsep = hmax(3, hmax(nd / 6, nd - 6 * info->ned));
     if (kr <= kl + minsep || kl + nd - kr + minsep > mnd) {
         if (ncl < kl && kl < kr && kr < ncr) {
             --kl;
             ++kr;
         } else if (info->lohi > 0) {
-            kr = std::max(minsep, std::min(nd / 3, ncr)) - 1;
+            kr = hmax(minsep, hmin(nd / 3, ncr)) - 1;
             kl = -1;
         } else if (info->lohi < 0) {
-            kl = std::min(nd - minsep, std::max((nd + nd) / 3, ncl + 2)) - 1;
+            kl = hmin(nd - minsep, hmax((nd + nd) / 3, ncl + 2)) - 1;
             kr = nd;
         } else {
             kl = (nd - minsep) / 2 - 2;
@@ -637,8 +638,10 @@ void shuffle_eig(int nd, int mnd, double *lambda, double *res, trl_info *info, i
         lambda[kl + i] = lambda[kr + i];
         res[kl + i] = res[kr + i];
     }
-    *kept = kl + std::max(1, nd - kr);
+    *kept = kl + hmax(1, nd - kr);
     if (info->lohi < -1) sort2(*kept, lambda, res);
 }
 
+
+}  // namespace core
 }  // namespace trlb
