@@ -116,6 +116,53 @@ void trlx_ztrlan(ztrl_matvec op, trl_info *info, int nrow, int mev,
                  trl_dcomplex *misc, int nmis, double *dwrk, int ldwrk,
                  const trlx_options *opts);
 
+/* ---------------------------------------------------------------------------
+ * Batched solver: many independent real symmetric problems of uneven size,
+ * smallest (lohi < 0) eigenpairs of each, solved by ONE persistent kernel
+ * launch.  Each problem is solved by a group of 256, 512 or 1024 threads of
+ * a CTA running the same thick-restart algorithm as trlan() (FP64 basis);
+ * problems are taken largest first from a device work queue.  The group
+ * size and the operator format (stencil or CSR) per size bucket
+ * (n > 32768, 8192 < n <= 32768, n <= 8192) are chosen by an autotuner
+ * that times a sample of each bucket.  No counterpart in the reference.
+ * ------------------------------------------------------------------------- */
+typedef struct trlx_batch trlx_batch;
+
+/* Problems A_p = 5-point Dirichlet Laplacian on an L[p] x L[p] grid
+   (4 on the diagonal, -1 couplings) + diag(d_p), d_p = diag[p] (host,
+   L[p]^2 doubles, site (i, j) at i + L*j).  L[p] >= 4. */
+int trlx_batch_create_stencil5(int nprob, const int *L,
+                               const double *const *diag, trlx_batch **out);
+/* Optional start vectors (host, n doubles each; NULL entries keep the
+   seeded uniform[-1, 1] start). */
+int trlx_batch_set_start(trlx_batch *b, const double *const *start);
+
+typedef struct {
+    int ned, maxlan, lohi, restart, maxmv; /* as in trl_info; maxlan <= 64 */
+    double tol;
+    unsigned long long seed; /* start vectors / random restarts          */
+    int threads;             /* 0: autotuned per bucket; else 256/512/1024 */
+    int format;              /* -1: autotuned; 0 stencil, 1 CSR           */
+} trlx_batch_options;
+
+typedef struct {
+    int bucket_threads[3];
+    int bucket_format[3];
+    double tune_seconds;
+} trlx_batch_config;
+
+void trlx_batch_default_options(trlx_batch_options *o);
+int trlx_batch_autotune(trlx_batch *b, const trlx_batch_options *o,
+                        trlx_batch_config *best);
+/* eval/res: nprob * ned (res = residual estimates), info: nprob * 4
+   (stat, nec, matvec, restarts); any may be NULL. */
+int trlx_batch_solve(trlx_batch *b, const trlx_batch_options *o, double *eval,
+                     double *res, int *info, trlx_batch_config *used);
+/* The ned eigenvectors of problem prob (ned * n doubles, host or device). */
+int trlx_batch_eigenvectors(trlx_batch *b, int prob, double *out);
+int trlx_batch_size(const trlx_batch *b, int prob);
+void trlx_batch_destroy(trlx_batch *b);
+
 /* Statistics of the last solve issued from the calling thread. */
 typedef struct {
     double seconds_total;     /* wall time of the solve                    */

@@ -1,0 +1,614 @@
+// Batched thick-restart Lanczos: many independent real symmetric problems
+// of uneven sizes solved by one persistent kernel launch.
+//
+// Every CTA repeatedly takes the next problem from an atomic work queue
+// (problems sorted largest first) and runs a complete thick-restart Lanczos
+// solve on it: the control flow of the reference's trlanczos
+// (SRC/trlcore.c:723-1532; same usecgs decision, classical Gram-Schmidt pass
+// loop, convergence tests and restart bookkeeping as the host engine), with
+// the projected-problem work done by thread 0 using the very same
+// __host__ __device__ routines as the host engine (dense_core.h,
+// restart_core.h).  Vector work is block-wide: the operator (5-point
+// stencil with a diagonal, or CSR), alpha and norm reductions, Gram-Schmidt
+// projection/update against the problem's basis, and the restart
+// recombination done in place tile by tile (the CTA owns all rows).
+//
+// The basis of each problem lives in HBM ((maxlan+1) columns); results are
+// deterministic per problem regardless of which CTA solved it.
+#include <algorithm>
+#include <cstdio>
+#include <numeric>
+#include <vector>
+
+#include "../../../include/trlx.h"
+#include "../host/dense_core.h"
+#include "../host/restart_core.h"
+#include "batched.h"
+#include "common.cuh"
+
+namespace trlb {
+namespace batched {
+
+constexpr int kMaxL = 64;  // largest supported maxlan
+
+struct Shared {
+    trl_info info;
+    double alpha[kMaxL + 2], beta[kMaxL + 2], alfrot[kMaxL + 2], betrot[kMaxL + 2];
+    double lambda[kMaxL + 2], res[kMaxL + 2], h[kMaxL + 2], g[kMaxL + 2], wrk2[2 * (kMaxL + 2)];
+    double red[32][8];
+    double scal[8];
+    int ctl[8];
+};
+
+// A group of threads of the CTA that solves one problem: its rank, size,
+// named-barrier id and shared state.  The CTA is split into 1, 2 or 4
+// groups per phase (1024, 512 or 256 threads).
+struct Grp {
+    int tid, nt, bar;
+    Shared *S;
+    __device__ inline void sync() const { asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nt) : "memory"); }
+};
+// Dynamic shared memory after Shared: rot (L^2), yy (L^2), dense workspace.
+__host__ __device__ inline size_t dyn_doubles(int maxlan) {
+    return 2 * (size_t)maxlan * maxlan + core::dense_ws_doubles(maxlan) + 8;
+}
+
+size_t group_bytes(int maxlan);
+__device__ inline size_t group_bytes_dev(int maxlan) {
+    return ((sizeof(Shared) + 15) / 16 * 16 + dyn_doubles(maxlan) * sizeof(double) + 127) / 128 * 128;
+}
+
+enum { kAlpha = 0, kR2Pre = 1, kH2 = 2, kR2 = 3, kTmp = 4 };
+enum { cGo = 0, cJnd = 1, cKept = 2, cLocked = 3, cFlag = 4, cIter = 5 };
+
+// ---- block-wide helpers ---------------------------------------------------
+// Sum K per-thread values over the block (fixed order); result in out[0..K).
+template <int K>
+__device__ inline void block_reduce(double (&v)[K], double *out, const Grp &G) {
+    Shared &S = *G.S;
+    const int lane = G.tid & 31, warp = G.tid >> 5, nw = G.nt >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) S.red[warp][k] = v[k];
+    }
+    G.sync();
+    if (G.tid < K) {
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += S.red[w][G.tid];
+        out[G.tid] = s;
+    }
+    G.sync();
+}
+
+__device__ inline double block_sum1(double v, const Grp &G) {
+    double a[1] = {v};
+    block_reduce<1>(a, &G.S->scal[kTmp], G);
+    return G.S->scal[kTmp];
+}
+
+// y = A x; returns alpha = x.y (all threads).
+__device__ inline double apply_op(const Params &P, const Problem &pr, const double *x, double *y, const Grp &G) {
+    double a = 0.0;
+    const int n = pr.n;
+    if (P.format == kFormatStencil5) {
+        const int L = pr.L;
+        const double *d = P.diag + pr.diag_off;
+        for (int i = G.tid; i < n; i += G.nt) {
+            const int ix = i % L, iy = i / L;
+            double s = (4.0 + d[i]) * x[i];
+            if (ix > 0) s -= x[i - 1];
+            if (ix < L - 1) s -= x[i + 1];
+            if (iy > 0) s -= x[i - L];
+            if (iy < L - 1) s -= x[i + L];
+            y[i] = s;
+            a += x[i] * s;
+        }
+    } else {
+        const long long *rp = P.row_ptr + pr.rp_off;
+        const int *ci = P.col + pr.ent_off;
+        const double *va = P.val + pr.ent_off;
+        for (int i = G.tid; i < n; i += G.nt) {
+            double s = 0.0;
+            for (long long k = rp[i]; k < rp[i + 1]; ++k) s += va[k] * x[ci[k]];
+            y[i] = s;
+            a += x[i] * s;
+        }
+    }
+    return block_sum1(a, G);
+}
+
+// h[c] = V[:,c].r (c < m) with r = y - alpha x - beta xp when rec; S.scal[kR2Pre] = |r|^2,
+// S.scal[kH2] = |h|^2.
+__device__ inline void project(const double *V, int ld, int n, int m, const double *y, bool rec, const double *x,
+                               const double *xp, double alpha, double beta, const Grp &G) {
+    Shared &S = *G.S;
+    double r2 = 0.0;
+    for (int c0 = 0; c0 < m; c0 += 8) {
+        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        const int mm = min(8, m - c0);
+        for (int i = G.tid; i < n; i += G.nt) {
+            double ri = y[i];
+            if (rec) ri -= alpha * x[i] + beta * xp[i];
+            if (c0 == 0) r2 += ri * ri;
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (k < mm) acc[k] = fma(V[(size_t)(c0 + k) * ld + i], ri, acc[k]);
+        }
+        block_reduce<8>(acc, &S.h[c0], G);
+    }
+    if (m == 0) {
+        for (int i = G.tid; i < n; i += G.nt) {
+            double ri = y[i];
+            r2 += ri * ri;
+        }
+    }
+    const double s = block_sum1(r2, G);
+    if (G.tid == 0) {
+        S.scal[kR2Pre] = s;
+        double h2 = 0.0;
+        for (int c = 0; c < m; ++c) h2 += S.h[c] * S.h[c];
+        S.scal[kH2] = h2;
+    }
+    G.sync();
+}
+
+// r = (y - alpha x - beta xp) - V h (in place in y); S.scal[kR2] = |r|^2.
+__device__ inline void update(const double *V, int ld, int n, int m, double *y, bool rec, const double *x,
+                              const double *xp, double alpha, double beta, const double *h, const Grp &G) {
+    Shared &S = *G.S;
+    double r2 = 0.0;
+    for (int i = G.tid; i < n; i += G.nt) {
+        double ri = y[i];
+        if (rec) ri -= alpha * x[i] + beta * xp[i];
+        for (int c = 0; c < m; ++c) ri = fma(-V[(size_t)c * ld + i], h[c], ri);
+        y[i] = ri;
+        r2 += ri * ri;
+    }
+    const double s = block_sum1(r2, G);
+    if (G.tid == 0) S.scal[kR2] = s;
+    G.sync();
+}
+
+__device__ inline void scale(double *y, int n, double sc, const Grp &G) {
+    for (int i = G.tid; i < n; i += G.nt) y[i] *= sc;
+    G.sync();
+}
+
+// Smoothed random vector (the breakdown restart; same stencil as the engine).
+__device__ inline void random_vector(double *y, int n, uint64_t seed, const Grp &G) {
+    for (int i = G.tid; i < n; i += G.nt) {
+        auto u = [&](long k) { return uniform01(seed, (uint64_t)k); };
+        double v;
+        if (n < 3)
+            v = u(i);
+        else if (i == 0)
+            v = 2.0 * u(0) + u(2) + u(n - 1);
+        else if (i == n - 1)
+            v = 2.0 * u(n - 1) + (2.0 * u(1) + u(2) + u(0)) + u(n - 2);
+        else
+            v = 2.0 * u(i) + u(i + 1) + u(i - 1);
+        y[i] = v;
+    }
+    G.sync();
+}
+
+// Classical Gram-Schmidt of column m against columns 0..m-1, continuing
+// after a first pass whose scalars are in S.scal (trl_cgs,
+// SRC/trlcore.c:2913-3117).  Returns the status; *rnrm the final norm.
+__device__ inline int cgs(const Params &P, int pid, double *V, int ld, int n, int m, bool pass_done, double *rnrm,
+                          const Grp &G) {
+    Shared &S = *G.S;
+    double *r = V + (size_t)m * ld;
+    const int maxorth = 3;
+    int irnd = 0, cnt = 0;
+    double normrr2 = 0.0, normdiff2 = 0.0;
+    if (m > 0) {
+        bool first = true;
+        while (cnt <= maxorth) {
+            if (!(first && pass_done)) {
+                project(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, G);
+                update(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, S.h, G);
+            }
+            first = false;
+            if (G.tid == 0) S.info.north++;
+            cnt++;
+            normdiff2 = S.scal[kH2];
+            normrr2 = S.scal[kR2];
+            *rnrm = sqrt(normrr2);
+            if (DBL_EPSILON * normrr2 > normdiff2) break;
+            if ((cnt > 1 && (m * DBL_EPSILON * DBL_EPSILON * (normrr2 + normdiff2) < normdiff2)) ||
+                !(normrr2 > DBL_MIN)) {
+                if (irnd > 0) break;
+                cnt = 0;
+                irnd++;
+                if (G.tid == 0) S.info.nrand++;
+                G.sync();
+                random_vector(r, n, P.seed ^ (0xD1B54A32D192ED03ull * (uint64_t)(pid + 1)) ^
+                                        (7919ull * (uint64_t)S.info.nrand), G);
+            }
+        }
+        if (normrr2 < normdiff2) return -203;
+    }
+    if (*rnrm > DBL_MIN)
+        scale(r, n, 1.0 / *rnrm, G);
+    else
+        return -204;
+    if (irnd > 0) *rnrm = 0.0;
+    return 0;
+}
+
+// trl_orth (SRC/trlcore.c:1766-1975) for the new column m: alpha(m-1) is in
+// S.alpha, the recurrence uses beta_prev; sets S.beta[m-1].
+__device__ inline int orth(const Params &P, int pid, double *V, int ld, int n, int m, bool recur, double beta_prev,
+                           int kept, const Grp &G) {
+    Shared &S = *G.S;
+    const int jnd = m, jm1 = jnd - 1;
+    double *r = V + (size_t)m * ld;
+    const double *x = V + (size_t)(m - 1) * ld;
+    const double *xp = m >= 2 ? V + (size_t)(m - 2) * ld : nullptr;
+    const double a = S.alpha[jnd - 1];
+    project(V, ld, n, m, r, recur, x, xp, a, beta_prev, G);
+    const double normrr2 = S.scal[kR2Pre];
+    if (!(normrr2 >= 0.0) || !(normrr2 <= DBL_MAX)) return -102;
+    double tmp = a * a;
+    // beta of the previous steps are in S.beta (thread-uniform reads).
+    if (jm1 > kept) {
+        tmp += S.beta[jm1 - 1] * S.beta[jm1 - 1];
+    } else if (kept > 0) {
+        for (int i = 0; i < jm1; ++i) tmp += S.beta[i] * S.beta[i];
+    }
+    bool usecgs;
+    if (jm1 == kept) {
+        usecgs = true;
+    } else if (jnd >= S.info.ntot) {
+        usecgs = false;
+    } else if (DBL_EPSILON * normrr2 >= tmp) {
+        double anorm = 0.0;
+        for (int i = 0; i < jnd; ++i) anorm = fmax(anorm, fabs(S.alpha[i]) + fabs(i == jnd - 1 ? sqrt(normrr2) : S.beta[i]));
+        usecgs = sqrt(normrr2) < DBL_EPSILON * anorm * S.info.ntot;
+    } else {
+        usecgs = true;
+    }
+    double beta_new;
+    if (usecgs) {
+        update(V, ld, n, m, r, recur, x, xp, a, beta_prev, S.h, G);
+        double rnrm = sqrt(normrr2);
+        const int st = cgs(P, pid, V, ld, n, m, true, &rnrm, G);
+        if (st) return st;
+        beta_new = rnrm;
+    } else {
+        // Local re-orthogonalisation against the last one or two vectors.
+        if (G.tid == 0) {
+            for (int c = 0; c < m; ++c) S.g[c] = (c >= m - min(2, m)) ? S.h[c] : 0.0;
+        }
+        G.sync();
+        update(V, ld, n, m, r, recur, x, xp, a, beta_prev, S.g, G);
+        if (G.tid == 0) S.alpha[jnd - 1] += S.h[m - 1];
+        beta_new = sqrt(normrr2);
+        G.sync();
+        scale(r, n, 1.0 / beta_new, G);
+    }
+    if (G.tid == 0) {
+        double b = beta_new;
+        if (b <= DBL_EPSILON * fabs(S.alpha[jnd - 1]))
+            b = 0.0;
+        else if (jnd >= S.info.ntot)
+            b = 0.0;
+        S.beta[jnd - 1] = b;
+    }
+    G.sync();
+    return 0;
+}
+
+// In place V[:, lck .. lck+kept) <- V[:, lck .. lck+jml) * yy (jml x kept),
+// tile by tile (the CTA owns every row, so no other reader exists).
+__device__ inline void ritz_in_place(double *V, int ld, int n, int lck, int jml, int kept, const double *yy,
+                                     double *tile /* kTile * jml */, const Grp &G) {
+    constexpr int kTile = 32;
+    for (int r0 = 0; r0 < n; r0 += kTile) {
+        const int rows = min(kTile, n - r0);
+        for (int e = G.tid; e < rows * jml; e += G.nt) {
+            const int rr = e % rows, c = e / rows;
+            tile[c * kTile + rr] = V[(size_t)(lck + c) * ld + r0 + rr];
+        }
+        G.sync();
+        for (int e = G.tid; e < rows * kept; e += G.nt) {
+            const int rr = e % rows, k = e / rows;
+            double s = 0.0;
+            for (int c = 0; c < jml; ++c) s = fma(tile[c * kTile + rr], yy[(size_t)k * jml + c], s);
+            V[(size_t)(lck + k) * ld + r0 + rr] = s;
+        }
+        G.sync();
+    }
+}
+
+__device__ inline void init_info(trl_info *info, int n, int maxlan, int lohi, int ned, double tol, int restart,
+                                 int maxmv) {
+    unsigned char *b = reinterpret_cast<unsigned char *>(info);
+    for (size_t i = 0; i < sizeof(trl_info); ++i) b[i] = 0;
+    info->tol = tol;
+    info->restart = restart > 0 ? restart : 0;
+    info->maxmv = maxmv;
+    info->maxlan = maxlan;
+    info->lohi = lohi;
+    info->ned = ned;
+    info->nloc = info->ntot = n;
+    info->tmv = -1;
+    info->trgt = -DBL_MAX;
+    info->tres = -1.0;
+    info->crat = 1.0;
+    info->npes = 1;
+    info->klan = min(maxlan, n);
+    if (info->restart >= 7) info->klan = min(maxlan, max(100, min(info->klan, 2 * ned)));
+}
+
+// One complete solve of problem pid by the calling CTA.
+__device__ void solve(const Params &P, int pid, const Grp &G, double *dyn) {
+    Shared &S = *G.S;
+    const Problem pr = P.probs[pid];
+    const int n = pr.n, ld = pr.ld, maxlan = P.maxlan, ned = P.ned, mev = ned + 1;
+    double *V = P.basis + pr.basis_off;
+    double *rot = dyn, *yy = dyn + (size_t)maxlan * maxlan, *dws = yy + (size_t)maxlan * maxlan;
+    double *tile = dws;  // the restart tile reuses the dense workspace
+    trl_info *info = &S.info;
+    if (G.tid == 0) init_info(info, n, maxlan, P.lohi, ned, P.tol, P.restart, P.maxmv);
+    G.sync();
+    // Start vector: caller's, or seeded uniform[-1, 1].
+    const uint64_t seed = P.seed + 0x9E3779B97F4A7C15ull * (uint64_t)(pid + 1);
+    for (int i = G.tid; i < n; i += G.nt)
+        V[i] = pr.start_off >= 0 ? P.start[pr.start_off + i] : 2.0 * uniform01(seed, (uint64_t)i) - 1.0;
+    G.sync();
+    double nrm = sqrt(block_sum1([&] {
+        double s = 0.0;
+        for (int i = G.tid; i < n; i += G.nt) s += V[i] * V[i];
+        return s;
+    }(), G));
+    int stat = 0;
+    if (!(nrm > DBL_MIN)) stat = -204;
+    if (!stat) scale(V, n, 1.0 / nrm, G);
+    int jnd = 0, kept = 0, locked = 0;
+    int i1 = ned;
+    int next_test = i1 + min(i1, min(6, ned / 2));
+    int prek = 0;
+    while (!stat && info->matvec < info->maxmv && info->nec < info->ned) {
+        jnd++;
+        if (jnd + 1 > maxlan + 1) {
+            stat = -1111;
+            break;
+        }
+        // First step after (re)start: arrowhead coupling.
+        double a = apply_op(P, pr, V + (size_t)(jnd - 1) * ld, V + (size_t)jnd * ld, G);
+        if (G.tid == 0) {
+            info->matvec++;
+            S.alpha[jnd - 1] = a;
+            S.beta[jnd - 1] = a;
+        }
+        G.sync();
+        update(V, ld, n, jnd, V + (size_t)jnd * ld, false, nullptr, nullptr, 0.0, 0.0, S.beta, G);
+        stat = orth(P, pid, V, ld, n, jnd, false, 0.0, kept, G);
+        if (stat) break;
+        if (G.tid == 0) {
+            for (int i = 0; i < locked; ++i) {
+                S.alfrot[i] = S.alpha[i];
+                S.betrot[i] = 0.0;
+            }
+            core::arrow_to_tridiag(jnd - locked, &S.alpha[locked], &S.beta[locked], rot, &S.alfrot[locked],
+                                   &S.betrot[locked], dws);
+            S.betrot[jnd - 1] = S.beta[jnd - 1];
+        }
+        G.sync();
+        while (jnd < info->klan && info->nec < info->ned) {
+            jnd++;
+            a = apply_op(P, pr, V + (size_t)(jnd - 1) * ld, V + (size_t)jnd * ld, G);
+            if (G.tid == 0) {
+                info->matvec++;
+                S.alpha[jnd - 1] = a;
+            }
+            G.sync();
+            stat = orth(P, pid, V, ld, n, jnd, true, S.beta[jnd - 2], kept, G);
+            if (G.tid == 0) {
+                S.alfrot[jnd - 1] = S.alpha[jnd - 1];
+                S.betrot[jnd - 1] = S.beta[jnd - 1];
+                if (!stat && info->matvec >= next_test) {
+                    int e = core::get_eval(jnd, locked, S.alfrot, S.betrot, S.lambda, S.res, dws);
+                    if (e) {
+                        S.ctl[cFlag] = e;
+                    } else {
+                        core::convergence_test(jnd, S.lambda, S.res, info, S.wrk2);
+                        if (info->nec < info->ned && info->nec > 0) {
+                            next_test = (int)((double)(info->ned * info->matvec) / (double)info->nec);
+                        } else if (info->nec == 0) {
+                            next_test = next_test + next_test;
+                            if (info->maxlan == info->ntot) next_test = (int)ceil(0.5 * (info->maxlan + info->matvec));
+                        }
+                        S.ctl[cFlag] = 0;
+                    }
+                } else {
+                    S.ctl[cFlag] = 0;
+                }
+                S.ctl[cIter] = next_test;
+            }
+            G.sync();
+            next_test = S.ctl[cIter];
+            if (stat) break;
+            if (S.ctl[cFlag]) {
+                stat = S.ctl[cFlag];
+                break;
+            }
+        }
+        if (stat) break;
+        // ---- restart or finish (thread 0 decides, all apply) ----------------
+        if (G.tid == 0) {
+            int st = 0;
+            prek = kept;
+            const int jml = jnd - locked;
+            int i2 = kept - locked + 1;
+            if (info->nec < info->ned) {
+                st = core::get_eval(jnd, locked, S.alfrot, S.betrot, S.lambda, S.res, dws);
+                if (!st) core::convergence_test(jnd, S.lambda, S.res, info, S.wrk2);
+            }
+            int go = 0;
+            if (!st && info->nec < info->ned && info->matvec < info->maxmv) {
+                go = 1;
+                core::shuffle_eig(jml, info->klan - locked, &S.lambda[locked], &S.res[locked], info, &kept, locked);
+                int ts = 0;
+                if (kept * 3 < jml) {
+                    ts = core::get_tvec(jml, &S.alfrot[locked], &S.betrot[locked], 0, i2, rot, kept,
+                                        &S.lambda[locked], yy, dws);
+                    if (ts == 0)
+                        for (int i = 0; i < locked + kept; ++i) S.alpha[i] = S.lambda[i];
+                }
+                if (kept * 3 >= jml || ts != 0) {
+                    for (int i = 0; i < locked + kept; ++i) S.alfrot[i] = S.lambda[i];
+                    ts = core::get_tvec_a(jml, prek - locked, &S.alpha[locked], &S.beta[locked], kept,
+                                          &S.alfrot[locked], yy, dws);
+                }
+                if (ts) st = ts;
+                if (!st) {
+                    for (int i = 0; i < kept; ++i) S.beta[locked + i] = yy[(size_t)(i + 1) * jml - 1] * S.betrot[jnd - 1];
+                    if (jml > info->ned + (info->ned / 5 + 6))
+                        core::set_locking(jml, kept, &S.alpha[locked], &S.beta[locked], yy, info->anrm, &i2);
+                    else
+                        i2 = 0;
+                    S.ctl[cJnd] = jml;       // columns recombined
+                    S.ctl[cKept] = kept;
+                    S.ctl[cLocked] = i2;     // newly locked
+                }
+            } else if (!st) {
+                // Final: sort and compute the wanted eigenvectors.
+                kept = min(info->nec, max(info->ned, mev - 1));
+                info->nec = kept;
+                if (kept == 0) kept = min(mev - 1, info->ned);
+                core::sort_eig(jnd, info->lohi, kept, info->ref, S.lambda, S.res);
+                double *ev = S.wrk2;
+                for (int i = 0; i < kept; ++i) ev[i] = S.lambda[i];
+                int ts = 0;
+                if (kept * 3 < jnd) ts = core::get_tvec(jnd, S.alfrot, S.betrot, locked, i2, rot, kept, ev, yy, dws);
+                if (kept * 3 >= jnd || ts != 0)
+                    ts = core::get_tvec_a(jnd, prek, S.alpha, S.beta, kept, ev, yy, dws);
+                if (ts) st = ts;
+                for (int i = 0; i < kept; ++i) {
+                    S.alpha[i] = ev[i];
+                    S.beta[i] = S.betrot[jnd - 1] * yy[(size_t)(1 + i) * jnd - 1];
+                }
+                S.ctl[cJnd] = jnd;
+                S.ctl[cKept] = kept;
+            }
+            S.ctl[cGo] = go;
+            S.ctl[cFlag] = st;
+        }
+        G.sync();
+        if (S.ctl[cFlag]) {
+            stat = S.ctl[cFlag];
+            break;
+        }
+        const int jml = S.ctl[cJnd];
+        kept = S.ctl[cKept];
+        if (S.ctl[cGo]) {
+            // Restart: kept Ritz vectors in place, then the residual vector.
+            ritz_in_place(V, ld, n, locked, jml, kept, yy, tile, G);
+            const double *rr = V + (size_t)jnd * ld;
+            double *dst = V + (size_t)(locked + kept) * ld;
+            for (int i = G.tid; i < n; i += G.nt) dst[i] = rr[i];
+            G.sync();
+            kept += locked;
+            locked += S.ctl[cLocked];
+            jnd = kept;
+            if (G.tid == 0) {
+                info->locked = locked;
+                if (info->nec > 0)
+                    next_test = (int)(((double)(info->matvec * info->ned)) / ((double)info->nec));
+                else
+                    next_test = next_test + info->maxlan;
+                S.ctl[cIter] = next_test;
+                info->nloop++;
+            }
+            G.sync();
+            next_test = S.ctl[cIter];
+        } else {
+            // Final eigenvectors straight into the output (not in place).
+            double *out = P.evec + pr.evec_off;
+            for (long e = G.tid; e < (long)n * kept; e += G.nt) {
+                const int i = (int)(e % n), k = (int)(e / n);
+                double s = 0.0;
+                for (int c = 0; c < jml; ++c) s = fma(V[(size_t)c * ld + i], yy[(size_t)k * jml + c], s);
+                out[(size_t)k * n + i] = s;
+            }
+            if (G.tid == 0) info->nloop++;
+            G.sync();
+            break;
+        }
+    }
+    if (G.tid == 0) {
+        const int ne = min(ned, max(info->nec, 0));
+        for (int i = 0; i < ned; ++i) {
+            P.eval[(size_t)pid * ned + i] = i < ne ? S.alpha[i] : 0.0;
+            P.res[(size_t)pid * ned + i] = i < ne ? fabs(S.beta[i]) : -1.0;
+        }
+        int *o = P.info_out + (size_t)pid * 4;
+        o[0] = stat;
+        o[1] = info->nec;
+        o[2] = info->matvec;
+        o[3] = info->nloop;
+    }
+    G.sync();
+}
+
+// Phases run largest problems first; in phase f the CTA is split into
+// groups of P.phase_threads[f] threads, each group taking problems from the
+// phase's queue until it is empty, then the whole CTA moves on.
+__global__ void __launch_bounds__(1024, 1) k_batched(Params P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const size_t per_group = group_bytes_dev(P.maxlan);
+    for (int f = 0; f < P.nphases; ++f) {
+        const int nt = P.phase_threads[f];
+        const int gidx = threadIdx.x / nt;
+        const int ngroups = blockDim.x / nt;
+        if (gidx < ngroups) {
+            Grp G{(int)threadIdx.x - gidx * nt, nt, 1 + gidx,
+                  reinterpret_cast<Shared *>(smem + gidx * per_group)};
+            double *dyn = reinterpret_cast<double *>(smem + gidx * per_group + (sizeof(Shared) + 15) / 16 * 16);
+            for (;;) {
+                if (G.tid == 0) G.S->ctl[cGo] = P.phase_begin[f] + (int)atomicAdd(P.queue + f, 1u);
+                G.sync();
+                const int q = G.S->ctl[cGo];
+                G.sync();
+                if (q >= P.phase_end[f]) break;
+                solve(P, P.order[q], G, dyn);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+size_t group_bytes(int maxlan) {
+    return ((sizeof(Shared) + 15) / 16 * 16 + dyn_doubles(maxlan) * sizeof(double) + 127) / 128 * 128;
+}
+// Shared memory for the largest split used by the launch.
+size_t smem_bytes(int maxlan, int min_threads) { return group_bytes(maxlan) * (1024 / min_threads); }
+
+int launch(const Params &P, int blocks, cudaStream_t st) {
+    int min_threads = 1024;
+    for (int f = 0; f < P.nphases; ++f) min_threads = std::min(min_threads, P.phase_threads[f]);
+    const size_t sm = smem_bytes(P.maxlan, min_threads);
+    if (cudaFuncSetAttribute(k_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+        return -1001;
+    k_batched<<<blocks, 1024, sm, st>>>(P);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1001;
+}
+
+int max_blocks_per_sm(int min_threads, int maxlan) {
+    int nb = 0;
+    const size_t sm = smem_bytes(maxlan, min_threads);
+    cudaFuncSetAttribute(k_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batched, 1024, sm) != cudaSuccess) return 1;
+    return std::max(nb, 1);
+}
+
+}  // namespace batched
+}  // namespace trlb

@@ -1,0 +1,403 @@
+// Host side of the batched solver: problem upload, the autotuner that picks
+// the thread-group size and operator format per size bucket, and the single
+// persistent launch that solves the whole batch.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "../../../include/trlx.h"
+#include "batched.h"
+
+using trlb::batched::Params;
+using trlb::batched::Problem;
+
+struct trlx_batch {
+    int nprob = 0;
+    bool stencil = false;            // created from 5-point stencil data
+    std::vector<Problem> probs;      // host copy (offsets)
+    std::vector<int> L;              // stencil grid sides
+    std::vector<long long> diag_off;
+    // device arrays
+    Problem *d_probs = nullptr;
+    int *d_order = nullptr;
+    double *d_diag = nullptr;
+    long long *d_rp = nullptr;
+    int *d_col = nullptr;
+    double *d_val = nullptr;
+    double *d_start = nullptr;
+    double *d_basis = nullptr;
+    size_t basis_doubles = 0;
+    double *d_evec = nullptr;
+    size_t evec_doubles = 0;
+    double *d_eval = nullptr, *d_res = nullptr;
+    int *d_info = nullptr;
+    unsigned *d_queue = nullptr;
+    int ned_alloc = 0, maxlan_alloc = 0;
+    // autotuned configuration (per bucket: threads, format)
+    bool tuned = false;
+    int tuned_maxlan = 0;
+    int bucket_threads[3] = {1024, 512, 256};
+    int bucket_format[3] = {0, 0, 0};
+    double tune_seconds = 0.0;
+};
+
+namespace {
+
+// Size buckets (rows): [0] > 32768, [1] (8192, 32768], [2] <= 8192.
+int bucket_of(int n) { return n > 32768 ? 0 : (n > 8192 ? 1 : 2); }
+
+template <class X>
+int upload(const std::vector<X> &h, X **d) {
+    if (h.empty()) return 0;
+    if (cudaMalloc(reinterpret_cast<void **>(d), sizeof(X) * h.size()) != cudaSuccess) {
+        cudaGetLastError();
+        return -5;
+    }
+    return cudaMemcpy(*d, h.data(), sizeof(X) * h.size(), cudaMemcpyHostToDevice) == cudaSuccess ? 0 : -1001;
+}
+
+int sms() {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+}
+
+// (Re)allocate basis, outputs and per-problem offsets for ned / maxlan.
+int prepare(trlx_batch *b, int ned, int maxlan) {
+    if (b->ned_alloc == ned && b->maxlan_alloc == maxlan && b->d_basis) return 0;
+    cudaFree(b->d_basis);
+    cudaFree(b->d_evec);
+    cudaFree(b->d_eval);
+    cudaFree(b->d_res);
+    cudaFree(b->d_info);
+    b->d_basis = b->d_evec = b->d_eval = b->d_res = nullptr;
+    b->d_info = nullptr;
+    size_t boff = 0, eoff = 0;
+    for (auto &p : b->probs) {
+        p.basis_off = (long long)boff;
+        p.evec_off = (long long)eoff;
+        boff += (size_t)(maxlan + 1) * p.ld;
+        eoff += (size_t)ned * p.n;
+    }
+    b->basis_doubles = boff;
+    b->evec_doubles = eoff;
+    if (cudaMalloc(&b->d_basis, sizeof(double) * boff) != cudaSuccess ||
+        cudaMalloc(&b->d_evec, sizeof(double) * eoff) != cudaSuccess ||
+        cudaMalloc(&b->d_eval, sizeof(double) * (size_t)b->nprob * ned) != cudaSuccess ||
+        cudaMalloc(&b->d_res, sizeof(double) * (size_t)b->nprob * ned) != cudaSuccess ||
+        cudaMalloc(&b->d_info, sizeof(int) * 4 * (size_t)b->nprob) != cudaSuccess) {
+        cudaGetLastError();
+        return -5;
+    }
+    cudaFree(b->d_probs);
+    b->d_probs = nullptr;
+    int rc = upload(b->probs, &b->d_probs);
+    if (rc) return rc;
+    b->ned_alloc = ned;
+    b->maxlan_alloc = maxlan;
+    return 0;
+}
+
+Params base_params(trlx_batch *b, const trlx_batch_options *o) {
+    Params P{};
+    P.nprob = b->nprob;
+    P.ned = o->ned;
+    P.maxlan = o->maxlan;
+    P.lohi = o->lohi;
+    P.restart = o->restart;
+    P.maxmv = o->maxmv;
+    P.tol = o->tol;
+    P.seed = o->seed;
+    P.probs = b->d_probs;
+    P.order = b->d_order;
+    P.diag = b->d_diag;
+    P.row_ptr = b->d_rp;
+    P.col = b->d_col;
+    P.val = b->d_val;
+    P.start = b->d_start;
+    P.basis = b->d_basis;
+    P.evec = b->d_evec;
+    P.eval = b->d_eval;
+    P.res = b->d_res;
+    P.info_out = b->d_info;
+    P.queue = b->d_queue;
+    return P;
+}
+
+// CSR arrays (5-point Laplacian + diagonal) for the problems listed; fills
+// the problems' rp/ent offsets.  Used when a stencil batch is tuned or run in
+// CSR format.
+int build_csr(trlx_batch *b, const std::vector<double> &hdiag) {
+    std::vector<long long> rp;
+    std::vector<int> col;
+    std::vector<double> val;
+    size_t rows = 0;
+    for (int p = 0; p < b->nprob; ++p) rows += (size_t)b->L[p] * b->L[p];
+    rp.reserve(rows + b->nprob);
+    col.reserve(5 * rows);
+    val.reserve(5 * rows);
+    for (int p = 0; p < b->nprob; ++p) {
+        const int L = b->L[p], n = L * L;
+        Problem &pr = b->probs[p];
+        pr.rp_off = (long long)rp.size();
+        pr.ent_off = (long long)col.size();
+        long long e = 0;
+        for (int i = 0; i < n; ++i) {
+            rp.push_back(e);
+            const int ix = i % L, iy = i / L;
+            auto put = [&](int j, double v) {
+                col.push_back(j);
+                val.push_back(v);
+                ++e;
+            };
+            if (iy > 0) put(i - L, -1.0);
+            if (ix > 0) put(i - 1, -1.0);
+            put(i, 4.0 + hdiag[b->diag_off[p] + i]);
+            if (ix < L - 1) put(i + 1, -1.0);
+            if (iy < L - 1) put(i + L, -1.0);
+        }
+        rp.push_back(e);
+    }
+    int rc = upload(rp, &b->d_rp);
+    if (!rc) rc = upload(col, &b->d_col);
+    if (!rc) rc = upload(val, &b->d_val);
+    return rc;
+}
+
+int run(trlx_batch *b, Params P, int blocks) {
+    if (cudaMemset(b->d_queue, 0, sizeof(unsigned) * 4) != cudaSuccess) return -1001;
+    int rc = trlb::batched::launch(P, blocks, 0);
+    if (rc) return rc;
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1001;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trlx_batch_create_stencil5(int nprob, const int *L, const double *const *diag, trlx_batch **out) {
+    if (nprob <= 0 || !L || !diag || !out) return -1;
+    auto *b = new trlx_batch();
+    b->nprob = nprob;
+    b->stencil = true;
+    b->L.assign(L, L + nprob);
+    std::vector<double> hdiag;
+    for (int p = 0; p < nprob; ++p) {
+        if (L[p] < 4) {
+            delete b;
+            return -1;
+        }
+        Problem pr{};
+        pr.n = L[p] * L[p];
+        pr.L = L[p];
+        pr.ld = (pr.n + 31) / 32 * 32;
+        pr.diag_off = (long long)hdiag.size();
+        pr.start_off = -1;
+        b->diag_off.push_back(pr.diag_off);
+        hdiag.insert(hdiag.end(), diag[p], diag[p] + pr.n);
+        b->probs.push_back(pr);
+    }
+    int rc = upload(hdiag, &b->d_diag);
+    // CSR form of the same operators, for the autotuner's format choice.
+    if (!rc) rc = build_csr(b, hdiag);
+    std::vector<int> order(nprob);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return b->probs[a].n > b->probs[c].n; });
+    if (!rc) rc = upload(order, &b->d_order);
+    if (!rc && cudaMalloc(&b->d_queue, sizeof(unsigned) * 4) != cudaSuccess) rc = -5;
+    if (rc) {
+        trlx_batch_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return 0;
+}
+
+int trlx_batch_set_start(trlx_batch *b, const double *const *start) {
+    if (!b || !start) return -1;
+    std::vector<double> h;
+    for (int p = 0; p < b->nprob; ++p) {
+        if (start[p]) {
+            b->probs[p].start_off = (long long)h.size();
+            h.insert(h.end(), start[p], start[p] + b->probs[p].n);
+        } else {
+            b->probs[p].start_off = -1;
+        }
+    }
+    cudaFree(b->d_start);
+    b->d_start = nullptr;
+    int rc = upload(h, &b->d_start);
+    if (rc) return rc;
+    if (b->d_probs) {
+        cudaFree(b->d_probs);
+        b->d_probs = nullptr;
+        rc = upload(b->probs, &b->d_probs);
+    }
+    return rc;
+}
+
+void trlx_batch_default_options(trlx_batch_options *o) {
+    if (!o) return;
+    o->ned = 8;
+    o->maxlan = 32;
+    o->lohi = -1;
+    o->restart = 1;
+    o->maxmv = 100000;
+    o->tol = 1e-8;
+    o->seed = 0x3243F6A8885A308Dull;
+    o->threads = 0;
+    o->format = -1;
+}
+
+int trlx_batch_autotune(trlx_batch *b, const trlx_batch_options *o, trlx_batch_config *best) {
+    if (!b || !o) return -1;
+    if (o->maxlan < 4 || o->maxlan > 64 || o->ned < 1 || o->ned >= o->maxlan) return -1;
+    int rc = prepare(b, o->ned, o->maxlan);
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int nsm = sms();
+    // Problems per bucket in solve order (largest first).
+    std::vector<int> order(b->nprob);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return b->probs[a].n > b->probs[c].n; });
+    double total = 0.0;
+    for (int bk = 0; bk < 3; ++bk) {
+        std::vector<int> members;
+        for (int q : order)
+            if (bucket_of(b->probs[q].n) == bk) members.push_back(q);
+        if (members.empty()) continue;
+        // A sample that fills the machine with the smallest groups once.
+        const int want = std::min<int>((int)members.size(), nsm * 4);
+        std::vector<int> sample;
+        for (int k = 0; k < want; ++k) sample.push_back(members[(size_t)k * members.size() / want]);
+        int *d_sample = nullptr;
+        if (upload(sample, &d_sample)) return -5;
+        double best_t = 1e30;
+        for (int fmt = 0; fmt < 2; ++fmt) {
+            for (int th : {1024, 512, 256}) {
+                Params P = base_params(b, o);
+                P.order = d_sample;
+                P.format = fmt;
+                P.nphases = 1;
+                P.phase_threads[0] = th;
+                P.phase_begin[0] = 0;
+                P.phase_end[0] = (int)sample.size();
+                P.maxmv = std::min(o->maxmv, 4 * o->maxlan);  // a bounded slice of the solve
+                cudaEventRecord(e0);
+                if (run(b, P, nsm)) {
+                    cudaFree(d_sample);
+                    return -1001;
+                }
+                cudaEventRecord(e1);
+                cudaEventSynchronize(e1);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                total += ms * 1e-3;
+                if (ms < best_t) {
+                    best_t = ms;
+                    b->bucket_threads[bk] = th;
+                    b->bucket_format[bk] = fmt;
+                }
+            }
+        }
+        cudaFree(d_sample);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->tuned = true;
+    b->tuned_maxlan = o->maxlan;
+    b->tune_seconds = total;
+    if (best) {
+        for (int k = 0; k < 3; ++k) {
+            best->bucket_threads[k] = b->bucket_threads[k];
+            best->bucket_format[k] = b->bucket_format[k];
+        }
+        best->tune_seconds = total;
+    }
+    return 0;
+}
+
+int trlx_batch_solve(trlx_batch *b, const trlx_batch_options *o, double *eval, double *res, int *info,
+                     trlx_batch_config *used) {
+    if (!b || !o) return -1;
+    if (o->maxlan < 4 || o->maxlan > 64 || o->ned < 1 || o->ned >= o->maxlan) return -1;
+    int rc = prepare(b, o->ned, o->maxlan);
+    if (rc) return rc;
+    if (o->threads == 0 && (!b->tuned || b->tuned_maxlan != o->maxlan)) {
+        rc = trlx_batch_autotune(b, o, nullptr);
+        if (rc) return rc;
+    }
+    // Phases follow the buckets (largest problems first).  One format per
+    // launch: the one most problems' buckets prefer.
+    int cnt[3] = {0, 0, 0};
+    for (auto &p : b->probs) cnt[bucket_of(p.n)]++;
+    Params P = base_params(b, o);
+    int fmt_votes[2] = {0, 0};
+    int pos = 0;
+    P.nphases = 0;
+    for (int bk = 0; bk < 3; ++bk) {
+        if (!cnt[bk]) continue;
+        int th = o->threads ? o->threads : b->bucket_threads[bk];
+        if (th != 256 && th != 512 && th != 1024) th = 1024;
+        fmt_votes[o->format >= 0 ? o->format : b->bucket_format[bk]] += cnt[bk];
+        P.phase_threads[P.nphases] = th;
+        P.phase_begin[P.nphases] = pos;
+        P.phase_end[P.nphases] = pos + cnt[bk];
+        pos += cnt[bk];
+        P.nphases++;
+    }
+    P.format = o->format >= 0 ? o->format : (fmt_votes[1] > fmt_votes[0] ? 1 : 0);
+    if (P.format == 0 && !b->stencil) P.format = 1;
+    rc = run(b, P, sms());
+    if (rc) return rc;
+    if (eval) cudaMemcpy(eval, b->d_eval, sizeof(double) * (size_t)b->nprob * o->ned, cudaMemcpyDeviceToHost);
+    if (res) cudaMemcpy(res, b->d_res, sizeof(double) * (size_t)b->nprob * o->ned, cudaMemcpyDeviceToHost);
+    if (info) cudaMemcpy(info, b->d_info, sizeof(int) * 4 * (size_t)b->nprob, cudaMemcpyDeviceToHost);
+    if (used) {
+        for (int k = 0; k < 3; ++k) {
+            used->bucket_threads[k] = o->threads ? o->threads : b->bucket_threads[k];
+            used->bucket_format[k] = P.format;
+        }
+        used->tune_seconds = b->tune_seconds;
+    }
+    return 0;
+}
+
+int trlx_batch_eigenvectors(trlx_batch *b, int prob, double *out) {
+    if (!b || prob < 0 || prob >= b->nprob || !out || !b->d_evec) return -1;
+    const Problem &p = b->probs[prob];
+    return cudaMemcpy(out, b->d_evec + p.evec_off, sizeof(double) * (size_t)b->ned_alloc * p.n, cudaMemcpyDefault) ==
+                   cudaSuccess
+               ? 0
+               : -1001;
+}
+
+int trlx_batch_size(const trlx_batch *b, int prob) {
+    if (!b || prob < 0 || prob >= b->nprob) return -1;
+    return b->probs[prob].n;
+}
+
+void trlx_batch_destroy(trlx_batch *b) {
+    if (!b) return;
+    cudaFree(b->d_probs);
+    cudaFree(b->d_order);
+    cudaFree(b->d_diag);
+    cudaFree(b->d_rp);
+    cudaFree(b->d_col);
+    cudaFree(b->d_val);
+    cudaFree(b->d_start);
+    cudaFree(b->d_basis);
+    cudaFree(b->d_evec);
+    cudaFree(b->d_eval);
+    cudaFree(b->d_res);
+    cudaFree(b->d_info);
+    cudaFree(b->d_queue);
+    delete b;
+}
+
+}  // extern "C"
