@@ -49,6 +49,8 @@ sys.path.insert(0, ROOT)
 
 WORKLOADS = {
     "anderson256": dict(kind="anderson", L=256, W=4.0, ned=32, maxlan=128, tol=1e-8),
+    "batched4096": dict(kind="batched", count=4096, ned=8, maxlan=32, tol=1e-8),
+    "batched512": dict(kind="batched", count=512, ned=8, maxlan=32, tol=1e-8),
     "anderson128": dict(kind="anderson", L=128, W=4.0, ned=32, maxlan=128, tol=1e-8),
     "laplace128": dict(kind="laplace", L=128, ned=10, maxlan=64, tol=1.4901e-8),
 }
@@ -134,6 +136,83 @@ def run_reference_sample(A, w, x0, sample_steps):
     return r["info"].matvec, r["seconds"]
 
 
+def run_batched(args, w, world, rank, local, pg):
+    """Batched configuration: `count` problems, L x L Dirichlet Laplacian +
+    uniform[0, 2] diagonal, L uniform in [48, 256]; 8 smallest each,
+    maxlan 32, tol 1e-8; one persistent launch per step.  Metric:
+    problems solved per second."""
+    import torch
+    from nutrlan_b200 import operators as ops
+    from nutrlan_b200.batched import Batch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    count = w["count"]
+    Ls = ops.batched_sizes(count, seed=777 + rank)
+    diags = [2.0 * ops.uniform01(1000 + 7919 * rank + k, np.arange(int(L) * int(L), dtype=np.uint64))
+             for k, L in enumerate(Ls)]
+    b = Batch.stencil5(Ls, diags)
+    kw = dict(ned=w["ned"], maxlan=w["maxlan"], tol=w["tol"], restart=1, maxmv=100000, seed=4242 + rank)
+    t_tune = time.perf_counter()
+    cfg = b.autotune(**kw)
+    t_tune = time.perf_counter() - t_tune
+    for _ in range(args.warmup):
+        b.solve(**kw)
+    torch.cuda.synchronize()
+    barrier(pg)
+    sampler = ClockSampler(local)
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        r = b.solve(**kw)
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    dt = reduce_max(pg, e0.elapsed_time(e1) * 1e-3, dev)
+    solved = int(np.sum((r.info[:, 0] == 0) & (r.info[:, 1] >= w["ned"])))
+    n_total = int(np.sum(Ls.astype(np.int64) ** 2))
+    matvecs = int(np.sum(r.info[:, 2]))
+    # Algorithmic bytes of one batch solve: per matvec, stencil (x, y, diag) +
+    # one Gram-Schmidt pass over the current basis (average size ~ 3/4 maxlan
+    # across a thick-restart cycle) read twice.
+    avg_cols = 0.75 * w["maxlan"]
+    sizes = Ls.astype(np.int64) ** 2
+    alg_bytes = float(np.sum(r.info[:, 2] * sizes * 8 * (3 + 2 * avg_cols + 4)))
+    value = count * world * args.steps / dt
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import ref
+        ref.build()
+        idx = np.linspace(0, count - 1, 6).astype(int)
+        t_cpu, n_cpu = 0.0, 0
+        for k in idx:
+            A = ops.laplacian_2d(int(Ls[k]), diag=diags[k])
+            from nutrlan_b200.batched import seeded_start
+            x0 = seeded_start(4242 + rank, int(k), A.n)
+            o = ref.trlan_csr(A, ned=w["ned"], maxlan=w["maxlan"], tol=w["tol"], restart=1,
+                              maxmv=100000, start=x0)
+            t_cpu += o["seconds"]
+            n_cpu += 1
+        cpu = {"value": n_cpu / t_cpu, "unit": "problems/s", "cores": os.cpu_count(), "kind": "reference",
+               "sample": f"reference trlan on {n_cpu} problems of the batch spread over the size range, "
+                         "solved one after another (OpenBLAS + OpenMP CSR callback)"}
+    if rank == 0:
+        line = {"metric": f"batched thick-restart Lanczos, {count} problems (smallest {w['ned']} each)",
+                "value": value, "unit": "problems/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+                "config": {"workload": f"batched{count}: L~U[48,256], 5-pt Laplacian + U[0,2] diag, "
+                                       f"ned={w['ned']}, maxlan={w['maxlan']}, tol={w['tol']}",
+                           "rows_total": n_total, "one_launch_per_step": True},
+                "solved": solved, "matvecs_total": matvecs,
+                "alg_GBps": alg_bytes / (dt / args.steps) / 1e9,
+                "autotune": {"bucket_threads": list(cfg.bucket_threads), "bucket_format": list(cfg.bucket_format),
+                             "seconds": t_tune},
+                "cpu_baseline": cpu, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    b.close()
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -183,6 +262,14 @@ def main():
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world, rank, local, pg = dist_setup(args)
+    if w["kind"] == "batched":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "batched workload: use the default workload"}))
+            return
+        run_batched(args, w, world, rank, local, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
     seed = 2024 + rank
     metric = f"Lanczos steps/s (SpMV + full CGS reorth), {args.workload}, smallest {w['ned']}"
     config = {"workload": f"{args.workload}: n={w['L'] ** (3 if w['kind'] == 'anderson' else 2)}, "
