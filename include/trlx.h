@@ -141,7 +141,9 @@ typedef struct {
     int ned, maxlan, lohi, restart, maxmv; /* as in trl_info; maxlan <= 64 */
     double tol;
     unsigned long long seed; /* start vectors / random restarts          */
-    int threads;             /* 0: autotuned per bucket; else 256/512/1024 */
+    int threads;             /* 0: autotuned per bucket; else 256/512/1024
+                                (-1 if that split's shared memory does not
+                                fit for this maxlan)                        */
     int format;              /* -1: autotuned; 0 stencil, 1 CSR           */
 } trlx_batch_options;
 
@@ -162,6 +164,59 @@ int trlx_batch_solve(trlx_batch *b, const trlx_batch_options *o, double *eval,
 int trlx_batch_eigenvectors(trlx_batch *b, int prob, double *out);
 int trlx_batch_size(const trlx_batch *b, int prob);
 void trlx_batch_destroy(trlx_batch *b);
+
+/* ---------------------------------------------------------------------------
+ * Seed network: a 5-layer convolutional network (3x3 kernels, dilations
+ * 1, 2, 4, 8, 1; channels 1 -> 32 -> 32 -> 32 -> 32 -> 16; ReLU after the
+ * first four layers; zero "same" padding) mapping a potential V on an
+ * H x W grid to 16 vectors whose span approximates the lowest eigenvectors
+ * of -Laplacian + V.  BF16 activations and weights, FP32 accumulation on the
+ * tensor cores, FP32 master weights updated by Adam.  Training minimises
+ * per sample  sum_k (1 - |U^T y_k|^2 / |y_k|^2)
+ *           + lam * sum_{j != k} (y_j . y_k)^2 / (|y_j|^2 |y_k|^2)
+ * against orthonormal reference eigenvectors U.  No counterpart in the
+ * reference.  Arrays (host or device): V is B * H * W floats (sample-major,
+ * site x + W * y), U and network outputs are B * H * W * 16 floats laid out
+ * [sample][site][vector].  Weights are exchanged as, per layer,
+ * [tap][c_in][c_out] (9 * 32 * 32 floats, tap = 3 * (dy + 1) + (dx + 1),
+ * unused channels zero) followed by 32 biases: trlx_seednet_num_params()
+ * floats in total.
+ * Returns 0, -1 (bad arguments), -5 (device allocation), -1001 (CUDA).
+ * ------------------------------------------------------------------------- */
+typedef struct trlx_seednet trlx_seednet;
+
+/* H >= 8, W >= 64 and a multiple of 64; max_batch samples per call. */
+int trlx_seednet_create(int H, int W, int max_batch, unsigned long long seed,
+                        trlx_seednet **out);
+void trlx_seednet_destroy(trlx_seednet *net);
+int trlx_seednet_forward(trlx_seednet *net, int B, const float *V, float *out);
+/* Loss per sample (loss_out, B floats) and, when grads != NULL, the
+   gradient of the batch-mean loss in the weight layout above. */
+int trlx_seednet_gradients(trlx_seednet *net, int B, const float *V,
+                           const float *U, float lam, float *loss_out,
+                           float *grads);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the batch-mean loss. */
+int trlx_seednet_train_step(trlx_seednet *net, int B, const float *V,
+                            const float *U, float lam, float lr,
+                            float *loss_out);
+int trlx_seednet_get_weights(trlx_seednet *net, float *out);
+/* Also resets the Adam state. */
+int trlx_seednet_set_weights(trlx_seednet *net, const float *in);
+int trlx_seednet_num_params(void);
+
+/* Rayleigh-Ritz start vector from a predicted subspace: Y (nrow x k FP32,
+   [site][vector], host or device, 1 <= k <= 32) is orthonormalised in FP64
+   (numerically dependent directions dropped), projected on the built-in
+   operator op (k applications), and start (nrow doubles, host or device)
+   receives the sum of the resulting Ritz vectors.  theta and res (k doubles,
+   host, optional) receive the Ritz values (ascending) and the residual norms
+   |A x - theta x| (-1 for dropped directions).  Pass start to trlan() with
+   trl_set_iguess(info, 0, 1, 0, NULL) and start in the first column of evec.
+   Returns the number of Ritz vectors (>= 1) or -1 (bad arguments), -5
+   (device allocation), -234 (Y numerically zero), -1001 (CUDA).  No
+   counterpart in the reference. */
+int trlx_seed_start(void *op, int nrow, int k, const float *Y, double *start,
+                    double *theta, double *res);
 
 /* Statistics of the last solve issued from the calling thread. */
 typedef struct {

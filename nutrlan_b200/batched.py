@@ -111,10 +111,22 @@ class Batch:
         self.ned = o.ned
         return BatchResult(ev, rs, info, cfg)
 
-    def eigenvectors(self, p):
+    def eigenvectors(self, p, out=None):
+        """(ned, n) eigenvectors of problem p: a new numpy array, or `out`
+        (a contiguous float64 numpy array or CUDA tensor of that size)."""
         n = self.lib.trlx_batch_size(self.handle, p)
-        out = np.zeros((self.ned, n))
-        rc = self.lib.trlx_batch_eigenvectors(self.handle, p, out.ctypes.data)
+        if out is None:
+            out = np.zeros((self.ned, n))
+        if hasattr(out, "data_ptr"):
+            import torch
+            if out.dtype != torch.float64 or not out.is_contiguous() or out.numel() != self.ned * n:
+                raise ValueError("out must be a contiguous float64 tensor of ned * n elements")
+            ptr = out.data_ptr()
+        else:
+            if out.dtype != np.float64 or not out.flags.c_contiguous or out.size != self.ned * n:
+                raise ValueError("out must be a contiguous float64 array of ned * n elements")
+            ptr = out.ctypes.data
+        rc = self.lib.trlx_batch_eigenvectors(self.handle, p, ptr)
         if rc:
             raise RuntimeError(f"trlx_batch_eigenvectors failed ({rc})")
         return out

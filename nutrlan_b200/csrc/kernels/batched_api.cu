@@ -252,6 +252,15 @@ void trlx_batch_default_options(trlx_batch_options *o) {
     o->format = -1;
 }
 
+// Whether groups of th threads fit: 1024 / th groups per CTA, each with its
+// shared state and dense workspace for maxlan.
+static bool split_fits(int maxlan, int th) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
+    return trlb::batched::smem_bytes(maxlan, th) <= (size_t)optin;
+}
+
 int trlx_batch_autotune(trlx_batch *b, const trlx_batch_options *o, trlx_batch_config *best) {
     if (!b || !o) return -1;
     if (o->maxlan < 4 || o->maxlan > 64 || o->ned < 1 || o->ned >= o->maxlan) return -1;
@@ -280,6 +289,7 @@ int trlx_batch_autotune(trlx_batch *b, const trlx_batch_options *o, trlx_batch_c
         double best_t = 1e30;
         for (int fmt = 0; fmt < 2; ++fmt) {
             for (int th : {1024, 512, 256}) {
+                if (!split_fits(o->maxlan, th)) continue;
                 Params P = base_params(b, o);
                 P.order = d_sample;
                 P.format = fmt;
@@ -344,6 +354,7 @@ int trlx_batch_solve(trlx_batch *b, const trlx_batch_options *o, double *eval, d
         if (!cnt[bk]) continue;
         int th = o->threads ? o->threads : b->bucket_threads[bk];
         if (th != 256 && th != 512 && th != 1024) th = 1024;
+        if (!split_fits(o->maxlan, th)) return -1;
         fmt_votes[o->format >= 0 ? o->format : b->bucket_format[bk]] += cnt[bk];
         P.phase_threads[P.nphases] = th;
         P.phase_begin[P.nphases] = pos;

@@ -1,0 +1,655 @@
+// Seed network: a 5-layer convolutional network that maps a potential V
+// (H x W, FP32) to 16 vectors spanning an approximation of the lowest
+// eigenvectors of -Laplacian + V; used to seed the thick-restart solve.
+//
+// Layers: 3x3 convolutions with dilations {1, 2, 4, 8, 1}, channels
+// 1 -> 32 -> 32 -> 32 -> 32 -> 16, ReLU after the first four; "same" zero
+// padding.  Activations are NHWC BF16 with 32 channels (the 1-channel input
+// and the 16-channel output are zero-padded to 32), weights BF16, every
+// product accumulated in FP32 on the tensor cores (mma.sync m16n8k16
+// bf16 -> f32), FP32 master weights updated by Adam.
+//
+// Kernels (all written for this project):
+//   k_conv      forward / backward-data implicit-GEMM convolution
+//               (pixels x 288 taps*channels x 32 output channels),
+//   k_conv_wgrad weight and bias gradients (288 x 32 per tap, summed over
+//               pixels; per-block partials reduced in a fixed order),
+//   k_loss_*    subspace loss against the true eigenvectors and its
+//               gradient with respect to the network output,
+//   k_adam      optimizer step and BF16 weight packing.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../../include/trlx.h"
+
+namespace trlb {
+namespace seednet {
+
+constexpr int kC = 32;          // channels of every activation tensor
+constexpr int kTaps = 9;
+constexpr int kLayers = 5;
+constexpr int kOut = 16;        // output vectors
+constexpr int kTilePix = 64;    // pixels per CTA in k_conv (4 warps x 16)
+constexpr int kDil[kLayers] = {1, 2, 4, 8, 1};
+constexpr int kCin[kLayers] = {1, 32, 32, 32, 32};
+constexpr int kCout[kLayers] = {32, 32, 32, 32, 16};
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<unsigned *>(&v);
+}
+
+// ---------------------------------------------------------------------------
+// out[p, co] = act( sum_{tap, ci} in[p + d*off(tap), ci] * w[tap][co][ci] + bias[co] )
+// in: NHWC bf16 (32 ch), w: [tap][co][ci] bf16, out: NHWC bf16 (32 ch) or,
+// when out_f32 != null, FP32 [pixel][16] (first 16 channels).
+// Each warp computes 16 pixels x 32 output channels (4 n8 tiles); A
+// fragments come straight from global/L1 (32-bit channel pairs), B from
+// shared memory.  relu: 1 applies max(0, .).  mask (optional, NHWC bf16):
+// multiply the input by [mask > 0] while loading (ReLU backward fused into
+// the backward-data convolution).
+__global__ void __launch_bounds__(128)
+    k_conv(const __nv_bfloat16 *__restrict__ in, const __nv_bfloat16 *__restrict__ w, const float *__restrict__ bias,
+           __nv_bfloat16 *out, float *out_f32, int B, int H, int W, int dil, int relu) {
+    __shared__ __align__(16) __nv_bfloat16 ws[kTaps * kC * kC];
+    for (int i = threadIdx.x; i < kTaps * kC * kC / 8; i += blockDim.x)
+        reinterpret_cast<uint4 *>(ws)[i] = reinterpret_cast<const uint4 *>(w)[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const long p0 = (long)blockIdx.x * kTilePix + warp * 16;  // first pixel of this warp
+    const long HW = (long)H * W;
+    // Pixels of rows g and g + 8 of the A fragment.
+    const long pa = p0 + g, pb = p0 + g + 8;
+    const int ba = (int)(pa / HW), ya = (int)((pa % HW) / W), xa = (int)(pa % W);
+    const int bb = (int)(pb / HW), yb = (int)((pb % HW) / W), xb = (int)(pb % W);
+    float acc[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[j][q] = 0.f;
+    const unsigned *in32 = reinterpret_cast<const unsigned *>(in);
+    const unsigned *w32 = reinterpret_cast<const unsigned *>(ws);
+#pragma unroll 1
+    for (int tap = 0; tap < kTaps; ++tap) {
+        const int dy = (tap / 3 - 1) * dil, dx = (tap % 3 - 1) * dil;
+        const int ya2 = ya + dy, xa2 = xa + dx, yb2 = yb + dy, xb2 = xb + dx;
+        const bool va = ya2 >= 0 && ya2 < H && xa2 >= 0 && xa2 < W;
+        const bool vb = yb2 >= 0 && yb2 < H && xb2 >= 0 && xb2 < W;
+        const long sa = (((long)ba * H + ya2) * W + xa2) * (kC / 2);  // 32-bit words
+        const long sb = (((long)bb * H + yb2) * W + xb2) * (kC / 2);
+#pragma unroll
+        for (int k0 = 0; k0 < kC; k0 += 16) {
+            unsigned a[4];
+            const int c = k0 / 2 + t;  // word index of channels (k0 + 2t, +1)
+            a[0] = va ? __ldg(in32 + sa + c) : 0u;
+            a[1] = vb ? __ldg(in32 + sb + c) : 0u;
+            a[2] = va ? __ldg(in32 + sa + c + 4) : 0u;
+            a[3] = vb ? __ldg(in32 + sb + c + 4) : 0u;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int co = j * 8 + g;
+                unsigned b[2];
+                const int base = (tap * kC + co) * (kC / 2) + k0 / 2 + t;
+                b[0] = w32[base];
+                b[1] = w32[base + 4];
+                mma_bf16(acc[j], a, b);
+            }
+        }
+    }
+    // Epilogue: rows g (pixel pa) and g + 8 (pixel pb); columns 2t, 2t+1 of
+    // each n8 tile j.
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int co = j * 8 + 2 * t;
+        const float b0 = bias ? bias[co] : 0.f, b1 = bias ? bias[co + 1] : 0.f;
+        float v0 = acc[j][0] + b0, v1 = acc[j][1] + b1, v2 = acc[j][2] + b0, v3 = acc[j][3] + b1;
+        if (relu) {
+            v0 = fmaxf(v0, 0.f);
+            v1 = fmaxf(v1, 0.f);
+            v2 = fmaxf(v2, 0.f);
+            v3 = fmaxf(v3, 0.f);
+        }
+        if (out_f32) {
+            if (co < kOut) {
+                out_f32[pa * kOut + co] = v0;
+                out_f32[pa * kOut + co + 1] = v1;
+                out_f32[pb * kOut + co] = v2;
+                out_f32[pb * kOut + co + 1] = v3;
+            }
+        } else {
+            reinterpret_cast<unsigned *>(out)[pa * (kC / 2) + co / 2] = pack_bf16(v0, v1);
+            reinterpret_cast<unsigned *>(out)[pb * (kC / 2) + co / 2] = pack_bf16(v2, v3);
+        }
+    }
+}
+
+// g_pre = g_post * [act > 0] (ReLU backward), NHWC bf16, elementwise.
+__global__ void k_relu_mask(__nv_bfloat16 *g, const __nv_bfloat16 *act, long n) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        if (!(__bfloat162float(act[i]) > 0.f)) g[i] = __float2bfloat16(0.f);
+}
+
+// ---------------------------------------------------------------------------
+// Weight gradient: dW[tap][ci][co] = sum_p in[p + d*off(tap), ci] * g[p, co];
+// db[co] = sum_p g[p, co].  Block b covers pixels [b*chunk, (b+1)*chunk);
+// warp w handles taps w, w+4, w+8 (A rows = ci, k = pixels, B = g).
+// Partials part[b][tap][ci][co] (+ part[b][9][0][co] for the bias).
+constexpr int kWgPix = 2048;
+
+__device__ __forceinline__ unsigned ld_pair(const __nv_bfloat16 *p0, const __nv_bfloat16 *p1, bool v0, bool v1) {
+    __nv_bfloat16 lo = v0 ? *p0 : __float2bfloat16(0.f);
+    __nv_bfloat16 hi = v1 ? *p1 : __float2bfloat16(0.f);
+    __nv_bfloat162 v(lo, hi);
+    return *reinterpret_cast<unsigned *>(&v);
+}
+
+__global__ void __launch_bounds__(128)
+    k_conv_wgrad(const __nv_bfloat16 *__restrict__ in, const __nv_bfloat16 *__restrict__ g, float *part, int B, int H,
+                 int W, int dil) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gi = lane >> 2, t = lane & 3;
+    const long HW = (long)H * W, P = (long)B * HW;
+    const long q0 = (long)blockIdx.x * kWgPix, q1 = min(P, q0 + kWgPix);
+    float acc[3][2][4][4];  // [tap slot][m16 tile of ci][n8 tile of co][frag]
+#pragma unroll
+    for (int s = 0; s < 3; ++s)
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[s][mi][j][q] = 0.f;
+    float bsum = 0.f;  // bias gradient of channel `lane` (warp 0)
+    for (long k0 = q0; k0 < q1; k0 += 16) {
+        // B fragments (k = pixel, n = co): pixels k0 + 2t, +1 and +8.
+        const long pk[4] = {k0 + 2 * t, k0 + 2 * t + 1, k0 + 2 * t + 8, k0 + 2 * t + 9};
+        bool pv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) pv[u] = pk[u] < q1;
+        unsigned bf[4][2];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int co = j * 8 + gi;
+            bf[j][0] = ld_pair(g + pk[0] * kC + co, g + pk[1] * kC + co, pv[0], pv[1]);
+            bf[j][1] = ld_pair(g + pk[2] * kC + co, g + pk[3] * kC + co, pv[2], pv[3]);
+        }
+        if (warp == 0) {
+            // Bias gradient: lane sums channel `lane` over these 16 pixels.
+            for (int u = 0; u < 16; ++u)
+                if (k0 + u < q1) bsum += __bfloat162float(g[(k0 + u) * kC + lane]);
+        }
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            const int tap = warp + 4 * s;
+            if (tap >= kTaps) break;
+            const int dy = (tap / 3 - 1) * dil, dx = (tap % 3 - 1) * dil;
+            // Source pixels of the 4 k positions of this thread, shifted by the tap.
+            const __nv_bfloat16 *src[4];
+            bool sv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const long p = pk[u];
+                const int b = (int)(p / HW), y = (int)((p % HW) / W) + dy, x = (int)(p % W) + dx;
+                sv[u] = pv[u] && y >= 0 && y < H && x >= 0 && x < W;
+                src[u] = in + (((long)b * H + y) * W + x) * kC;
+            }
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi) {
+                // A (m = ci, k = pixel): rows gi, gi + 8 of the ci tile mi.
+                const int ca = mi * 16 + gi, cb = ca + 8;
+                unsigned a[4];
+                a[0] = ld_pair(src[0] + ca, src[1] + ca, sv[0], sv[1]);
+                a[1] = ld_pair(src[0] + cb, src[1] + cb, sv[0], sv[1]);
+                a[2] = ld_pair(src[2] + ca, src[3] + ca, sv[2], sv[3]);
+                a[3] = ld_pair(src[2] + cb, src[3] + cb, sv[2], sv[3]);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) mma_bf16(acc[s][mi][j], a, bf[j]);
+            }
+        }
+    }
+    float *pb = part + (size_t)blockIdx.x * (kTaps + 1) * kC * kC;
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        const int tap = warp + 4 * s;
+        if (tap >= kTaps) break;
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int ci0 = mi * 16 + gi, co = j * 8 + 2 * t;
+                float *o = pb + (size_t)tap * kC * kC;
+                o[ci0 * kC + co] = acc[s][mi][j][0];
+                o[ci0 * kC + co + 1] = acc[s][mi][j][1];
+                o[(ci0 + 8) * kC + co] = acc[s][mi][j][2];
+                o[(ci0 + 8) * kC + co + 1] = acc[s][mi][j][3];
+            }
+    }
+    if (warp == 0) pb[(size_t)kTaps * kC * kC + lane] = bsum;
+}
+
+// Sum partials over blocks in order: grad[i] = sum_b part[b][i].
+__global__ void k_reduce_parts(const float *part, int nb, int stride, int len, float *grad) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (int b = 0; b < nb; ++b) s += part[(size_t)b * stride + i];
+        grad[i] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Loss.  Y: FP32 [pixel][16] network output, U: FP32 [pixel][16] true
+// eigenvectors (orthonormal columns per sample).  Per sample b:
+//   C = U^T Y, G = Y^T Y (16 x 16), n_k^2 = G_kk,
+//   L = sum_k (1 - |C[:,k]|^2 / n_k^2) + lam sum_{j != k} G_jk^2 / (n_j^2 n_k^2)
+// (the output columns lie in span(U) and are mutually orthogonal).
+// dL/dY = U A + Y Bm with A_jk = -2 C_jk / n_k^2,
+//   Bm_jk = 4 lam G_jk / (n_j^2 n_k^2) (j != k),
+//   Bm_kk = 2 |C[:,k]|^2 / n_k^4 - 4 lam sum_{j != k} G_jk^2 / (n_j^2 n_k^4).
+constexpr int kLossPix = 1024;
+
+__global__ void __launch_bounds__(256) k_loss_stats(const float *Y, const float *U, int HW, float *part) {
+    // Block (c, b): pixels [c*kLossPix, ...) of sample b; thread t owns entry
+    // (t / 16, t % 16) of C and of G.
+    const int b = blockIdx.y;
+    const long base = (long)b * HW;
+    const int i = threadIdx.x >> 4, k = threadIdx.x & 15;
+    float c = 0.f, gsum = 0.f;
+    const int p0 = blockIdx.x * kLossPix, p1 = min(HW, p0 + kLossPix);
+    for (int p = p0; p < p1; ++p) {
+        const float yk = Y[(base + p) * kOut + k];
+        c += U[(base + p) * kOut + i] * yk;
+        gsum += Y[(base + p) * kOut + i] * yk;
+    }
+    float *o = part + ((size_t)b * gridDim.x + blockIdx.x) * 512;
+    o[threadIdx.x] = c;
+    o[256 + threadIdx.x] = gsum;
+}
+
+__global__ void k_loss_coeffs(const float *part, int nchunks, float lam, float *coef, float *loss) {
+    // One block per sample, 256 threads: reduce C, G; then thread 0 builds
+    // A and Bm (coef[b][0..256) = A, [256..512) = Bm) and the loss.
+    const int b = blockIdx.x;
+    __shared__ float C[256], G[256];
+    float c = 0.f, gsum = 0.f;
+    for (int ch = 0; ch < nchunks; ++ch) {
+        const float *o = part + ((size_t)b * nchunks + ch) * 512;
+        c += o[threadIdx.x];
+        gsum += o[256 + threadIdx.x];
+    }
+    C[threadIdx.x] = c;  // C[i*16 + k] = (U^T Y)_ik
+    G[threadIdx.x] = gsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float n2[16], cc[16];
+        for (int k = 0; k < 16; ++k) {
+            n2[k] = fmaxf(G[k * 16 + k], 1e-30f);
+            float s = 0.f;
+            for (int i = 0; i < 16; ++i) s += C[i * 16 + k] * C[i * 16 + k];
+            cc[k] = s;
+        }
+        float L = 0.f;
+        float *A = coef + (size_t)b * 512, *Bm = A + 256;
+        for (int k = 0; k < 16; ++k) {
+            L += 1.f - cc[k] / n2[k];
+            float diag = 2.f * cc[k] / (n2[k] * n2[k]);
+            for (int j = 0; j < 16; ++j) {
+                A[j * 16 + k] = -2.f * C[j * 16 + k] / n2[k];
+                if (j != k) {
+                    const float s = G[j * 16 + k] * G[j * 16 + k] / (n2[j] * n2[k]);
+                    L += lam * s;
+                    Bm[j * 16 + k] = 4.f * lam * G[j * 16 + k] / (n2[j] * n2[k]);
+                    diag -= 4.f * lam * s / n2[k];
+                }
+            }
+            Bm[k * 16 + k] = diag;
+        }
+        loss[b] = L;
+    }
+}
+
+// dY[p, k] = sum_j U[p, j] A_jk + Y[p, j] Bm_jk, written as NHWC bf16 with
+// 32 channels (16..31 zero) for the backward pass of the last layer.
+__global__ void k_loss_grad(const float *Y, const float *U, const float *coef, int HW, long P, float scale,
+                            __nv_bfloat16 *dY) {
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (long)gridDim.x * blockDim.x) {
+        const int b = (int)(p / HW);
+        const float *A = coef + (size_t)b * 512, *Bm = A + 256;
+        float u[16], y[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            u[j] = U[p * kOut + j];
+            y[j] = Y[p * kOut + j];
+        }
+        for (int k = 0; k < 16; k += 2) {
+            float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                s0 += u[j] * A[j * 16 + k] + y[j] * Bm[j * 16 + k];
+                s1 += u[j] * A[j * 16 + k + 1] + y[j] * Bm[j * 16 + k + 1];
+            }
+            reinterpret_cast<unsigned *>(dY)[p * (kC / 2) + k / 2] = pack_bf16(scale * s0, scale * s1);
+        }
+        for (int k = 16; k < kC; k += 2) reinterpret_cast<unsigned *>(dY)[p * (kC / 2) + k / 2] = 0u;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Adam on the FP32 master weights (layout [tap][ci][co] per layer, zero
+// outside the layer's real channels) and packing of the BF16 copies:
+// forward [tap][co][ci] and backward-data [tap'][ci][co] with tap' = 8 - tap.
+__global__ void k_adam(float *w, const float *gw, float *m, float *v, int len, float lr, float b1, float b2,
+                       float eps, float bc1, float bc2, const unsigned char *mask) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) {
+        if (mask && !mask[i]) continue;
+        const float gr = gw[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gr;
+        const float vi = b2 * v[i] + (1.f - b2) * gr * gr;
+        m[i] = mi;
+        v[i] = vi;
+        w[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    }
+}
+
+__global__ void k_pack(const float *w, __nv_bfloat16 *wf, __nv_bfloat16 *wb) {
+    // w: [tap][ci][co] FP32 -> wf[tap][co][ci], wb[8 - tap][ci][co]
+    // (backward data: input channels co, output channels ci).
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kTaps * kC * kC; i += gridDim.x * blockDim.x) {
+        const int tap = i / (kC * kC), ci = (i / kC) % kC, co = i % kC;
+        const __nv_bfloat16 v = __float2bfloat16(w[i]);
+        wf[(tap * kC + co) * kC + ci] = v;
+        wb[((kTaps - 1 - tap) * kC + ci) * kC + co] = v;
+    }
+}
+
+// Input packing: V (FP32, [b][y][x]) * scale into channel 0 of NHWC bf16.
+__global__ void k_pack_input(const float *V, long P, float scale, __nv_bfloat16 *x) {
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (long)gridDim.x * blockDim.x) {
+        unsigned *o = reinterpret_cast<unsigned *>(x) + p * (kC / 2);
+        o[0] = pack_bf16(V[p] * scale, 0.f);
+        for (int k = 1; k < kC / 2; ++k) o[k] = 0u;
+    }
+}
+
+}  // namespace seednet
+}  // namespace trlb
+
+// ===========================================================================
+// Host API
+// ===========================================================================
+using namespace trlb::seednet;
+
+struct trlx_seednet {
+    int H = 0, W = 0, Bmax = 0;
+    float in_scale = 1.f / 50.f;
+    // per layer: FP32 master [tap][ci][co], Adam moments, BF16 packs, bias
+    float *w[kLayers] = {}, *m[kLayers] = {}, *v[kLayers] = {}, *gw[kLayers] = {};
+    float *bias[kLayers] = {}, *mb[kLayers] = {}, *vb[kLayers] = {}, *gb[kLayers] = {};
+    unsigned char *mask[kLayers] = {};
+    __nv_bfloat16 *wf[kLayers] = {}, *wb[kLayers] = {};
+    // activations: act[0] = input, act[l+1] = output of layer l (hidden)
+    __nv_bfloat16 *act[kLayers] = {};
+    __nv_bfloat16 *g0 = nullptr, *g1 = nullptr;  // gradient ping-pong
+    float *Y = nullptr;                           // network output [P][16]
+    float *part = nullptr;
+    size_t part_len = 0;
+    float *coef = nullptr, *loss = nullptr, *Vd = nullptr, *Ud = nullptr;
+    int step = 0;
+};
+
+namespace {
+
+int blocks_for(long n, int t = 256) { return (int)std::min<long>((n + t - 1) / t, 148L * 16); }
+
+void pack_layer(trlx_seednet *net, int l) {
+    k_pack<<<36, 256>>>(net->w[l], net->wf[l], net->wb[l]);
+}
+
+// Forward pass for B samples already packed in act[0]; output in net->Y.
+void forward(trlx_seednet *net, int B) {
+    const long P = (long)B * net->H * net->W;
+    const int grid = (int)(P / kTilePix);
+    for (int l = 0; l < kLayers; ++l) {
+        const bool last = l == kLayers - 1;
+        k_conv<<<grid, 128>>>(net->act[l], net->wf[l], net->bias[l], last ? nullptr : net->act[l + 1],
+                              last ? net->Y : nullptr, B, net->H, net->W, kDil[l], last ? 0 : 1);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int trlx_seednet_create(int H, int W, int max_batch, unsigned long long seed, trlx_seednet **out) {
+    if (!out || H < 8 || W < 64 || W % 64 || max_batch < 1) return -1;
+    auto *net = new trlx_seednet();
+    net->H = H;
+    net->W = W;
+    net->Bmax = max_batch;
+    const long P = (long)max_batch * H * W;
+    const size_t wl = (size_t)kTaps * kC * kC;
+    bool ok = true;
+    auto alloc = [&](void **p, size_t bytes) {
+        if (cudaMalloc(p, bytes) != cudaSuccess) ok = false;
+        else cudaMemset(*p, 0, bytes);
+    };
+    for (int l = 0; l < kLayers; ++l) {
+        alloc((void **)&net->w[l], wl * 4);
+        alloc((void **)&net->m[l], wl * 4);
+        alloc((void **)&net->v[l], wl * 4);
+        alloc((void **)&net->gw[l], (wl + kC) * 4);
+        alloc((void **)&net->bias[l], kC * 4);
+        alloc((void **)&net->mb[l], kC * 4);
+        alloc((void **)&net->vb[l], kC * 4);
+        alloc((void **)&net->gb[l], kC * 4);
+        alloc((void **)&net->mask[l], wl);
+        alloc((void **)&net->wf[l], wl * 2);
+        alloc((void **)&net->wb[l], wl * 2);
+        alloc((void **)&net->act[l], (size_t)P * kC * 2);
+        // He-style initialisation of the real channels (host RNG, splitmix).
+        std::vector<float> hw(wl, 0.f);
+        std::vector<unsigned char> hm(wl, 0);
+        const float sd = std::sqrt(2.0f / (kTaps * kCin[l]));
+        uint64_t s = seed + 0x9E3779B97F4A7C15ull * (l + 1);
+        for (int tap = 0; tap < kTaps; ++tap)
+            for (int ci = 0; ci < kCin[l]; ++ci)
+                for (int co = 0; co < kCout[l]; ++co) {
+                    // Box-Muller from two splitmix draws.
+                    auto draw = [&]() {
+                        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+                        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+                        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+                        z ^= z >> 31;
+                        return ((z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+                    };
+                    const double u1 = draw(), u2 = draw();
+                    const size_t i = ((size_t)tap * kC + ci) * kC + co;
+                    hw[i] = (float)(sd * std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2));
+                    hm[i] = 1;
+                }
+        if (ok) {
+            cudaMemcpy(net->w[l], hw.data(), wl * 4, cudaMemcpyHostToDevice);
+            cudaMemcpy(net->mask[l], hm.data(), wl, cudaMemcpyHostToDevice);
+        }
+    }
+    alloc((void **)&net->g0, (size_t)P * kC * 2);
+    alloc((void **)&net->g1, (size_t)P * kC * 2);
+    alloc((void **)&net->Y, (size_t)P * kOut * 4);
+    const long nwg = (P + kWgPix - 1) / kWgPix;
+    net->part_len = std::max<size_t>((size_t)nwg * (kTaps + 1) * kC * kC, (size_t)max_batch * ((H * W + kLossPix - 1) / kLossPix) * 512);
+    alloc((void **)&net->part, net->part_len * 4);
+    alloc((void **)&net->coef, (size_t)max_batch * 512 * 4);
+    alloc((void **)&net->loss, (size_t)max_batch * 4);
+    alloc((void **)&net->Vd, (size_t)P * 4);
+    alloc((void **)&net->Ud, (size_t)P * kOut * 4);
+    if (!ok) {
+        trlx_seednet_destroy(net);
+        return -5;
+    }
+    for (int l = 0; l < kLayers; ++l) pack_layer(net, l);
+    cudaDeviceSynchronize();
+    *out = net;
+    return 0;
+}
+
+void trlx_seednet_destroy(trlx_seednet *net) {
+    if (!net) return;
+    for (int l = 0; l < kLayers; ++l) {
+        cudaFree(net->w[l]);
+        cudaFree(net->m[l]);
+        cudaFree(net->v[l]);
+        cudaFree(net->gw[l]);
+        cudaFree(net->bias[l]);
+        cudaFree(net->mb[l]);
+        cudaFree(net->vb[l]);
+        cudaFree(net->gb[l]);
+        cudaFree(net->mask[l]);
+        cudaFree(net->wf[l]);
+        cudaFree(net->wb[l]);
+        cudaFree(net->act[l]);
+    }
+    cudaFree(net->g0);
+    cudaFree(net->g1);
+    cudaFree(net->Y);
+    cudaFree(net->part);
+    cudaFree(net->coef);
+    cudaFree(net->loss);
+    cudaFree(net->Vd);
+    cudaFree(net->Ud);
+    delete net;
+}
+
+// V: B potentials (H*W FP32 each, host or device).  out: B * H*W * 16 FP32
+// ([sample][pixel][vector], host or device).
+int trlx_seednet_forward(trlx_seednet *net, int B, const float *V, float *out) {
+    if (!net || B < 1 || B > net->Bmax || !V) return -1;
+    const long P = (long)B * net->H * net->W;
+    if (cudaMemcpy(net->Vd, V, P * 4, cudaMemcpyDefault) != cudaSuccess) return -1001;
+    k_pack_input<<<blocks_for(P), 256>>>(net->Vd, P, net->in_scale, net->act[0]);
+    forward(net, B);
+    if (out && cudaMemcpy(out, net->Y, P * kOut * 4, cudaMemcpyDefault) != cudaSuccess) return -1001;
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1001;
+}
+
+// Loss and gradients of a batch (no update); loss_out[b] per sample,
+// grads (optional, host or device): per layer [tap][ci][co] then bias (32),
+// concatenated: 5 * (9*32*32 + 32) floats.
+static int loss_and_grad(trlx_seednet *net, int B, const float *V, const float *U, float lam, float *loss_out) {
+    const int H = net->H, W = net->W, HW = H * W;
+    const long P = (long)B * HW;
+    if (cudaMemcpy(net->Vd, V, P * 4, cudaMemcpyDefault) != cudaSuccess) return -1001;
+    if (cudaMemcpy(net->Ud, U, P * kOut * 4, cudaMemcpyDefault) != cudaSuccess) return -1001;
+    k_pack_input<<<blocks_for(P), 256>>>(net->Vd, P, net->in_scale, net->act[0]);
+    forward(net, B);
+    const int nch = (HW + kLossPix - 1) / kLossPix;
+    k_loss_stats<<<dim3(nch, B), 256>>>(net->Y, net->Ud, HW, net->part);
+    k_loss_coeffs<<<B, 256>>>(net->part, nch, lam, net->coef, net->loss);
+    k_loss_grad<<<blocks_for(P), 256>>>(net->Y, net->Ud, net->coef, HW, P, 1.0f / B, net->g0);
+    // Backward through the layers.
+    const int nwg = (int)((P + kWgPix - 1) / kWgPix);
+    __nv_bfloat16 *g = net->g0, *gn = net->g1;
+    for (int l = kLayers - 1; l >= 0; --l) {
+        if (l < kLayers - 1) k_relu_mask<<<blocks_for(P * kC), 256>>>(g, net->act[l + 1], P * kC);
+        k_conv_wgrad<<<nwg, 128>>>(net->act[l], g, net->part, B, H, W, kDil[l]);
+        // Partials have stride (kTaps + 1) * kC * kC; only the weight taps and
+        // the kC bias entries after them are written and reduced.
+        const int len = kTaps * kC * kC + kC;
+        k_reduce_parts<<<(len + 255) / 256, 256>>>(net->part, nwg, (kTaps + 1) * kC * kC, len, net->gw[l]);
+        cudaMemcpyAsync(net->gb[l], net->gw[l] + (size_t)kTaps * kC * kC, kC * 4, cudaMemcpyDeviceToDevice);
+        if (l > 0) {
+            const int grid = (int)(P / kTilePix);
+            k_conv<<<grid, 128>>>(g, net->wb[l], nullptr, gn, nullptr, B, H, W, kDil[l], 0);
+            std::swap(g, gn);
+        }
+    }
+    if (loss_out) cudaMemcpy(loss_out, net->loss, B * 4, cudaMemcpyDeviceToHost);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1001;
+}
+
+int trlx_seednet_gradients(trlx_seednet *net, int B, const float *V, const float *U, float lam, float *loss_out,
+                           float *grads) {
+    if (!net || B < 1 || B > net->Bmax || !V || !U) return -1;
+    int rc = loss_and_grad(net, B, V, U, lam, loss_out);
+    if (rc || !grads) return rc;
+    const size_t wl = (size_t)kTaps * kC * kC;
+    size_t off = 0;
+    for (int l = 0; l < kLayers; ++l) {
+        cudaMemcpy(grads + off, net->gw[l], wl * 4, cudaMemcpyDefault);
+        off += wl;
+        cudaMemcpy(grads + off, net->gb[l], kC * 4, cudaMemcpyDefault);
+        off += kC;
+    }
+    return 0;
+}
+
+int trlx_seednet_train_step(trlx_seednet *net, int B, const float *V, const float *U, float lam, float lr,
+                            float *loss_out) {
+    if (!net || B < 1 || B > net->Bmax || !V || !U) return -1;
+    int rc = loss_and_grad(net, B, V, U, lam, loss_out);
+    if (rc) return rc;
+    net->step++;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float bc1 = 1.f - std::pow(b1, (float)net->step), bc2 = 1.f - std::pow(b2, (float)net->step);
+    const int wl = kTaps * kC * kC;
+    for (int l = 0; l < kLayers; ++l) {
+        k_adam<<<(wl + 255) / 256, 256>>>(net->w[l], net->gw[l], net->m[l], net->v[l], wl, lr, b1, b2, eps, bc1, bc2,
+                                          net->mask[l]);
+        k_adam<<<1, 32>>>(net->bias[l], net->gb[l], net->mb[l], net->vb[l], kCout[l], lr, b1, b2, eps, bc1, bc2,
+                          nullptr);
+        pack_layer(net, l);
+    }
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1001;
+}
+
+// Weights (FP32) in/out: per layer [tap][ci][co] (9*32*32) then bias (32).
+int trlx_seednet_get_weights(trlx_seednet *net, float *out) {
+    if (!net || !out) return -1;
+    const size_t wl = (size_t)kTaps * kC * kC;
+    size_t off = 0;
+    for (int l = 0; l < kLayers; ++l) {
+        cudaMemcpy(out + off, net->w[l], wl * 4, cudaMemcpyDefault);
+        off += wl;
+        cudaMemcpy(out + off, net->bias[l], kC * 4, cudaMemcpyDefault);
+        off += kC;
+    }
+    return 0;
+}
+
+int trlx_seednet_set_weights(trlx_seednet *net, const float *in) {
+    if (!net || !in) return -1;
+    const size_t wl = (size_t)kTaps * kC * kC;
+    size_t off = 0;
+    for (int l = 0; l < kLayers; ++l) {
+        cudaMemcpy(net->w[l], in + off, wl * 4, cudaMemcpyDefault);
+        off += wl;
+        cudaMemcpy(net->bias[l], in + off, kC * 4, cudaMemcpyDefault);
+        off += kC;
+        pack_layer(net, l);
+    }
+    net->step = 0;
+    for (int l = 0; l < kLayers; ++l) {
+        cudaMemset(net->m[l], 0, wl * 4);
+        cudaMemset(net->v[l], 0, wl * 4);
+        cudaMemset(net->mb[l], 0, kC * 4);
+        cudaMemset(net->vb[l], 0, kC * 4);
+    }
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1001;
+}
+
+int trlx_seednet_num_params(void) { return kLayers * (kTaps * kC * kC + kC); }
+
+}  // extern "C"

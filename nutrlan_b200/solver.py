@@ -111,8 +111,8 @@ def solve(op, ned, maxlan, lohi=-1, tol=1.4901e-8, restart=1, maxmv=0, start=Non
           basis_bits=64, device=False, seed=0, evec=None):
     """Run trlan/ztrlan on a DeviceOperator through the C ABI.
 
-    ``start`` (length n) becomes the initial vector (guess = 1); otherwise the
-    reference's default ones vector is used.  ``device=True`` passes a torch
+    ``start`` (length n, numpy or CUDA tensor) becomes the initial vector
+    (guess = 1); otherwise the reference's default ones vector is used.  ``device=True`` passes a torch
     CUDA tensor as evec, so the solver never copies vectors to the host.
     """
     lib = load()
@@ -130,13 +130,17 @@ def solve(op, ned, maxlan, lohi=-1, tol=1.4901e-8, restart=1, maxmv=0, start=Non
         tdt = torch.complex128 if op.complex else torch.float64
         ev = evec if evec is not None else torch.zeros((mev, n), dtype=tdt, device="cuda")
         if start is not None:
-            ev[0].copy_(torch.as_tensor(np.asarray(start, dtype=dtype)))
+            if hasattr(start, "data_ptr"):
+                if start.data_ptr() != ev[0].data_ptr():
+                    ev[0].copy_(start)
+            else:
+                ev[0].copy_(torch.as_tensor(np.asarray(start, dtype=dtype)))
         torch.cuda.synchronize()
         evec_ptr = ev.data_ptr()
     else:
         ev = np.zeros((mev, n), dtype=dtype)
         if start is not None:
-            ev[0] = start
+            ev[0] = start.cpu().numpy() if hasattr(start, "data_ptr") else start
         evec_ptr = ev.ctypes.data
     wrk = np.zeros(mev)
     opts = TrlxOptions()

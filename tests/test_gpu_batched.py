@@ -80,3 +80,23 @@ def test_batched_caller_start_vectors(small):
         assert abs(r.info[2][2] - e.info.matvec) <= 0.05 * e.info.matvec + 8
     finally:
         b.set_start([None] * len(Ls))
+
+
+def test_batched_large_maxlan_uses_fitting_splits():
+    """maxlan 48, ned 16 (the learned-seed training configuration): the
+    autotuner only uses thread splits whose shared memory fits, and an
+    explicit split that does not fit is rejected up front."""
+    Ls = [48, 64, 40]
+    diags = [ops.wells_potential(L, 900 + k).reshape(-1) for k, L in enumerate(Ls)]
+    b = Batch.stencil5(Ls, diags)
+    try:
+        r = b.solve(ned=16, maxlan=48, tol=1e-8, seed=SEED)
+        for p, L in enumerate(Ls):
+            assert r.info[p][0] == 0 and r.info[p][1] >= 16
+            A = ops.laplacian_2d(L, diag=diags[p])
+            dense = np.linalg.eigvalsh(A.to_scipy().toarray())
+            np.testing.assert_allclose(r.eval[p], dense[:16], rtol=1e-10, atol=1e-12)
+        with pytest.raises(RuntimeError):
+            b.solve(ned=16, maxlan=48, tol=1e-8, seed=SEED, threads=256)
+    finally:
+        b.close()

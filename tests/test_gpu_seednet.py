@@ -1,0 +1,153 @@
+"""Seed network on the GPU: forward pass, per-sample loss and every layer's
+weight and bias gradient of the BF16 tensor-core kernels against the FP64
+oracle restatement (oracle/seednet_np.py, which rounds to bfloat16 where the
+kernels store bfloat16; tolerances below are relative to each tensor's
+norm), Adam training reducing the loss on real eigenvectors, the
+Rayleigh-Ritz seed against numpy, and the learned-seed solve against the
+plain solve on held-out well operators."""
+import os
+
+import numpy as np
+import pytest
+
+from nutrlan_b200 import operators as ops, DeviceOperator, solve
+from nutrlan_b200.seednet import SeedNet, seed_start, NOUT, WEIGHTS_PATH
+from oracle import seednet_np as sn
+
+pytestmark = pytest.mark.gpu
+
+H, W = 16, 64
+
+
+def _problem(seed, B=2):
+    rng = np.random.default_rng(seed)
+    V = (-50.0 * rng.random((B, H, W))).astype(np.float32)
+    U = np.stack([np.linalg.qr(rng.standard_normal((H * W, NOUT)))[0] for _ in range(B)]).astype(np.float32)
+    return V, U
+
+
+def _rel(a, b):
+    return np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-30)
+
+
+@pytest.fixture(scope="module")
+def net():
+    n = SeedNet(H, W, max_batch=4)
+    yield n
+    n.close()
+
+
+def test_forward_matches_oracle(net):
+    p = sn.init_params(1)
+    net.weights = p.astype(np.float32)
+    V, _ = _problem(2)
+    Y = net.forward(V)
+    _, Yo = sn.forward(p, V, emulate=True)
+    assert _rel(Y, Yo.reshape(Y.shape)) <= 2e-3
+    _, Y64 = sn.forward(p, V, emulate=False)
+    assert _rel(Y, Y64.reshape(Y.shape)) <= 3e-2
+
+
+@pytest.mark.parametrize("lam", [0.0, 1.0])
+def test_gradients_match_oracle(net, lam):
+    p = sn.init_params(3)
+    net.weights = p.astype(np.float32)
+    V, U = _problem(4, B=3)
+    loss, g = net.gradients(V, U, lam)
+    lo, go = sn.loss_and_grad(p, V, U, lam, emulate=True)
+    np.testing.assert_allclose(loss, lo, rtol=2e-3)
+    for l in range(5):
+        a, b = l * sn.LAYER_LEN, (l + 1) * sn.LAYER_LEN
+        wl = sn.TAPS * sn.NC * sn.NC
+        assert _rel(g[a:a + wl], go[a:a + wl]) <= 2e-2, ("weights", l)
+        assert _rel(g[a + wl:b], go[a + wl:b]) <= 2e-2, ("bias", l)
+    # Against the unrounded FP64 gradient (the true gradient of the loss).
+    _, g64 = sn.loss_and_grad(p, V, U, lam, emulate=False)
+    assert _rel(g, g64) <= 0.1
+
+
+def test_weights_roundtrip(net):
+    w = sn.init_params(9).astype(np.float32)
+    net.weights = w
+    np.testing.assert_array_equal(net.weights, w)
+
+
+def test_training_reduces_loss_on_eigenvectors():
+    # Real targets: the 16 lowest eigenvectors of small well operators.
+    import scipy.sparse.linalg as sla
+    L = 64
+    Vs, Us = [], []
+    for s in range(8):
+        A, V = ops.wells_2d(L, seed=500 + s)
+        w, U = sla.eigsh(A.to_scipy().tocsc(), k=NOUT, sigma=-60.0, which="LM")
+        Vs.append(V.astype(np.float32))
+        Us.append(U[:, np.argsort(w)].astype(np.float32))
+    V = np.stack(Vs)
+    U = np.stack(Us)
+    net = SeedNet(L, L, max_batch=8)
+    try:
+        first = net.train_step(V, U, lam=1.0, lr=2e-3).mean()
+        for _ in range(150):
+            last = net.train_step(V, U, lam=1.0, lr=2e-3).mean()
+        assert last < 0.7 * first, (first, last)
+    finally:
+        net.close()
+
+
+def test_seed_start_matches_numpy_rayleigh_ritz():
+    import torch
+    L = 64
+    A, V = ops.wells_2d(L, seed=77)
+    S = A.to_scipy().tocsr()
+    rng = np.random.default_rng(0)
+    Y = rng.standard_normal((A.n, NOUT)).astype(np.float32)
+    with DeviceOperator(A) as op:
+        start, theta, res = seed_start(op, Y)
+        Yd = torch.as_tensor(Y, device="cuda")
+        out = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+        start_d, theta_d, _ = seed_start(op, Yd, out=out)
+    Q = Y.astype(np.float64)
+    G = Q.T @ Q
+    lam, Wg = np.linalg.eigh(G)
+    B = Wg / np.sqrt(lam)
+    AQ = S @ Q
+    th, Z = np.linalg.eigh(B.T @ (Q.T @ AQ) @ B)
+    BZ = B @ Z
+    BZ *= np.sign(BZ[np.argmax(np.abs(BZ), axis=0), np.arange(NOUT)])
+    X = Q @ BZ
+    np.testing.assert_allclose(theta, th, rtol=1e-9, atol=1e-9)
+    np.testing.assert_allclose(start, X.sum(axis=1), rtol=1e-7, atol=1e-9)
+    r = np.linalg.norm(S @ X - X * th, axis=0)
+    np.testing.assert_allclose(res, r, rtol=1e-5, atol=1e-8)
+    np.testing.assert_allclose(start_d.cpu().numpy(), start, rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(theta_d, theta, rtol=1e-12)
+
+
+def test_seed_start_rejects_bad_arguments():
+    A = ops.laplacian_2d(16)
+    with DeviceOperator(A) as op:
+        with pytest.raises(ValueError):
+            seed_start(op, np.zeros((A.n + 1, NOUT), np.float32))
+        with pytest.raises(RuntimeError):
+            seed_start(op, np.zeros((A.n, NOUT), np.float32))   # numerically zero
+
+
+@pytest.mark.skipif(not os.path.exists(WEIGHTS_PATH), reason="trained weights not built")
+def test_learned_seed_against_plain_on_held_out_wells():
+    """Trained network on held-out operators: the seeded solve returns the
+    plain solve's eigenvalues (1e-10 relative) with true residuals <= tol *
+    ||A||, and needs fewer matvecs on average (the 16 applications of the
+    Rayleigh-Ritz projection included)."""
+    from nutrlan_b200.seed_train import evaluate
+    net = SeedNet.pretrained()
+    try:
+        recs = evaluate(net, range(2 * 10 ** 6, 2 * 10 ** 6 + 6), log=lambda *a: None)
+    finally:
+        net.close()
+    for r in recs:
+        assert r["plain_nec"] >= NOUT and r["seeded_nec"] >= NOUT, r
+        assert r["eval_rel_diff"] <= 1e-10, r
+        assert r["max_true_res"] <= 1.01 * r["tol_abs"], r
+    plain = np.mean([r["plain_matvec"] for r in recs])
+    seeded = np.mean([r["seeded_matvec"] for r in recs])
+    assert seeded < plain, (plain, seeded)
