@@ -170,7 +170,8 @@ void trlx_batch_destroy(trlx_batch *b);
  * 1, 2, 4, 8, 1; channels 1 -> 32 -> 32 -> 32 -> 32 -> 16; ReLU after the
  * first four layers; zero "same" padding) mapping a potential V on an
  * H x W grid to 16 vectors whose span approximates the lowest eigenvectors
- * of -Laplacian + V.  BF16 activations and weights, FP32 accumulation on the
+ * of -Laplacian + V.  The input is (V - min V) / 50 per sample.  BF16
+ * activations and weights, FP32 accumulation on the
  * tensor cores, FP32 master weights updated by Adam.  Training minimises
  * per sample  sum_k (1 - |U^T y_k|^2 / |y_k|^2)
  *           + lam * sum_{j != k} (y_j . y_k)^2 / (|y_j|^2 |y_k|^2)
@@ -204,19 +205,20 @@ int trlx_seednet_get_weights(trlx_seednet *net, float *out);
 int trlx_seednet_set_weights(trlx_seednet *net, const float *in);
 int trlx_seednet_num_params(void);
 
-/* Rayleigh-Ritz start vector from a predicted subspace: Y (nrow x k FP32,
-   [site][vector], host or device, 1 <= k <= 32) is orthonormalised in FP64
-   (numerically dependent directions dropped), projected on the built-in
-   operator op (k applications), and start (nrow doubles, host or device)
-   receives the sum of the resulting Ritz vectors.  theta and res (k doubles,
-   host, optional) receive the Ritz values (ascending) and the residual norms
-   |A x - theta x| (-1 for dropped directions).  Pass start to trlan() with
-   trl_set_iguess(info, 0, 1, 0, NULL) and start in the first column of evec.
-   Returns the number of Ritz vectors (>= 1) or -1 (bad arguments), -5
-   (device allocation), -234 (Y numerically zero), -1001 (CUDA).  No
-   counterpart in the reference. */
-int trlx_seed_start(void *op, int nrow, int k, const float *Y, double *start,
-                    double *theta, double *res);
+/* Start vector from a predicted subspace Y (nrow x k FP32, [site][vector],
+   host or device, 1 <= k <= 32).  project = 1: Rayleigh-Ritz -- Y is
+   orthonormalised in FP64 (numerically dependent directions dropped) and
+   projected on the built-in operator op (k applications); start (nrow
+   doubles, host or device) receives the sum of the Ritz vectors, theta and
+   res (k doubles, host, optional) the Ritz values (ascending) and residual
+   norms |A x - theta x| (-1 for dropped directions).  project = 0: start =
+   sum of the normalised columns of Y, no operator application (theta 0,
+   res -1).  Pass start to trlan() with trl_set_iguess(info, 0, 1, 0, NULL)
+   and start in the first column of evec.  Returns the number of vectors
+   used (>= 1) or -1 (bad arguments), -5 (device allocation), -234 (Y
+   numerically zero), -1001 (CUDA).  No counterpart in the reference. */
+int trlx_seed_start(void *op, int nrow, int k, const float *Y, int project,
+                    double *start, double *theta, double *res);
 
 /* Statistics of the last solve issued from the calling thread. */
 typedef struct {

@@ -11,6 +11,8 @@
 // columns of Q is positive).  The thick-restart solver takes it through its ordinary
 // start-vector channel (trl_set_iguess with guess = 1), so the Lanczos
 // recurrence and the convergence test are exactly those of a plain solve.
+// With project = 0 the start vector is the sum of the normalised columns of
+// Y and the operator is not applied.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -142,9 +144,36 @@ bool is_device(const void *p) {
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// start = sum_i y_i / |y_i| over the columns that are not zero (no
+// operator applications).
+int normalized_sum(SeedWork &w, long n, int k, const double *gram, double *start, double *theta, double *res) {
+    std::vector<double> coef(k, 0.0);
+    double gmax = 0.0;
+    for (int i = 0; i < k; ++i) gmax = std::max(gmax, gram[i * k + i]);
+    if (!(gmax > 0.0)) return -234;
+    int r = 0;
+    for (int i = 0; i < k; ++i) {
+        const double g = gram[i * k + i];
+        if (g > 1e-24 * gmax) {
+            coef[i] = 1.0 / std::sqrt(g);
+            ++r;
+        }
+        if (theta) theta[i] = 0.0;
+        if (res) res[i] = -1.0;
+    }
+    if (cudaMemcpy(w.coef, coef.data(), sizeof(double) * k, cudaMemcpyHostToDevice) != cudaSuccess) return -1001;
+    double *out = is_device(start) ? start : w.start;
+    k_combine<<<(int)std::min<long>(148 * 8, (n + 255) / 256), 256>>>(w.Q, n, k, w.coef, out);
+    if (out != start && cudaMemcpy(start, out, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -1001;
+    if (cudaDeviceSynchronize() != cudaSuccess) return -1001;
+    return r;
+}
+
 }  // namespace
 
-extern "C" int trlx_seed_start(void *op, int nrow, int k, const float *Y, double *start, double *theta, double *res) {
+extern "C" int trlx_seed_start(void *op, int nrow, int k, const float *Y, int project, double *start, double *theta,
+                               double *res) {
     auto *A = static_cast<trlx_operator *>(op);
     if (!A || !Y || !start || k < 1 || k > kMaxK || nrow < k || A->nrow != nrow || A->kind == 2) return -1;
     SeedWork &w = g_work;
@@ -157,16 +186,19 @@ extern "C" int trlx_seed_start(void *op, int nrow, int k, const float *Y, double
     }
     const int eb = (int)std::min<long>(148 * 8, (n * k + 255) / 256);
     k_gather_cols<<<eb, 256>>>(Yd, n, k, w.Q);
-    for (int c = 0; c < k; ++c) trlb::spmv_plain(A, w.Q + (long)c * n, w.AQ + (long)c * n, 0);
+    if (project)
+        for (int c = 0; c < k; ++c) trlb::spmv_plain(A, w.Q + (long)c * n, w.AQ + (long)c * n, 0);
     const long chunk = (n + w.nb - 1) / w.nb;
     const int kk = k * k;
     const double *pairs[3][2] = {{w.Q, w.Q}, {w.Q, w.AQ}, {w.AQ, w.AQ}};
-    for (int m = 0; m < 3; ++m) {
+    for (int m = 0; m < (project ? 3 : 1); ++m) {
         k_xtz<<<w.nb, 256>>>(pairs[m][0], pairs[m][1], n, k, chunk, w.part);
         k_sum_parts<<<(kk + 255) / 256, 256>>>(w.part, w.nb, kk, w.gram + (long)m * kk);
     }
     std::vector<double> h(3 * kk);
-    if (cudaMemcpy(h.data(), w.gram, sizeof(double) * 3 * kk, cudaMemcpyDeviceToHost) != cudaSuccess) return -1001;
+    if (cudaMemcpy(h.data(), w.gram, sizeof(double) * (project ? 3 : 1) * kk, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -1001;
+    if (!project) return normalized_sum(w, n, k, h.data(), start, theta, res);
     // Row-major part[i*k+j] = X_i . Z_j; the Gram matrices are symmetric in
     // exact arithmetic: symmetrise G and H.
     std::vector<double> G(kk), H(kk), M(kk);

@@ -376,11 +376,29 @@ __global__ void k_pack(const float *w, __nv_bfloat16 *wf, __nv_bfloat16 *wb) {
     }
 }
 
-// Input packing: V (FP32, [b][y][x]) * scale into channel 0 of NHWC bf16.
-__global__ void k_pack_input(const float *V, long P, float scale, __nv_bfloat16 *x) {
+// Minimum of each sample's potential (one block per sample).
+__global__ void __launch_bounds__(1024) k_sample_min(const float *V, int HW, float *vmin) {
+    __shared__ float red[32];
+    const float *v = V + (long)blockIdx.x * HW;
+    float m = INFINITY;
+    for (int i = threadIdx.x; i < HW; i += blockDim.x) m = fminf(m, v[i]);
+    for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : INFINITY;
+        for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) vmin[blockIdx.x] = m;
+    }
+}
+
+// Input packing: (V - min V) * scale (FP32, per sample) into channel 0 of
+// NHWC bf16.  Measuring the potential from its global minimum makes "the
+// lowest states" a local property the convolutions can see.
+__global__ void k_pack_input(const float *V, const float *vmin, int HW, long P, float scale, __nv_bfloat16 *x) {
     for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (long)gridDim.x * blockDim.x) {
         unsigned *o = reinterpret_cast<unsigned *>(x) + p * (kC / 2);
-        o[0] = pack_bf16(V[p] * scale, 0.f);
+        o[0] = pack_bf16((V[p] - vmin[p / HW]) * scale, 0.f);
         for (int k = 1; k < kC / 2; ++k) o[k] = 0u;
     }
 }
@@ -407,7 +425,7 @@ struct trlx_seednet {
     float *Y = nullptr;                           // network output [P][16]
     float *part = nullptr;
     size_t part_len = 0;
-    float *coef = nullptr, *loss = nullptr, *Vd = nullptr, *Ud = nullptr;
+    float *coef = nullptr, *loss = nullptr, *Vd = nullptr, *Ud = nullptr, *vmin = nullptr;
     int step = 0;
 };
 
@@ -417,6 +435,12 @@ int blocks_for(long n, int t = 256) { return (int)std::min<long>((n + t - 1) / t
 
 void pack_layer(trlx_seednet *net, int l) {
     k_pack<<<36, 256>>>(net->w[l], net->wf[l], net->wb[l]);
+}
+
+void pack_input(trlx_seednet *net, int B) {
+    const int HW = net->H * net->W;
+    k_sample_min<<<B, 1024>>>(net->Vd, HW, net->vmin);
+    k_pack_input<<<blocks_for((long)B * HW), 256>>>(net->Vd, net->vmin, HW, (long)B * HW, net->in_scale, net->act[0]);
 }
 
 // Forward pass for B samples already packed in act[0]; output in net->Y.
@@ -495,6 +519,7 @@ int trlx_seednet_create(int H, int W, int max_batch, unsigned long long seed, tr
     alloc((void **)&net->coef, (size_t)max_batch * 512 * 4);
     alloc((void **)&net->loss, (size_t)max_batch * 4);
     alloc((void **)&net->Vd, (size_t)P * 4);
+    alloc((void **)&net->vmin, (size_t)max_batch * 4);
     alloc((void **)&net->Ud, (size_t)P * kOut * 4);
     if (!ok) {
         trlx_seednet_destroy(net);
@@ -529,6 +554,7 @@ void trlx_seednet_destroy(trlx_seednet *net) {
     cudaFree(net->coef);
     cudaFree(net->loss);
     cudaFree(net->Vd);
+    cudaFree(net->vmin);
     cudaFree(net->Ud);
     delete net;
 }
@@ -539,7 +565,7 @@ int trlx_seednet_forward(trlx_seednet *net, int B, const float *V, float *out) {
     if (!net || B < 1 || B > net->Bmax || !V) return -1;
     const long P = (long)B * net->H * net->W;
     if (cudaMemcpy(net->Vd, V, P * 4, cudaMemcpyDefault) != cudaSuccess) return -1001;
-    k_pack_input<<<blocks_for(P), 256>>>(net->Vd, P, net->in_scale, net->act[0]);
+    pack_input(net, B);
     forward(net, B);
     if (out && cudaMemcpy(out, net->Y, P * kOut * 4, cudaMemcpyDefault) != cudaSuccess) return -1001;
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1001;
@@ -553,7 +579,7 @@ static int loss_and_grad(trlx_seednet *net, int B, const float *V, const float *
     const long P = (long)B * HW;
     if (cudaMemcpy(net->Vd, V, P * 4, cudaMemcpyDefault) != cudaSuccess) return -1001;
     if (cudaMemcpy(net->Ud, U, P * kOut * 4, cudaMemcpyDefault) != cudaSuccess) return -1001;
-    k_pack_input<<<blocks_for(P), 256>>>(net->Vd, P, net->in_scale, net->act[0]);
+    pack_input(net, B);
     forward(net, B);
     const int nch = (HW + kLossPix - 1) / kLossPix;
     k_loss_stats<<<dim3(nch, B), 256>>>(net->Y, net->Ud, HW, net->part);

@@ -9,14 +9,15 @@ depths uniform[5, 50]).
 * ``train``: Adam on the subspace loss through the library's own BF16
   forward/backward kernels.
 * ``evaluate``: for held-out seeds, the plain solve (seeded uniform start)
-  against the learned-seed solve (network forward + Rayleigh-Ritz start,
-  both timed inside the seeded solve's wall time), same operator, same
-  solver options.
+  against the learned-seed solves (network forward and the start vector
+  built from it timed inside the seeded solve's wall time), same operator,
+  same solver options.
 
 Run ``python -m nutrlan_b200.seed_train --help``.
 """
 import argparse
 import json
+import os
 import time
 
 import numpy as np
@@ -76,7 +77,7 @@ def generate(count, L=256, seed0=1, ned=NOUT, maxlan=48, tol=1e-8, chunk=1024, l
     return Vall, Uall, info
 
 
-def train(net, V, U, epochs=10, batch=32, lr=2e-3, lr_min=1e-4, lam=1.0, holdout=256, log=print):
+def train(net, V, U, epochs=30, batch=32, lr=2e-3, lr_min=1e-4, lam=0.1, holdout=256, log=print):
     """Adam with a cosine learning-rate schedule; the last ``holdout``
     samples are kept for validation.  Returns a list of per-epoch records."""
     import torch
@@ -117,49 +118,66 @@ def validate(net, V, U, batch=32, lam=1.0):
 
 
 def evaluate(net, seeds, L=256, ned=NOUT, maxlan=48, tol=1e-8, restart=1, log=print):
-    """Plain vs learned-seed solves on held-out operators; returns one record
-    per seed with matvecs, wall seconds, eigenvalue agreement and the true
-    residuals of the seeded solve."""
+    """Plain vs learned-seed solves on held-out operators.  Per seed: the
+    plain solve (seeded uniform start), the seed injected as the sum of its
+    Rayleigh-Ritz vectors ("rr", its NOUT projection matvecs counted) and as
+    the sum of the normalised network outputs ("sum"); matvecs, wall seconds
+    (network forward and projection inside the seeded times), eigenvalue
+    agreement with the plain solve and true residuals of the seeded ones."""
     import torch
+    from .solver import residual_norms
     out = []
     Y = torch.empty((1, L * L, NOUT), dtype=torch.float32, device="cuda")
+    kw = dict(ned=ned, maxlan=maxlan, tol=tol, restart=restart, maxmv=100000, device=True)
     for s in seeds:
         A, V = ops.wells_2d(L, seed=int(s))
+        rec = dict(seed=int(s))
         with DeviceOperator(A) as op:
             x0 = torch.as_tensor(ops.start_vector(A.n), device="cuda")
             ev = torch.zeros((ned + 1, A.n), dtype=torch.float64, device="cuda")
-            # warm the operator / workspace once (not timed)
-            solve(op, ned=ned, maxlan=maxlan, tol=tol, restart=restart, maxmv=100000, start=x0,
-                  device=True, evec=ev)
+            solve(op, start=x0, evec=ev, **kw)          # warm-up, not timed
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            rp = solve(op, ned=ned, maxlan=maxlan, tol=tol, restart=restart, maxmv=100000, start=x0,
-                       device=True, evec=ev)
+            rp = solve(op, start=x0, evec=ev, **kw)
             torch.cuda.synchronize()
-            tp = time.perf_counter() - t0
+            rec.update(plain_matvec=int(rp.info.matvec), plain_s=time.perf_counter() - t0, plain_nec=int(rp.nec))
+            ep_ = np.sort(rp.eval[:min(rp.nec, ned)])
             Vd = torch.as_tensor(V, dtype=torch.float32, device="cuda")[None]
-            ev2 = torch.zeros((ned + 1, A.n), dtype=torch.float64, device="cuda")
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            net.forward(Vd, out=Y)
-            _, theta, sres = seed_start(op, Y[0], out=ev2[0])
-            rs = solve(op, ned=ned, maxlan=maxlan, tol=tol, restart=restart, maxmv=100000, start=ev2[0],
-                       device=True, evec=ev2)
-            torch.cuda.synchronize()
-            ts = time.perf_counter() - t0
-            from .solver import residual_norms
-            nec = min(rp.nec, rs.nec, ned)
-            true_res = residual_norms(op, rs.eval[:nec], ev2[:nec])
-            ep_, es_ = np.sort(rp.eval[:nec]), np.sort(rs.eval[:nec])
-            rel = np.max(np.abs(es_ - ep_) / np.abs(ep_)) if nec else np.inf
-        rec = dict(seed=int(s), plain_matvec=int(rp.info.matvec), seeded_matvec=int(rs.info.matvec) + NOUT,
-                   plain_s=tp, seeded_s=ts, plain_nec=int(rp.nec), seeded_nec=int(rs.nec),
-                   eval_rel_diff=float(rel), max_true_res=float(true_res.max()) if nec else np.inf,
-                   tol_abs=tol * float(rs.info.anrm), seed_res_median=float(np.median(sres)))
+            for mode, project in (("rr", True), ("sum", False)):
+                ev2 = torch.zeros((ned + 1, A.n), dtype=torch.float64, device="cuda")
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                net.forward(Vd, out=Y)
+                _, theta, sres = seed_start(op, Y[0], out=ev2[0], project=project)
+                rs = solve(op, start=ev2[0], evec=ev2, **kw)
+                torch.cuda.synchronize()
+                ts = time.perf_counter() - t0
+                nec = min(rp.nec, rs.nec, ned)
+                true_res = residual_norms(op, rs.eval[:nec], ev2[:nec])
+                es_ = np.sort(rs.eval[:nec])
+                rel = float(np.max(np.abs(es_ - ep_[:nec]) / np.abs(ep_[:nec]))) if nec else np.inf
+                rec.update({f"{mode}_matvec": int(rs.info.matvec) + (NOUT if project else 0),
+                            f"{mode}_s": ts, f"{mode}_nec": int(rs.nec), f"{mode}_eval_rel_diff": rel,
+                            f"{mode}_max_true_res": float(true_res.max()) if nec else np.inf})
+                if project:
+                    rec["seed_res_median"] = float(np.median(sres))
+            rec["tol_abs"] = tol * float(rp.info.anrm)
         out.append(rec)
-        log(f"eval seed {s}: plain {rec['plain_matvec']} mv {tp * 1e3:.1f} ms, seeded "
-            f"{rec['seeded_matvec']} mv (incl. {NOUT} for the projection) {ts * 1e3:.1f} ms, "
-            f"eig rel diff {rel:.1e}, seed residual median {rec['seed_res_median']:.2e}")
+        log(f"eval seed {s}: plain {rec['plain_matvec']} mv {rec['plain_s'] * 1e3:.1f} ms | rr "
+            f"{rec['rr_matvec']} mv (incl. {NOUT} projection) {rec['rr_s'] * 1e3:.1f} ms | sum "
+            f"{rec['sum_matvec']} mv {rec['sum_s'] * 1e3:.1f} ms | seed residual median "
+            f"{rec['seed_res_median']:.2e}")
+    return out
+
+
+def summarize(recs):
+    m = lambda k: float(np.mean([r[k] for r in recs]))
+    out = dict(problems=len(recs), plain_matvec=m("plain_matvec"), plain_s=m("plain_s"))
+    for mode in ("rr", "sum"):
+        out[f"{mode}_matvec"] = m(f"{mode}_matvec")
+        out[f"{mode}_s"] = m(f"{mode}_s")
+        out[f"{mode}_matvec_ratio"] = out["plain_matvec"] / out[f"{mode}_matvec"]
+        out[f"{mode}_time_ratio"] = out["plain_s"] / out[f"{mode}_s"]
     return out
 
 
@@ -167,10 +185,10 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--samples", type=int, default=20000)
     ap.add_argument("--L", type=int, default=256)
-    ap.add_argument("--epochs", type=int, default=10)
+    ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--lr", type=float, default=2e-3)
-    ap.add_argument("--lam", type=float, default=1.0)
+    ap.add_argument("--lam", type=float, default=0.1)
     ap.add_argument("--maxlan", type=int, default=48)
     ap.add_argument("--eval", type=int, default=16, help="held-out operators for the A/B test")
     ap.add_argument("--weights", default=WEIGHTS_PATH)
@@ -189,16 +207,12 @@ def main(argv=None):
     t0 = time.perf_counter()
     rep["train"] = train(net, V, U, epochs=a.epochs, batch=a.batch, lr=a.lr, lam=a.lam)
     rep["train_seconds"] = time.perf_counter() - t0
+    os.makedirs(os.path.dirname(os.path.abspath(a.weights)), exist_ok=True)
     net.save(a.weights)
     del V, U
     ev = evaluate(net, range(10 ** 6, 10 ** 6 + a.eval), a.L, maxlan=a.maxlan)
     rep["eval"] = ev
-    pm = np.mean([r["plain_matvec"] for r in ev])
-    sm = np.mean([r["seeded_matvec"] for r in ev])
-    ps = np.mean([r["plain_s"] for r in ev])
-    ss = np.mean([r["seeded_s"] for r in ev])
-    rep["summary"] = dict(plain_matvec=pm, seeded_matvec=sm, matvec_ratio=pm / sm, plain_s=ps, seeded_s=ss,
-                          time_ratio=ps / ss)
+    rep["summary"] = summarize(ev)
     print(json.dumps(rep["summary"]))
     if a.report:
         with open(a.report, "w") as f:

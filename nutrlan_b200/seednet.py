@@ -40,7 +40,7 @@ def _declare(lib):
     lib.trlx_seednet_get_weights.argtypes = [vp, vp]
     lib.trlx_seednet_set_weights.argtypes = [vp, vp]
     lib.trlx_seednet_num_params.argtypes = []
-    lib.trlx_seed_start.argtypes = [vp, i, i, vp, vp, vp, vp]
+    lib.trlx_seed_start.argtypes = [vp, i, i, vp, i, vp, vp, vp]
     return lib
 
 
@@ -150,11 +150,13 @@ class SeedNet:
             pass
 
 
-def seed_start(op, Y, out=None):
-    """Rayleigh-Ritz start vector from a predicted subspace Y ((n, k) float32,
-    numpy or CUDA tensor) on the DeviceOperator `op`.  Returns (start, theta,
-    res): start is `out` (n doubles, numpy or CUDA tensor) or a new numpy
-    array; theta/res are the Ritz values and residual norms."""
+def seed_start(op, Y, out=None, project=True):
+    """Start vector from a predicted subspace Y ((n, k) float32, numpy or
+    CUDA tensor) on the DeviceOperator `op`: the sum of its Rayleigh-Ritz
+    vectors (project=True, k operator applications) or of its normalised
+    columns (project=False).  Returns (start, theta, res): start is `out`
+    (n doubles, numpy or CUDA tensor) or a new numpy array; theta/res are the
+    Ritz values and residual norms (zeros / -1 without projection)."""
     lib = _declare(load())
     n = op.n
     k = Y.shape[-1]
@@ -164,7 +166,7 @@ def seed_start(op, Y, out=None):
     po, _ = _ptr(out, np.float64, (n,), output=True)
     theta = np.zeros(k)
     res = np.zeros(k)
-    r = lib.trlx_seed_start(op.handle, n, k, py, po, theta.ctypes.data, res.ctypes.data)
+    r = lib.trlx_seed_start(op.handle, n, k, py, 1 if project else 0, po, theta.ctypes.data, res.ctypes.data)
     if r < 1:
         raise RuntimeError(f"trlx_seed_start failed ({r})")
     return out, theta[:r], res[:r]
