@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstring>
 #include <type_traits>
+#include <numeric>
 #include <vector>
 
 #include "../kernels/lanczos_kernels.h"
@@ -60,6 +61,8 @@ struct Workspace {
     size_t partial_bytes = 0;
     void *out = nullptr;  // staging of final eigenvectors for host evec
     size_t out_bytes = 0;
+    void *refine = nullptr;  // FP64 refinement blocks (32-bit bases)
+    size_t refine_bytes = 0;
     unsigned *tickets = nullptr;
     double *h_scal = nullptr;
     int device = -1;
@@ -70,10 +73,11 @@ struct Workspace {
         cudaFree(small);
         cudaFree(partials);
         cudaFree(out);
+        cudaFree(refine);
         cudaFree(tickets);
         cudaFreeHost(h_scal);
-        pool = fbuf = small = partials = out = nullptr;
-        out_bytes = 0;
+        pool = fbuf = small = partials = out = refine = nullptr;
+        out_bytes = refine_bytes = 0;
         tickets = nullptr;
         h_scal = nullptr;
         pool_bytes = fbuf_bytes = small_bytes = partial_bytes = 0;
@@ -214,6 +218,13 @@ class Engine {
     int initial_guess(int *jnd);
     int restart_ritz(int locked, int jml, int kept, int jnd);
     int final_vectors(int jnd, int kept);
+    int refine_fp64(int k, double *max_res);
+    void track_ritz(int nd) {
+        for (int i = 0; i < nd; ++i) {
+            ritz_min_ = std::min(ritz_min_, lambda_[i]);
+            ritz_max_ = std::max(ritz_max_, lambda_[i]);
+        }
+    }
     void log_progress();
     void release();
     void count_launch(int k = 1) { launches_ += k; }
@@ -259,6 +270,7 @@ class Engine {
     // host state (reference names)
     std::vector<double> alpha_, beta_, alfrot_, betrot_, rot_, lambda_, res_, yy_, wrk2_;
     int final_j1_ = 0;
+    double ritz_min_ = 1e300, ritz_max_ = -1e300;  // extreme Ritz values seen (spectrum bounds)
     long long launches_ = 0;
     int syncs_ = 0;
     double t_op_ = 0, t_orth_ = 0, t_res_ = 0;
@@ -818,6 +830,194 @@ int Engine<T>::final_vectors(int jnd, int kept) {
     return 0;
 }
 
+// FP64 refinement of the k converged pairs (real problems).  The converged
+// Ritz vectors of a 32-bit basis carry the basis' rounding noise, which is
+// spread over the whole spectrum; most of its residual comes from the
+// upper part.  Each vector is passed through a scaled Chebyshev filter of
+// degree kChebDegree that damps [a, b] (a = the far end of the wanted
+// Ritz values + 10% of the distance to the far spectrum bound, b = that
+// bound, both from the Ritz values seen during the solve), then a
+// Rayleigh-Ritz projection in FP64 over the filtered block gives the pairs
+// and their true residuals |A x - theta x|.  Repeated (at most kRefinePasses
+// times) until every residual is <= tol * anrm.  Operator applications are
+// counted in info->matvec.
+template <class T>
+int Engine<T>::refine_fp64(int k, double *max_res) {
+    if constexpr (kComplex) {
+        (void)k;
+        (void)max_res;
+        return 0;
+    } else {
+        constexpr int kChebDegree = 8;
+        constexpr int kRefinePasses = 3;
+        trl_info *info = info_;
+        if (k <= 0 || !(ritz_max_ > ritz_min_)) return 0;
+        const bool low = info->lohi < 0;
+        // Wanted Ritz values and the damped interval.
+        double th_lo = eval_[0], th_hi = eval_[0];
+        for (int i = 1; i < k; ++i) {
+            th_lo = std::min(th_lo, eval_[i]);
+            th_hi = std::max(th_hi, eval_[i]);
+        }
+        double a, b, ref;
+        if (low) {
+            const double top = ritz_max_ + 0.01 * (ritz_max_ - th_lo);
+            a = th_hi + 0.1 * (top - th_hi);
+            b = top;
+            ref = th_lo;
+        } else {
+            const double bot = ritz_min_ - 0.01 * (th_hi - ritz_min_);
+            a = bot;
+            b = th_lo - 0.1 * (th_lo - bot);
+            ref = th_hi;
+        }
+        if (!(b > a)) return 0;
+        const double e = 0.5 * (b - a), c = 0.5 * (b + a);
+        const double sigma1 = e / (ref - c);
+
+        Workspace &ws = workspace();
+        const size_t vec = (size_t)n_pad_;
+        const size_t kk = (size_t)k * k;
+        const size_t doubles = (2 * (size_t)k + 4) * vec + 3 * kk + 2 * kk + (size_t)k + 8 + 3 * (size_t)k;
+        if (!Workspace::ensure(&ws.refine, &ws.refine_bytes, doubles * sizeof(double))) return -5;
+        double *base = static_cast<double *>(ws.refine);
+        CK(cudaMemsetAsync(base, 0, doubles * sizeof(double), st_));
+        double *Wb = base, *AWb = Wb + k * vec, *y0 = AWb + k * vec, *y1 = y0 + vec, *ay = y1 + vec,
+               *zero = ay + vec;
+        double *dG = zero + vec, *dH = dG + kk, *dC = dH + kk, *dh = dC + kk, *dr2 = dh + 2 * kk,
+               *dout2 = dr2 + k, *dtab = dout2 + 8;  // 3k pointer slots: W columns, then [AW W] columns
+        double **tabW = reinterpret_cast<double **>(dtab);
+        double **tabAWW = tabW + k;
+        std::vector<double *> htab(3 * (size_t)k);
+        for (int j = 0; j < k; ++j) {
+            htab[j] = Wb + j * vec;
+            htab[k + j] = AWb + j * vec;
+            htab[2 * k + j] = Wb + j * vec;
+        }
+        CK(cudaMemcpyAsync(tabW, htab.data(), sizeof(double *) * 3 * k, cudaMemcpyHostToDevice, st_));
+        // Converged vectors: the caller's device evec or the host staging.
+        double *X = user_dev_ ? reinterpret_cast<double *>(evec_) : static_cast<double *>(workspace().out);
+        const long ldx = user_dev_ ? lde_ : n_pad_;
+        CK(cudaMemcpy2DAsync(Wb, vec * sizeof(double), X, ldx * sizeof(double), nrow_ * sizeof(double), k,
+                             cudaMemcpyDeviceToDevice, st_));
+        const double tol_abs = info->tol * std::max(info->anrm, 1e-300);
+        std::vector<double> G(kk), H(kk), th, Cm, r2(k);
+        std::vector<int> perm(k);
+        std::iota(perm.begin(), perm.end(), 0);
+        std::stable_sort(perm.begin(), perm.end(), [&](int i, int j) { return eval_[i] < eval_[j]; });
+        double worst = -1.0;
+        bool refined = false;
+        for (int pass = 0; pass < kRefinePasses; ++pass) {
+            for (int j = 0; j < k; ++j) {
+                double *w = Wb + j * vec;
+                // Scaled Chebyshev filter (Zhou & Saad): the wanted end keeps
+                // magnitude ~1, [a, b] is damped by ~1/T_d.
+                int rc = apply_op(w, ay, false);
+                if (rc) return rc;
+                launch_cheb(ay, w, nullptr, n_pad_, sigma1 / e, c, 0.0, y1, st_);
+                const double *prev = w;
+                double *cur = y1, *spare = y0;
+                double s1 = sigma1;
+                for (int t = 2; t <= kChebDegree; ++t) {
+                    const double s2 = 1.0 / (2.0 / sigma1 - s1);
+                    if ((rc = apply_op(cur, ay, false))) return rc;
+                    double *out = prev == w ? spare : const_cast<double *>(prev);
+                    launch_cheb(ay, cur, prev, n_pad_, 2.0 * s2 / e, c, -s1 * s2, out, st_);
+                    prev = cur;
+                    cur = out;
+                    s1 = s2;
+                }
+                CK(cudaMemcpyAsync(w, cur, vec * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+                if ((rc = apply_op(w, AWb + j * vec, false))) return rc;
+                count_launch(kChebDegree);
+            }
+            // Gram matrix and projection: columns of W^T W and W^T A W.
+            for (int j = 0; j < k; ++j) {
+                launch_project<double>(tabW, k, n_pad_, Wb + j * vec, Recur<double>{}, dG + (size_t)j * k, dout2,
+                                       scratch_, st_);
+                launch_project<double>(tabW, k, n_pad_, AWb + j * vec, Recur<double>{}, dH + (size_t)j * k, dout2,
+                                       scratch_, st_);
+            }
+            count_launch(2 * k);
+            CK(cudaMemcpyAsync(G.data(), dG, sizeof(double) * kk, cudaMemcpyDeviceToHost, st_));
+            CK(cudaMemcpyAsync(H.data(), dH, sizeof(double) * kk, cudaMemcpyDeviceToHost, st_));
+            CK(cudaStreamSynchronize(st_));
+            ++syncs_;
+            for (int i = 0; i < k; ++i)
+                for (int j = 0; j < i; ++j) {
+                    G[i + j * k] = G[j + i * k] = 0.5 * (G[i + j * k] + G[j + i * k]);
+                    H[i + j * k] = H[j + i * k] = 0.5 * (H[i + j * k] + H[j + i * k]);
+                }
+            // G = Q diag(g) Q^T; B = Q g^{-1/2}; (B^T H B) Z = Z diag(theta).
+            // A filtered block that lost rank keeps the pairs of the last
+            // completed pass (or the unrefined ones).
+            std::vector<double> gl(k);
+            if (sym_eig(k, G.data(), k, gl.data()) || !(gl[0] > 1e-14 * gl[k - 1])) break;
+            std::vector<double> B(kk), P(kk), HB(kk);
+            for (int cc = 0; cc < k; ++cc)
+                for (int i = 0; i < k; ++i) B[i + cc * k] = G[i + cc * k] / std::sqrt(gl[cc]);
+            for (int cc = 0; cc < k; ++cc)
+                for (int i = 0; i < k; ++i) {
+                    double acc = 0.0;
+                    for (int j = 0; j < k; ++j) acc += H[i + j * k] * B[j + cc * k];
+                    HB[i + cc * k] = acc;
+                }
+            for (int i = 0; i < k; ++i)
+                for (int cc = 0; cc <= i; ++cc) {
+                    double acc = 0.0;
+                    for (int j = 0; j < k; ++j) acc += B[j + i * k] * HB[j + cc * k];
+                    P[i + cc * k] = P[cc + i * k] = acc;
+                }
+            th.assign(k, 0.0);
+            if (sym_eig(k, P.data(), k, th.data())) break;
+            // Coefficients of the refined vectors, placed so that the i-th
+            // smallest refined value lands where the i-th smallest of the
+            // solver's values was.
+            Cm.assign(kk, 0.0);
+            std::vector<double> hv(2 * kk);
+            for (int i = 0; i < k; ++i) {
+                const int dst = perm[i];
+                for (int r = 0; r < k; ++r) {
+                    double acc = 0.0;
+                    for (int q = 0; q < k; ++q) acc += B[r + q * k] * P[q + i * k];
+                    Cm[r + (size_t)dst * k] = acc;
+                    hv[(size_t)dst * 2 * k + r] = -acc;              // AW part
+                    hv[(size_t)dst * 2 * k + k + r] = th[i] * acc;   // W part
+                }
+                eval_[dst] = th[i];
+            }
+            CK(cudaMemcpyAsync(dC, Cm.data(), sizeof(double) * kk, cudaMemcpyHostToDevice, st_));
+            CK(cudaMemcpyAsync(dh, hv.data(), sizeof(double) * 2 * kk, cudaMemcpyHostToDevice, st_));
+            launch_ritz_out<double>(tabW, k, n_pad_, dC, k, k, X, ldx, nrow_, st_);
+            // r_c = 0 - [AW W] h_c = AW C_c - theta_c W C_c, |r_c|^2 -> dr2[c].
+            for (int cc = 0; cc < k; ++cc)
+                launch_update<double>(tabAWW, 2 * k, n_pad_, zero, Recur<double>{}, dh + (size_t)cc * 2 * k, ay,
+                                      dr2 + cc, scratch_, st_);
+            count_launch(k + 1);
+            CK(cudaMemcpyAsync(r2.data(), dr2, sizeof(double) * k, cudaMemcpyDeviceToHost, st_));
+            CK(cudaStreamSynchronize(st_));
+            ++syncs_;
+            worst = 0.0;
+            for (int i = 0; i < k; ++i) {
+                beta_[i] = std::sqrt(std::max(r2[i], 0.0));
+                worst = std::max(worst, beta_[i]);
+            }
+            refined = true;
+            if (worst <= tol_abs || pass + 1 == kRefinePasses) break;
+            CK(cudaMemcpy2DAsync(Wb, vec * sizeof(double), X, ldx * sizeof(double), nrow_ * sizeof(double), k,
+                                 cudaMemcpyDeviceToDevice, st_));
+        }
+        if (!refined) return 0;
+        if (!user_dev_) {
+            const size_t ue = sizeof(User);
+            CK(cudaMemcpy2DAsync(evec_, ue * lde_, X, ue * n_pad_, ue * nrow_, k, cudaMemcpyDeviceToHost, st_));
+            CK(cudaStreamSynchronize(st_));
+        }
+        *max_res = worst;
+        return 0;
+    }
+}
+
 template <class T>
 void Engine<T>::log_progress() {
     if (info_->verbose <= 0) return;
@@ -956,6 +1156,7 @@ void Engine<T>::run() {
             if (info->matvec >= next_test) {
                 if ((stat = get_eval(jnd, locked, alfrot_.data(), betrot_.data(), lambda_.data(), res_.data())))
                     break;
+                track_ritz(jnd);
                 const int ne = std::min(mev_, jnd);
                 std::memcpy(eval_, lambda_.data(), sizeof(double) * ne);
                 convergence_test(jnd, lambda_.data(), res_.data(), info, wrk2_.data());
@@ -978,6 +1179,7 @@ void Engine<T>::run() {
         int i2 = kept - locked + 1;
         if (info->nec < info->ned) {
             if ((stat = get_eval(jnd, locked, alfrot_.data(), betrot_.data(), lambda_.data(), res_.data()))) break;
+            track_ritz(jnd);
             convergence_test(jnd, lambda_.data(), res_.data(), info, wrk2_.data());
             log_progress();
         }
@@ -1049,6 +1251,14 @@ void Engine<T>::run() {
     }
     final_j1_ = j1;
     info->stat = stat;
+    double max_res = -1.0;
+    const bool want_refine = opt_.refine > 0 || (opt_.refine < 0 && !kWide);
+    if (want_refine && stat == 0 && info->nec > 0 && info->lohi != 0) {
+        const double tr0 = now_s();
+        const int rs = refine_fp64(std::min(info->nec, j1), &max_res);
+        t_res_ += now_s() - tr0;
+        if (rs) info->stat = rs;
+    }
     // Flop counts go to the floating-point counters (the int ones would
     // overflow at these sizes); timers are seconds in the tick_* fields.
     info->rflp += fl_;
@@ -1065,7 +1275,7 @@ void Engine<T>::run() {
     s.kernel_launches = launches_;
     s.cgs_passes = info->north;
     s.host_syncs = syncs_;
-    s.max_true_residual = -1.0;
+    s.max_true_residual = max_res;
     s.op_bytes = builtin_ ? spmv_bytes(builtin_) * info->matvec : 0.0;
     cudaStreamSynchronize(st_);
     flush_prof();

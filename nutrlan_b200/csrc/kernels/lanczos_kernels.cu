@@ -534,6 +534,22 @@ void launch_random<zd>(zd *dst, long n, long n_pad, uint64_t seed, cudaStream_t 
     k_random_cplx<<<elementwise_blocks(n_pad), kThreads, 0, st>>>(dst, n, n_pad, seed);
 }
 
+// out = a * (ay - c * y) + b * yp  (one step of a scaled Chebyshev filter;
+// out may alias yp).
+__global__ void k_cheb(const double *__restrict__ ay, const double *__restrict__ y, const double *yp, long n_pad,
+                       double a, double c, double b, double *out) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += stride) {
+        const double prev = yp ? yp[i] : 0.0;
+        out[i] = a * (ay[i] - c * y[i]) + b * prev;
+    }
+}
+
+void launch_cheb(const double *ay, const double *y, const double *yp, long n_pad, double a, double c, double b,
+                 double *out, cudaStream_t st) {
+    k_cheb<<<elementwise_blocks(n_pad), kThreads, 0, st>>>(ay, y, yp, n_pad, a, c, b, out);
+}
+
 #define TRLB_INST(T)                                                                              \
     template void launch_project<T>(T *const *, int, long, const Store<T>::C *, Recur<Store<T>::C>, \
                                     Store<T>::C *, double *, Scratch &, cudaStream_t);            \

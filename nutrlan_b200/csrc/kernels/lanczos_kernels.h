@@ -84,6 +84,11 @@ template <class T>
 void launch_load(const T *src, long n, typename Store<T>::C *dst,
                  cudaStream_t st);
 
+// out = a * (ay - c * y) + b * yp (yp may be null; out may alias yp): one
+// step of the scaled Chebyshev filter of the FP64 refinement.
+void launch_cheb(const double *ay, const double *y, const double *yp, long n_pad, double a, double c, double b,
+                 double *out, cudaStream_t st);
+
 // Smoothed uniform random vector (the breakdown restart of Gram-Schmidt);
 // rows >= n are set to zero.
 template <class C>

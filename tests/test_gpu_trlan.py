@@ -222,17 +222,39 @@ def test_host_operator_simple_example():
     assert np.all(res <= 1.4901e-8 * d.max() * 1.01)
 
 
-def test_fp32_basis_accuracy_stated(lap128):
+def test_fp32_basis_refined_to_tolerance(lap128):
+    """32-bit basis storage with the default FP64 refinement: eigenvalues
+    within 1e-10 relative of the analytic spectrum and true residuals
+    <= tol * ||A|| (the refinement's operator applications are counted)."""
     A, x0, exact = lap128
     with DeviceOperator(A) as op:
-        r64 = solve(op, ned=10, maxlan=64, restart=1, maxmv=100000, start=x0, basis_bits=64)
         r32 = solve(op, ned=10, maxlan=64, restart=1, maxmv=100000, start=x0, basis_bits=32)
+        raw = solve(op, ned=10, maxlan=64, restart=1, maxmv=100000, start=x0, basis_bits=32, refine=False)
     assert r32.stat == 0 and r32.nec >= 10
-    # FP32 storage: eigenvalues still within 1e-9 relative of the analytic
-    # spectrum; residuals at the FP32 storage level (stated tolerance 1e-6).
-    _match(r32.eval[: r32.nec], exact, rel=1e-9)
+    _match(r32.eval[: r32.nec], exact, rel=1e-10)
     res = _residuals(A, r32.eval[: r32.nec], r32.evec[: r32.nec])
-    assert np.all(res <= 1e-6 * np.max(exact)), res
+    assert np.all(res <= 1.01 * 1.4901e-8 * r32.info.anrm), res
+    np.testing.assert_allclose(r32.res[: r32.nec], res, rtol=1e-3, atol=1e-12)
+    assert 0.0 < r32.stats.max_true_residual <= 1.4901e-8 * r32.info.anrm
+    assert r32.info.matvec > raw.info.matvec
+    # Without refinement the residuals sit at the FP32 storage level.
+    res_raw = _residuals(A, raw.eval[: raw.nec], raw.evec[: raw.nec])
+    assert np.all(res_raw <= 1e-6 * np.max(exact)), res_raw
+    assert raw.stats.max_true_residual == -1.0
+
+
+def test_fp32_basis_matches_fp64_on_anderson():
+    """Non-degenerate spectrum: the refined 32-bit-basis solve returns the
+    FP64-basis eigenvalues to 1e-10 relative, residuals <= tol * ||A||."""
+    A = ops.anderson_3d(24)
+    x0 = ops.start_vector(A.n)
+    with DeviceOperator(A, fmt="sell") as op:
+        r64 = solve(op, ned=12, maxlan=48, tol=1e-8, restart=1, maxmv=100000, start=x0)
+        r32 = solve(op, ned=12, maxlan=48, tol=1e-8, restart=1, maxmv=100000, start=x0, basis_bits=32)
+    assert r32.nec >= 12 and r64.nec >= 12
+    np.testing.assert_allclose(np.sort(r32.eval[:12]), np.sort(r64.eval[:12]), rtol=1e-10)
+    res = _residuals(A, r32.eval[:12], r32.evec[:12])
+    assert np.all(res <= 1.01 * 1e-8 * r32.info.anrm), res
 
 
 def test_complex_diagonal_example():
