@@ -265,7 +265,36 @@ class Engine {
     cudaStream_t st_ = nullptr;
     bool own_stream_ = false;
     User *hx_ = nullptr, *hy_ = nullptr;  // pinned staging for host operators
-    cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+    // Per-step op / orth timing: two sets of (start, after op, after orth)
+    // events used alternately; a step's set is read at the next step, after
+    // that step's scalar sync has retired it, so timing adds no host wait.
+    cudaEvent_t ev_[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    int evset_ = 0, ev_pending_ = -1;
+    void tm_begin() {
+        if (ev_pending_ == evset_) tm_collect(true);
+        cudaEventRecord(ev_[3 * evset_], st_);
+    }
+    void tm_mid() { cudaEventRecord(ev_[3 * evset_ + 1], st_); }
+    void tm_end() {
+        if (ev_pending_ >= 0 && ev_pending_ != evset_) tm_collect(false);
+        cudaEventRecord(ev_[3 * evset_ + 2], st_);
+        ev_pending_ = evset_;
+        evset_ ^= 1;
+    }
+    void tm_collect(bool wait) {
+        if (ev_pending_ < 0) return;
+        cudaEvent_t *e = ev_ + 3 * ev_pending_;
+        if (wait)
+            cudaEventSynchronize(e[2]);
+        else if (cudaEventQuery(e[2]) != cudaSuccess)
+            return;
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, e[0], e[1]);
+        cudaEventElapsedTime(&b, e[1], e[2]);
+        t_op_ += a * 1e-3;
+        t_orth_ += b * 1e-3;
+        ev_pending_ = -1;
+    }
 
     // host state (reference names)
     std::vector<double> alpha_, beta_, alfrot_, betrot_, rot_, lambda_, res_, yy_, wrk2_;
@@ -1066,9 +1095,9 @@ void Engine<T>::run() {
             qb64_ = jnd >= 2 ? reinterpret_cast<C *>(col(jnd - 2)) : nullptr;
             r64_ = reinterpret_cast<C *>(col(jnd));
         }
-        cudaEventRecord(ev_[0], st_);
+        tm_begin();
         if ((stat = apply_op(qa64_, r64_, true))) break;
-        cudaEventRecord(ev_[1], st_);
+        tm_mid();
         // Coefficients (beta_0 .. beta_{jnd-2}, alpha_{jnd-1}); the device
         // writes alpha into the last slot before the coupling update.
         {
@@ -1100,16 +1129,8 @@ void Engine<T>::run() {
         double f0 = fl_;
         stat = orth(jnd, false, 0.0, kept);
         fl_h_ += fl_ - f0;
-        cudaEventRecord(ev_[2], st_);
+        tm_end();
         if (stat) break;
-        {
-            cudaEventSynchronize(ev_[2]);
-            float a = 0, b = 0;
-            cudaEventElapsedTime(&a, ev_[0], ev_[1]);
-            cudaEventElapsedTime(&b, ev_[1], ev_[2]);
-            t_op_ += a * 1e-3;
-            t_orth_ += b * 1e-3;
-        }
         rotate_fp64();
         // Arrow -> tridiagonal for the non-locked part.
         for (int i = 0; i < locked; ++i) {
@@ -1133,25 +1154,17 @@ void Engine<T>::run() {
                 qb64_ = reinterpret_cast<C *>(col(jnd - 2));
                 r64_ = reinterpret_cast<C *>(col(jnd));
             }
-            cudaEventRecord(ev_[0], st_);
+            tm_begin();
             if ((stat = apply_op(qa64_, r64_, true))) break;
-            cudaEventRecord(ev_[1], st_);
+            tm_mid();
             fl_ += 6 * nrow_;
             double f1 = fl_;
             stat = orth(jnd, true, beta_[jnd - 2], kept);
             fl_h_ += fl_ - f1;
-            cudaEventRecord(ev_[2], st_);
+            tm_end();
             alfrot_[jnd - 1] = alpha_[jnd - 1];
             betrot_[jnd - 1] = beta_[jnd - 1];
             if (stat) break;
-            {
-                cudaEventSynchronize(ev_[2]);
-                float a = 0, b = 0;
-                cudaEventElapsedTime(&a, ev_[0], ev_[1]);
-                cudaEventElapsedTime(&b, ev_[1], ev_[2]);
-                t_op_ += a * 1e-3;
-                t_orth_ += b * 1e-3;
-            }
             rotate_fp64();
             if (info->matvec >= next_test) {
                 if ((stat = get_eval(jnd, locked, alfrot_.data(), betrot_.data(), lambda_.data(), res_.data())))
@@ -1251,6 +1264,7 @@ void Engine<T>::run() {
     }
     final_j1_ = j1;
     info->stat = stat;
+    tm_collect(true);
     double max_res = -1.0;
     const bool want_refine = opt_.refine > 0 || (opt_.refine < 0 && !kWide);
     if (want_refine && stat == 0 && info->nec > 0 && info->lohi != 0) {

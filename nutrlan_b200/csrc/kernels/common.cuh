@@ -170,6 +170,15 @@ __device__ __forceinline__ C block_sum(C v, C *smem /* >= 32 entries */) {
     return s;
 }
 
+// Final sum of nb per-block partials, run by every thread of the last block
+// in a fixed order: thread t adds part[t], part[t + blockDim.x], ..., then
+// the block tree of block_sum.  Returns the total in thread 0.
+__device__ __forceinline__ double sum_partials(const double *part, int nb, double *smem /* >= 32 entries */) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += __ldcg(part + b);
+    return block_sum(s, smem);
+}
+
 // Called by every thread after the block wrote its partials: returns true in
 // exactly one block (the last to arrive), which then owns the final sums.
 __device__ __forceinline__ bool last_block_arrived(unsigned *ticket) {

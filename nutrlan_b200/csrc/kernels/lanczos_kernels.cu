@@ -59,9 +59,8 @@ __global__ void __launch_bounds__(kThreads) k_dot(const C *__restrict__ x, const
     double s = block_sum(acc, red);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
     if (last_block_arrived(ticket)) {
+        const double tot = sum_partials(part, gridDim.x, red);
         if (threadIdx.x == 0) {
-            double tot = 0.0;
-            for (unsigned b = 0; b < gridDim.x; ++b) tot += __ldcg(part + b);
             *out = tot;
             *ticket = 0;
         }
@@ -172,13 +171,85 @@ __global__ void __launch_bounds__(kThreads, (proj_min_blocks<T, CPW>()))
     }
     if (last_block_arrived(ticket)) {
         __shared__ C red_cols[kThreads];
+        __shared__ double red_r2x[32];
         const int nb = gridDim.x;
         const double h2 = reduce_columns(part, nb, m, h, red_cols);
+        const double r2 = sum_partials(part_r2, nb, red_r2x);
         if (threadIdx.x == 0) {
-            double r2 = 0.0;
-            for (int b = 0; b < nb; ++b) r2 += __ldcg(part_r2 + b);
             out2[0] = r2;
             out2[1] = h2;
+            *ticket = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Update for short vectors (few rows per thread): a block works on tiles of
+// 32 * R rows; its 8 warps take every 8th column of the tile, so each
+// thread's chain of dependent loads is m / 8 long instead of m, and the
+// slices' partial sums are combined in shared memory in slice order.
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    k_update_split(T *const *__restrict__ cols, int m, long n_pad, const typename Store<T>::C *r,
+                   Recur<typename Store<T>::C> rec, const typename Store<T>::C *__restrict__ h,
+                   typename Store<T>::C *r_out, double *part_r2, unsigned *ticket, double *out_r2) {
+    using S = Store<T>;
+    using C = typename S::C;
+    constexpr int R = S::R;
+    constexpr int NS = kThreads / 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *hs = reinterpret_cast<C *>(smem_raw);
+    const T **ps = reinterpret_cast<const T **>(smem_raw + sizeof(C) * m);
+    __shared__ C red[NS][32 * R];
+    for (int c = threadIdx.x; c < m; c += blockDim.x) {
+        hs[c] = h[c];
+        ps[c] = cols[c];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, sl = threadIdx.x >> 5;
+    const double alpha = rec.on ? *rec.alpha : 0.0;
+    double r2acc = 0.0;
+    for (long t0 = (long)blockIdx.x * 32 * R; t0 < n_pad; t0 += (long)gridDim.x * 32 * R) {
+        const long i = t0 + (long)lane * R;
+        C acc[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) acc[q] = czero(C());
+        for (int c = sl; c < m; c += NS) {
+            C v[R];
+            S::load(ps[c] + i, v);
+            const C hc = hs[c];
+#pragma unroll
+            for (int q = 0; q < R; ++q) fms(acc[q], v[q], hc);
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) red[sl][lane * R + q] = acc[q];
+        __syncthreads();
+        if (sl == 0) {
+            C base[R];
+            load_c<R>(r + i, base);
+            if (rec.on) {
+                C xv[R], xpv[R];
+                load_c<R>(rec.x + i, xv);
+                load_c<R>(rec.xp + i, xpv);
+#pragma unroll
+                for (int q = 0; q < R; ++q) base[q] = base[q] - alpha * xv[q] - rec.beta * xpv[q];
+            }
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+                for (int k = 0; k < NS; ++k) base[q] = base[q] + red[k][lane * R + q];
+                r2acc += abs2(base[q]);
+            }
+            store_c<R>(r_out + i, base);
+        }
+        __syncthreads();
+    }
+    __shared__ double redb[32];
+    double s = block_sum(r2acc, redb);
+    if (threadIdx.x == 0) part_r2[blockIdx.x] = s;
+    if (last_block_arrived(ticket)) {
+        const double tot = sum_partials(part_r2, gridDim.x, redb);
+        if (threadIdx.x == 0) {
+            *out_r2 = tot;
             *ticket = 0;
         }
     }
@@ -248,9 +319,8 @@ __global__ void __launch_bounds__(kThreads)
     double s = block_sum(r2acc, red);
     if (threadIdx.x == 0) part_r2[blockIdx.x] = s;
     if (last_block_arrived(ticket)) {
+        const double tot = sum_partials(part_r2, gridDim.x, red);
         if (threadIdx.x == 0) {
-            double tot = 0.0;
-            for (unsigned b = 0; b < gridDim.x; ++b) tot += __ldcg(part_r2 + b);
             *out_r2 = tot;
             *ticket = 0;
         }
@@ -422,7 +492,14 @@ int elementwise_blocks(long n) {
 
 int stream_blocks(long n_pad, int rows_per_group) {
     long need = (n_pad + (long)kThreads * rows_per_group - 1) / ((long)kThreads * rows_per_group);
-    long cap = (long)num_sms() * 4;
+    const long cap = (long)num_sms() * 4;
+    const long fill = (long)num_sms() * 2;
+    if (need < fill) {
+        // Short vectors: smaller blocks (down to one warp-row of
+        // 32 * rows_per_group rows) so that every SM has work in flight.
+        const long min_rows = 32L * rows_per_group;
+        need = std::min(fill, (n_pad + min_rows - 1) / min_rows);
+    }
     return (int)std::max<long>(1, std::min(need, cap));
 }
 
@@ -477,6 +554,18 @@ void launch_update(T *const *cols, int m, long n_pad, const typename Store<T>::C
     constexpr int R = Store<T>::R;
     int nb = std::min(stream_blocks(n_pad, R), s.max_blocks);
     size_t smem = (sizeof(C) + sizeof(T *)) * (size_t)std::max(m, 1);
+    // Short vectors (at most one row tile per thread at this grid) with
+    // enough columns: split the columns across the warps of a block.
+    const bool split = m >= 16 && n_pad <= (long)nb * kThreads * R;
+    if (split) {
+        const int nt = (int)std::min<long>((n_pad + 32L * R - 1) / (32L * R), s.max_blocks);
+        if (smem > 40 * 1024)
+            cudaFuncSetAttribute(k_update_split<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_update_split<T><<<nt, kThreads, smem, st>>>(cols, m, n_pad, r, rec, h, r_out,
+                                                       reinterpret_cast<double *>(s.partials),
+                                                       s.tickets + kTicketUpdate, out_r2);
+        return;
+    }
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_update<T><<<nb, kThreads, smem, st>>>(cols, m, n_pad, r, rec, h, r_out,

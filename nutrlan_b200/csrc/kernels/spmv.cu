@@ -72,9 +72,8 @@ __global__ void __launch_bounds__(kThreads)
     double s = block_sum(aacc, red);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
     if (last_block_arrived(ticket)) {
+        const double tot = sum_partials(part, gridDim.x, red);
         if (threadIdx.x == 0) {
-            double tot = 0.0;
-            for (unsigned b = 0; b < gridDim.x; ++b) tot += __ldcg(part + b);
             *alpha_out = tot;
             *ticket = 0;
         }
@@ -125,9 +124,8 @@ __global__ void __launch_bounds__(kThreads)
     double s = block_sum(aacc, red);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
     if (last_block_arrived(ticket)) {
+        const double tot = sum_partials(part, gridDim.x, red);
         if (threadIdx.x == 0) {
-            double tot = 0.0;
-            for (unsigned b = 0; b < gridDim.x; ++b) tot += __ldcg(part + b);
             *alpha_out = tot;
             *ticket = 0;
         }
@@ -165,9 +163,8 @@ __global__ void __launch_bounds__(kThreads)
     double s2 = block_sum(aacc, red);
     if (threadIdx.x == 0) part[blockIdx.x] = s2;
     if (last_block_arrived(ticket)) {
+        const double tot = sum_partials(part, gridDim.x, red);
         if (threadIdx.x == 0) {
-            double tot = 0.0;
-            for (unsigned bb = 0; bb < gridDim.x; ++bb) tot += __ldcg(part + bb);
             *alpha_out = tot;
             *ticket = 0;
         }
@@ -188,12 +185,26 @@ int spmv_blocks(long work_items, int per_block) {
 
 }  // namespace
 
+// The 256-row-tile CSR kernel needs whole tiles and pays off once every SM
+// has at least two tiles; shorter vectors use the 8-lanes-per-row kernel,
+// whose many small blocks hide latency better.
+static bool use_row_tiles(long n_pad) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return n_pad % kThreads == 0 && n_pad / kThreads >= 2L * sms;
+}
+
 void spmv_fused_real(const trlx_operator *A, const double *x, double *y, long n_pad,
                      double *alpha_out, Scratch *s, cudaStream_t st) {
     double *part = s ? reinterpret_cast<double *>(s->partials) : nullptr;
     unsigned *tk = s ? s->tickets + kTicketSpmv : nullptr;
     if (A->kind == 0) {
-        if (n_pad % kThreads == 0) {
+        if (use_row_tiles(n_pad)) {
             int nb = spmv_blocks(n_pad, kThreads);
             if (s) nb = std::min(nb, s->max_blocks);
             k_csr_stream<double><<<nb, kThreads, 0, st>>>(A->nrow, n_pad, A->row_ptr, A->col,
@@ -219,7 +230,7 @@ void spmv_fused_cplx(const trlx_operator *A, const zd *x, zd *y, long n_pad, dou
                      Scratch *s, cudaStream_t st) {
     double *part = s ? reinterpret_cast<double *>(s->partials) : nullptr;
     unsigned *tk = s ? s->tickets + kTicketSpmv : nullptr;
-    if (n_pad % kThreads == 0) {
+    if (use_row_tiles(n_pad)) {
         int nb = spmv_blocks(n_pad, kThreads);
         if (s) nb = std::min(nb, s->max_blocks);
         k_csr_stream<zd><<<nb, kThreads, 0, st>>>(A->nrow, n_pad, A->row_ptr, A->col,

@@ -108,7 +108,7 @@ class SolveResult:
 
 
 def solve(op, ned, maxlan, lohi=-1, tol=1.4901e-8, restart=1, maxmv=0, start=None, mev=None,
-          basis_bits=64, device=False, seed=0, evec=None, refine=None):
+          basis_bits=64, device=False, seed=0, evec=None, refine=None, profile=False):
     """Run trlan/ztrlan on a DeviceOperator through the C ABI.
 
     ``start`` (length n, numpy or CUDA tensor) becomes the initial vector
@@ -149,6 +149,7 @@ def solve(op, ned, maxlan, lohi=-1, tol=1.4901e-8, restart=1, maxmv=0, start=Non
     opts.seed = seed
     if refine is not None:
         opts.refine = 1 if refine else 0
+    opts.profile = 1 if profile else 0
     if op.complex:
         misc = np.zeros(mev, dtype=np.complex128)
         lib.trlx_ztrlan(op.applier, C.byref(info), n, mev, eval_.ctypes.data, evec_ptr, n,
