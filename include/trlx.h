@@ -240,6 +240,11 @@ typedef struct {
     double kernel_bytes[8];
     long long kernel_count[8];
     double seconds_setup;     /* workspace acquisition and initialisation  */
+    long long speculative_steps;     /* Lanczos steps issued ahead of the
+                                        host decisions and accepted         */
+    long long speculative_discarded; /* speculative steps rerun (their
+                                        operator applications are not in
+                                        info->matvec)                       */
 } trlx_stats;
 
 #define TRLX_K_SPMV 0      /* built-in operator (+ fused alpha)          */

@@ -23,6 +23,7 @@ class TrlxStats(C.Structure):
         ("host_syncs", c_int), ("max_true_residual", c_double),
         ("kernel_seconds", c_double * 8), ("kernel_bytes", c_double * 8),
         ("kernel_count", C.c_longlong * 8), ("seconds_setup", c_double),
+        ("speculative_steps", C.c_longlong), ("speculative_discarded", C.c_longlong),
     ]
 
     KERNEL_CLASSES = ("spmv", "project", "update", "normalize", "ritz", "dot", "other")

@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstring>
 #include <type_traits>
+#include <cstdlib>
 #include <numeric>
 #include <vector>
 
@@ -65,6 +66,8 @@ struct Workspace {
     size_t refine_bytes = 0;
     unsigned *tickets = nullptr;
     double *h_scal = nullptr;
+    double *h_log = nullptr;  // pinned copy of the speculative step log
+    size_t h_log_len = 0;
     int device = -1;
     ~Workspace() { release(); }
     void release() {
@@ -76,6 +79,9 @@ struct Workspace {
         cudaFree(refine);
         cudaFree(tickets);
         cudaFreeHost(h_scal);
+        cudaFreeHost(h_log);
+        h_log = nullptr;
+        h_log_len = 0;
         pool = fbuf = small = partials = out = refine = nullptr;
         out_bytes = refine_bytes = 0;
         tickets = nullptr;
@@ -219,6 +225,9 @@ class Engine {
     int restart_ritz(int locked, int jml, int kept, int jnd);
     int final_vectors(int jnd, int kept);
     int refine_fp64(int k, double *max_res);
+    bool spec_enabled() const;
+    int spec_segment(int *jnd, int S, int kept);
+    bool accept_step(int jnd, int kept, const double *lg);
     void track_ritz(int nd) {
         for (int i = 0; i < nd; ++i) {
             ritz_min_ = std::min(ritz_min_, lambda_[i]);
@@ -261,6 +270,9 @@ class Engine {
     C *d_coef_ = nullptr;
     double *d_scal_ = nullptr, *h_scal_ = nullptr;
     double *d_Y_ = nullptr;
+    double *d_log_ = nullptr, *h_log_ = nullptr;  // speculative steps: alpha, |r|^2 pre/post, |h|^2
+    long long discarded_ = 0;                     // speculative operator applications rerun
+    long long spec_accepted_ = 0;
     Scratch scratch_;
     cudaStream_t st_ = nullptr;
     bool own_stream_ = false;
@@ -268,7 +280,7 @@ class Engine {
     // Per-step op / orth timing: two sets of (start, after op, after orth)
     // events used alternately; a step's set is read at the next step, after
     // that step's scalar sync has retired it, so timing adds no host wait.
-    cudaEvent_t ev_[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // [6], [7]: speculative segments
     int evset_ = 0, ev_pending_ = -1;
     void tm_begin() {
         if (ev_pending_ == evset_) tm_collect(true);
@@ -415,13 +427,23 @@ int Engine<T>::setup() {
     // Small buffers carved from one allocation (256-byte aligned pieces).
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
     const size_t b_coef = al(sizeof(C) * P_), b_scal = al(sizeof(double) * kNumScal),
-                 b_Y = al(sizeof(double) * (size_t)maxlan_ * maxlan_), b_cols = al(sizeof(T *) * P_);
-    if (!Workspace::ensure(&ws.small, &ws.small_bytes, b_coef + b_scal + b_Y + b_cols)) return -5;
+                 b_Y = al(sizeof(double) * (size_t)maxlan_ * maxlan_), b_cols = al(sizeof(T *) * P_),
+                 log_len = 4 * ((size_t)maxlan_ + 2), b_log = al(sizeof(double) * log_len);
+    if (!Workspace::ensure(&ws.small, &ws.small_bytes, b_coef + b_scal + b_Y + b_cols + b_log)) return -5;
     char *sp = static_cast<char *>(ws.small);
     d_coef_ = reinterpret_cast<C *>(sp);
     d_scal_ = reinterpret_cast<double *>(sp + b_coef);
     d_Y_ = reinterpret_cast<double *>(sp + b_coef + b_scal);
     d_cols_ = reinterpret_cast<T **>(sp + b_coef + b_scal + b_Y);
+    d_log_ = reinterpret_cast<double *>(sp + b_coef + b_scal + b_Y + b_cols);
+    if (ws.h_log_len < log_len) {
+        cudaFreeHost(ws.h_log);
+        ws.h_log = nullptr;
+        ws.h_log_len = 0;
+        CK(cudaMallocHost(&ws.h_log, sizeof(double) * log_len));
+        ws.h_log_len = log_len;
+    }
+    h_log_ = ws.h_log;
     CK(cudaMemsetAsync(d_scal_, 0, sizeof(double) * kNumScal, st_));
     if (!ws.h_scal) CK(cudaMallocHost(&ws.h_scal, sizeof(double) * kNumScal));
     h_scal_ = ws.h_scal;
@@ -859,6 +881,138 @@ int Engine<T>::final_vectors(int jnd, int kept) {
     return 0;
 }
 
+// ---- speculative regular steps ---------------------------------------------
+// For short vectors the host round trip of every Lanczos step (read alpha
+// and the norms, take trl_orth's decisions, launch the next step) costs more
+// than the step's kernels.  With a built-in operator and an FP64/c128 basis
+// the engine issues a run of steps without waiting, each assuming the
+// outcome trl_orth takes in almost every step: the full classical
+// Gram-Schmidt path with one pass (its stop test passes) and a beta that is
+// neither negligible nor a random restart.  Each step logs alpha, |r|^2
+// before and after the pass and |h|^2; the recurrence of the next step takes
+// beta = sqrt(|r|^2 after) from that log on the device, and the normalisation
+// uses the same value, so an accepted step is bitwise identical to the
+// sequential one.  The host then replays trl_orth's decisions on the logged
+// values in order; the first step whose decisions differ and everything after
+// it are discarded (their operator applications are subtracted from matvec)
+// and rerun by the sequential path.  TRLX_SPECULATE=0 disables it.
+template <class T>
+bool Engine<T>::spec_enabled() const {
+    if constexpr (!kWide) {
+        return false;
+    } else {
+        if (!builtin_ || uo_ || n_pad_ > (1L << 21)) return false;
+        const char *e = std::getenv("TRLX_SPECULATE");
+        return !(e && e[0] == '0');
+    }
+}
+
+template <class T>
+bool Engine<T>::accept_step(int jnd, int kept, const double *lg) {
+    const int jm1 = jnd - 1;
+    const double alpha = lg[0], normrr2 = lg[1], normdiff2 = lg[2], r2post = lg[3];
+    if (!(normrr2 >= 0.0) || !(normrr2 <= DBL_MAX)) return false;
+    const double beta_pre = std::sqrt(normrr2);
+    double tmp = alpha * alpha, fo = 0.0;
+    if (jm1 > kept) {
+        tmp += beta_[jm1 - 1] * beta_[jm1 - 1];
+        fo = 2 * nrow_ + 4;
+    } else if (kept > 0) {
+        for (int i = 0; i < jm1; ++i) tmp += beta_[i] * beta_[i];
+        fo = 2 * (nrow_ + kept + 2);
+    }
+    bool usecgs;
+    if (jm1 == kept) {
+        usecgs = true;
+    } else if (jnd >= info_->ntot) {
+        usecgs = false;
+    } else if (DBL_EPSILON * normrr2 >= tmp) {
+        double anorm = 0.0;
+        for (int i = 0; i < jm1; ++i) anorm = std::max(anorm, std::fabs(alpha_[i]) + std::fabs(beta_[i]));
+        anorm = std::max(anorm, std::fabs(alpha) + std::fabs(beta_pre));
+        usecgs = beta_pre < DBL_EPSILON * anorm * info_->ntot;
+    } else {
+        usecgs = true;
+    }
+    if (!usecgs) return false;
+    if (!(DBL_EPSILON * r2post > normdiff2)) return false;  // a second pass would follow
+    const double rnrm = std::sqrt(r2post);
+    if (!(rnrm > DBL_MIN)) return false;
+    if (rnrm <= DBL_EPSILON * std::fabs(alpha) || jnd >= info_->ntot) return false;
+    alpha_[jnd - 1] = alpha;
+    beta_[jnd - 1] = rnrm;
+    alfrot_[jnd - 1] = alpha;
+    betrot_[jnd - 1] = rnrm;
+    fl_ += 6 * nrow_;
+    const double f1 = fl_;
+    fl_ += fo + 4.0 * nrow_ * jnd + nrow_;
+    fl_h_ += fl_ - f1;
+    info_->north++;
+    return true;
+}
+
+template <class T>
+int Engine<T>::spec_segment(int *jnd_io, int S, int kept) {
+    if constexpr (!kWide) {
+        (void)jnd_io;
+        (void)S;
+        (void)kept;
+        return 0;
+    } else {
+        const int j0 = *jnd_io;
+        cudaEventRecord(ev_[6], st_);
+        for (int s = 1; s <= S; ++s) {
+            const int j = j0 + s;
+            C *qa = reinterpret_cast<C *>(col(j - 1)), *qb = reinterpret_cast<C *>(col(j - 2)),
+              *r = reinterpret_cast<C *>(col(j));
+            double *lg = d_log_ + 4 * (size_t)s;
+            int pid = pbeg();
+            if constexpr (kComplex)
+                spmv_fused_cplx(builtin_, qa, r, n_pad_, lg, &scratch_, st_);
+            else
+                spmv_fused_real(builtin_, qa, r, n_pad_, lg, &scratch_, st_);
+            pend(pid, TRLX_K_SPMV, spmv_bytes(builtin_));
+            info_->matvec++;
+            Recur<C> rec;
+            rec.x = qa;
+            rec.xp = qb;
+            rec.alpha = lg;
+            rec.on = 1;
+            if (s == 1)
+                rec.beta = beta_[j - 2];
+            else
+                rec.beta_r2 = lg - 4 + 3;
+            const double recb = 2.0 * nrow_ * cs();
+            int p1 = pbeg();
+            launch_project<T>(d_cols_, j, n_pad_, r, rec, d_coef_, lg + 1, scratch_, st_);
+            pend(p1, TRLX_K_PROJECT, (double)j * nrow_ * sv() + nrow_ * cs() + recb);
+            int p2 = pbeg();
+            launch_update<T>(d_cols_, j, n_pad_, r, rec, d_coef_, r, lg + 3, scratch_, st_);
+            pend(p2, TRLX_K_UPDATE, (double)j * nrow_ * sv() + 2.0 * nrow_ * cs() + recb);
+            int p3 = pbeg();
+            launch_normalize<T>(r, n_pad_, lg + 3, 0.0, r, nullptr, st_);
+            pend(p3, TRLX_K_NORMALIZE, 2.0 * nrow_ * cs());
+            count_launch(4);
+        }
+        cudaEventRecord(ev_[7], st_);
+        CK(cudaMemcpyAsync(h_log_ + 4, d_log_ + 4, sizeof(double) * 4 * S, cudaMemcpyDeviceToHost, st_));
+        CK(cudaStreamSynchronize(st_));
+        ++syncs_;
+        if (!prof_.empty()) flush_prof();
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev_[6], ev_[7]);
+        t_orth_ += ms * 1e-3;
+        int acc = 0;
+        while (acc < S && accept_step(j0 + acc + 1, kept, h_log_ + 4 * (acc + 1))) ++acc;
+        const int dropped = S - acc;
+        spec_accepted_ += acc;
+        info_->matvec -= dropped;
+        discarded_ += dropped;
+        *jnd_io = j0 + acc;
+        return acc;
+    }
+}
+
 // FP64 refinement of the k converged pairs (real problems).  The converged
 // Ritz vectors of a 32-bit basis carry the basis' rounding noise, which is
 // spread over the whole spectrum; most of its residual comes from the
@@ -1143,7 +1297,38 @@ void Engine<T>::run() {
         betrot_[jnd - 1] = beta_[jnd - 1];
 
         // ---- regular Lanczos steps ---------------------------------------------
+        auto test_convergence = [&]() -> int {
+            int st2 = get_eval(jnd, locked, alfrot_.data(), betrot_.data(), lambda_.data(), res_.data());
+            if (st2) return st2;
+            track_ritz(jnd);
+            const int ne = std::min(mev_, jnd);
+            std::memcpy(eval_, lambda_.data(), sizeof(double) * ne);
+            convergence_test(jnd, lambda_.data(), res_.data(), info, wrk2_.data());
+            if (info->nec < info->ned && info->nec > 0) {
+                next_test = (int)((double)(info->ned * info->matvec) / (double)info->nec);
+            } else if (info->nec == 0) {
+                next_test = next_test + next_test;
+                if (info->maxlan == info->ntot) next_test = (int)std::ceil(0.5 * (info->maxlan + info->matvec));
+            }
+            log_progress();
+            return 0;
+        };
         while (jnd < info->klan && info->nec < info->ned) {
+            if (jnd >= 2 && spec_enabled()) {
+                // Steps up to the next convergence test (or the restart).
+                long S = (long)info->klan - jnd;
+                if (next_test > info->matvec) S = std::min<long>(S, (long)next_test - info->matvec);
+                else S = 1;
+                S = std::min<long>(S, (long)info->maxmv - info->matvec);
+                if (S >= 2) {
+                    const int acc = spec_segment(&jnd, (int)S, kept);
+                    if (acc == S) {
+                        if (info->matvec >= next_test && (stat = test_convergence())) break;
+                        continue;
+                    }
+                    if (jnd >= info->klan) break;
+                }
+            }
             jnd++;
             if (jnd + 1 >= P_) {
                 stat = -1111;
@@ -1166,21 +1351,7 @@ void Engine<T>::run() {
             betrot_[jnd - 1] = beta_[jnd - 1];
             if (stat) break;
             rotate_fp64();
-            if (info->matvec >= next_test) {
-                if ((stat = get_eval(jnd, locked, alfrot_.data(), betrot_.data(), lambda_.data(), res_.data())))
-                    break;
-                track_ritz(jnd);
-                const int ne = std::min(mev_, jnd);
-                std::memcpy(eval_, lambda_.data(), sizeof(double) * ne);
-                convergence_test(jnd, lambda_.data(), res_.data(), info, wrk2_.data());
-                if (info->nec < info->ned && info->nec > 0) {
-                    next_test = (int)((double)(info->ned * info->matvec) / (double)info->nec);
-                } else if (info->nec == 0) {
-                    next_test = next_test + next_test;
-                    if (info->maxlan == info->ntot) next_test = (int)std::ceil(0.5 * (info->maxlan + info->matvec));
-                }
-                log_progress();
-            }
+            if (info->matvec >= next_test && (stat = test_convergence())) break;
         }
         if (stat) break;
 
@@ -1300,6 +1471,8 @@ void Engine<T>::run() {
     }
     s.basis_bytes = kb_[TRLX_K_PROJECT] + kb_[TRLX_K_UPDATE] + kb_[TRLX_K_RITZ];
     s.seconds_setup = setup_seconds_;
+    s.speculative_steps = spec_accepted_;
+    s.speculative_discarded = discarded_;
 }
 
 template <class T>

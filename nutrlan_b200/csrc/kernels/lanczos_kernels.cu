@@ -101,6 +101,7 @@ __global__ void __launch_bounds__(kThreads, (proj_min_blocks<T, CPW>()))
     const long row0 = (long)blockIdx.x * chunk;
     const long row1 = min(n_pad, row0 + chunk);
     const double alpha = rec.on ? *rec.alpha : 0.0;
+    const double beta = rec.on ? (rec.beta_r2 ? sqrt(*rec.beta_r2) : rec.beta) : 0.0;
     const int ngroups = (m + CPW - 1) / CPW;
     double r2acc = 0.0;
     for (int g0 = 0; g0 < ngroups; g0 += W) {
@@ -125,7 +126,7 @@ __global__ void __launch_bounds__(kThreads, (proj_min_blocks<T, CPW>()))
                     load_c<R>(rec.x + i, xv);
                     load_c<R>(rec.xp + i, xpv);
 #pragma unroll
-                    for (int q = 0; q < R; ++q) rv[q] = rv[q] - alpha * xv[q] - rec.beta * xpv[q];
+                    for (int q = 0; q < R; ++q) rv[q] = rv[q] - alpha * xv[q] - beta * xpv[q];
                 }
                 if (count_r2) {
 #pragma unroll
@@ -208,6 +209,7 @@ __global__ void __launch_bounds__(kThreads)
     __syncthreads();
     const int lane = threadIdx.x & 31, sl = threadIdx.x >> 5;
     const double alpha = rec.on ? *rec.alpha : 0.0;
+    const double beta = rec.on ? (rec.beta_r2 ? sqrt(*rec.beta_r2) : rec.beta) : 0.0;
     double r2acc = 0.0;
     for (long t0 = (long)blockIdx.x * 32 * R; t0 < n_pad; t0 += (long)gridDim.x * 32 * R) {
         const long i = t0 + (long)lane * R;
@@ -232,7 +234,7 @@ __global__ void __launch_bounds__(kThreads)
                 load_c<R>(rec.x + i, xv);
                 load_c<R>(rec.xp + i, xpv);
 #pragma unroll
-                for (int q = 0; q < R; ++q) base[q] = base[q] - alpha * xv[q] - rec.beta * xpv[q];
+                for (int q = 0; q < R; ++q) base[q] = base[q] - alpha * xv[q] - beta * xpv[q];
             }
 #pragma unroll
             for (int q = 0; q < R; ++q) {
@@ -276,6 +278,7 @@ __global__ void __launch_bounds__(kThreads)
     }
     __syncthreads();
     const double alpha = rec.on ? *rec.alpha : 0.0;
+    const double beta = rec.on ? (rec.beta_r2 ? sqrt(*rec.beta_r2) : rec.beta) : 0.0;
     double r2acc = 0.0;
     const long stride = (long)gridDim.x * blockDim.x * R;
     for (long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) * R; i < n_pad; i += stride) {
@@ -286,7 +289,7 @@ __global__ void __launch_bounds__(kThreads)
             load_c<R>(rec.x + i, xv);
             load_c<R>(rec.xp + i, xpv);
 #pragma unroll
-            for (int q = 0; q < R; ++q) acc[q] = acc[q] - alpha * xv[q] - rec.beta * xpv[q];
+            for (int q = 0; q < R; ++q) acc[q] = acc[q] - alpha * xv[q] - beta * xpv[q];
         }
         int c = 0;
         for (; c + 4 <= m; c += 4) {

@@ -30,6 +30,7 @@ struct Recur {
     const C *xp = nullptr;
     const double *alpha = nullptr;  // device scalar
     double beta = 0.0;
+    const double *beta_r2 = nullptr;  // when set: beta = sqrt(*beta_r2) (device)
     int on = 0;
 };
 

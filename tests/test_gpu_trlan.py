@@ -285,3 +285,33 @@ def test_peierls_small_matches_oracle():
     for lam, v in zip(r.eval[: r.nec], r.evec[: r.nec]):
         rr = A.matvec(v) - lam * v
         assert np.linalg.norm(rr) <= 1.4901e-8 * np.max(np.abs(dense)) * 1.01
+
+
+@pytest.mark.parametrize("case", ["laplace64", "anderson16", "wells64", "peierls32"])
+def test_speculative_steps_match_sequential(case, monkeypatch):
+    """Steps issued ahead of the host decisions (short vectors, built-in
+    operator) give bitwise the same eigenvalues, eigenvectors and counters
+    as the sequential engine, with fewer host synchronisations."""
+    import torch
+    if case == "laplace64":
+        A, ned, maxlan = ops.laplacian_2d(64), 10, 40
+    elif case == "anderson16":
+        A, ned, maxlan = ops.anderson_3d(16), 12, 48
+    elif case == "wells64":
+        A, ned, maxlan = ops.wells_2d(64, seed=3)[0], 16, 48
+    else:
+        A, ned, maxlan = ops.peierls_2d(32, phi=1.0 / 16.0), 8, 40
+    x0 = ops.start_vector(A.n)
+    if np.iscomplexobj(A.val):
+        x0 = x0 + 1j * ops.start_vector(A.n, seed=7)
+    with DeviceOperator(A) as op:
+        monkeypatch.setenv("TRLX_SPECULATE", "0")
+        seq = solve(op, ned=ned, maxlan=maxlan, tol=1e-10, restart=1, maxmv=100000, start=x0, device=True)
+        monkeypatch.delenv("TRLX_SPECULATE")
+        spec = solve(op, ned=ned, maxlan=maxlan, tol=1e-10, restart=1, maxmv=100000, start=x0, device=True)
+    assert seq.stats.speculative_steps == 0 and spec.stats.speculative_steps > 0
+    assert spec.info.matvec == seq.info.matvec and spec.info.nloop == seq.info.nloop
+    assert spec.info.north == seq.info.north and spec.nec == seq.nec >= ned
+    np.testing.assert_array_equal(spec.eval[:spec.nec], seq.eval[:seq.nec])
+    assert torch.equal(spec.evec[:spec.nec], seq.evec[:seq.nec])
+    assert spec.stats.host_syncs < seq.stats.host_syncs
