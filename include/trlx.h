@@ -282,6 +282,8 @@ int trlx_host_arrow_to_tridiag(int nd, const double *alpha,
                                double *alfrot, double *betrot);
 /* Symmetric eigen-decomposition in place (A n x n column-major). */
 int trlx_host_sym_eig(int n, double *A, int lda, double *w);
+int trlx_host_herm_eig(int n, const trl_dcomplex *A, int lda, double *w,
+                       trl_dcomplex *Z, int ldz);
 /* Restart decision: kept pairs (and info->klan for schemes 7/8). */
 void trlx_host_shuffle_eig(int nd, int mnd, double *lambda, double *res,
                            trl_info *info, int *kept, int locked);

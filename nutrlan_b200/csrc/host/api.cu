@@ -588,6 +588,10 @@ int trlx_host_arrow_to_tridiag(int nd, const double *alpha, const double *beta, 
     return trlb::arrow_to_tridiag(nd, alpha, beta, rot, alfrot, betrot);
 }
 int trlx_host_sym_eig(int n, double *A, int lda, double *w) { return trlb::sym_eig(n, A, lda, w); }
+int trlx_host_herm_eig(int n, const trl_dcomplex *A, int lda, double *w, trl_dcomplex *Z, int ldz) {
+    return trlb::herm_eig(n, reinterpret_cast<const std::complex<double> *>(A), lda, w,
+                          reinterpret_cast<std::complex<double> *>(Z), ldz);
+}
 void trlx_host_shuffle_eig(int nd, int mnd, double *lambda, double *res, trl_info *info, int *kept, int locked) {
     trlb::shuffle_eig(nd, mnd, lambda, res, info, kept, locked);
 }

@@ -15,6 +15,7 @@
 //     (reference SRC/dsort2.c).
 #pragma once
 
+#include <complex>
 #include <vector>
 
 struct strct_trl_info;
@@ -47,6 +48,11 @@ int tridiag_eig_last(int n, const double *d, const double *e, double *lambda,
 // Full symmetric eigen-decomposition: eigenvalues ascending into w, vectors
 // into A (columns).  Returns 0 on success.
 int sym_eig(int n, double *A, int lda, double *w);
+
+// Hermitian eigen-decomposition (cyclic Jacobi; n small): eigenvalues
+// ascending into w, unitary eigenvectors into Z (columns).  Returns 0, or 1
+// if the sweeps did not converge.
+int herm_eig(int n, const std::complex<double> *A, int lda, double *w, std::complex<double> *Z, int ldz);
 
 // ---- pieces of the reference's Lanczos driver ----------------------------
 // trl_tridiag: arrow matrix (alpha on diag, beta[0..nd-1) in the last

@@ -1013,192 +1013,219 @@ int Engine<T>::spec_segment(int *jnd_io, int S, int kept) {
     }
 }
 
-// FP64 refinement of the k converged pairs (real problems).  The converged
-// Ritz vectors of a 32-bit basis carry the basis' rounding noise, which is
-// spread over the whole spectrum; most of its residual comes from the
-// upper part.  Each vector is passed through a scaled Chebyshev filter of
-// degree kChebDegree that damps [a, b] (a = the far end of the wanted
-// Ritz values + 10% of the distance to the far spectrum bound, b = that
-// bound, both from the Ritz values seen during the solve), then a
-// Rayleigh-Ritz projection in FP64 over the filtered block gives the pairs
-// and their true residuals |A x - theta x|.  Repeated (at most kRefinePasses
-// times) until every residual is <= tol * anrm.  Operator applications are
-// counted in info->matvec.
+// FP64 refinement of the k converged pairs.  The converged Ritz vectors of a
+// 32-bit basis carry the basis' rounding noise, which is spread over the
+// whole spectrum; most of its residual comes from the far end.  Each vector
+// is passed through a scaled Chebyshev filter of degree kChebDegree that
+// damps [a, b] (a = the far end of the wanted Ritz values + 10% of the
+// distance to the far spectrum bound, b = that bound, both from the Ritz
+// values seen during the solve), then a Rayleigh-Ritz projection in FP64
+// over the filtered block (Hermitian for complex problems) gives the pairs
+// and their true residuals |A x - theta x|.  Repeated (at most
+// kRefinePasses times) until every residual is <= tol * anrm.  Operator
+// applications are counted in info->matvec.
 template <class T>
 int Engine<T>::refine_fp64(int k, double *max_res) {
-    if constexpr (kComplex) {
-        (void)k;
-        (void)max_res;
-        return 0;
-    } else {
-        constexpr int kChebDegree = 8;
-        constexpr int kRefinePasses = 3;
-        trl_info *info = info_;
-        if (k <= 0 || !(ritz_max_ > ritz_min_)) return 0;
-        const bool low = info->lohi < 0;
-        // Wanted Ritz values and the damped interval.
-        double th_lo = eval_[0], th_hi = eval_[0];
-        for (int i = 1; i < k; ++i) {
-            th_lo = std::min(th_lo, eval_[i]);
-            th_hi = std::max(th_hi, eval_[i]);
-        }
-        double a, b, ref;
-        if (low) {
-            const double top = ritz_max_ + 0.01 * (ritz_max_ - th_lo);
-            a = th_hi + 0.1 * (top - th_hi);
-            b = top;
-            ref = th_lo;
-        } else {
-            const double bot = ritz_min_ - 0.01 * (th_hi - ritz_min_);
-            a = bot;
-            b = th_lo - 0.1 * (th_lo - bot);
-            ref = th_hi;
-        }
-        if (!(b > a)) return 0;
-        const double e = 0.5 * (b - a), c = 0.5 * (b + a);
-        const double sigma1 = e / (ref - c);
-
-        Workspace &ws = workspace();
-        const size_t vec = (size_t)n_pad_;
-        const size_t kk = (size_t)k * k;
-        const size_t doubles = (2 * (size_t)k + 4) * vec + 3 * kk + 2 * kk + (size_t)k + 8 + 3 * (size_t)k;
-        if (!Workspace::ensure(&ws.refine, &ws.refine_bytes, doubles * sizeof(double))) return -5;
-        double *base = static_cast<double *>(ws.refine);
-        CK(cudaMemsetAsync(base, 0, doubles * sizeof(double), st_));
-        double *Wb = base, *AWb = Wb + k * vec, *y0 = AWb + k * vec, *y1 = y0 + vec, *ay = y1 + vec,
-               *zero = ay + vec;
-        double *dG = zero + vec, *dH = dG + kk, *dC = dH + kk, *dh = dC + kk, *dr2 = dh + 2 * kk,
-               *dout2 = dr2 + k, *dtab = dout2 + 8;  // 3k pointer slots: W columns, then [AW W] columns
-        double **tabW = reinterpret_cast<double **>(dtab);
-        double **tabAWW = tabW + k;
-        std::vector<double *> htab(3 * (size_t)k);
-        for (int j = 0; j < k; ++j) {
-            htab[j] = Wb + j * vec;
-            htab[k + j] = AWb + j * vec;
-            htab[2 * k + j] = Wb + j * vec;
-        }
-        CK(cudaMemcpyAsync(tabW, htab.data(), sizeof(double *) * 3 * k, cudaMemcpyHostToDevice, st_));
-        // Converged vectors: the caller's device evec or the host staging.
-        double *X = user_dev_ ? reinterpret_cast<double *>(evec_) : static_cast<double *>(workspace().out);
-        const long ldx = user_dev_ ? lde_ : n_pad_;
-        CK(cudaMemcpy2DAsync(Wb, vec * sizeof(double), X, ldx * sizeof(double), nrow_ * sizeof(double), k,
-                             cudaMemcpyDeviceToDevice, st_));
-        const double tol_abs = info->tol * std::max(info->anrm, 1e-300);
-        std::vector<double> G(kk), H(kk), th, Cm, r2(k);
-        std::vector<int> perm(k);
-        std::iota(perm.begin(), perm.end(), 0);
-        std::stable_sort(perm.begin(), perm.end(), [&](int i, int j) { return eval_[i] < eval_[j]; });
-        double worst = -1.0;
-        bool refined = false;
-        for (int pass = 0; pass < kRefinePasses; ++pass) {
-            for (int j = 0; j < k; ++j) {
-                double *w = Wb + j * vec;
-                // Scaled Chebyshev filter (Zhou & Saad): the wanted end keeps
-                // magnitude ~1, [a, b] is damped by ~1/T_d.
-                int rc = apply_op(w, ay, false);
-                if (rc) return rc;
-                launch_cheb(ay, w, nullptr, n_pad_, sigma1 / e, c, 0.0, y1, st_);
-                const double *prev = w;
-                double *cur = y1, *spare = y0;
-                double s1 = sigma1;
-                for (int t = 2; t <= kChebDegree; ++t) {
-                    const double s2 = 1.0 / (2.0 / sigma1 - s1);
-                    if ((rc = apply_op(cur, ay, false))) return rc;
-                    double *out = prev == w ? spare : const_cast<double *>(prev);
-                    launch_cheb(ay, cur, prev, n_pad_, 2.0 * s2 / e, c, -s1 * s2, out, st_);
-                    prev = cur;
-                    cur = out;
-                    s1 = s2;
-                }
-                CK(cudaMemcpyAsync(w, cur, vec * sizeof(double), cudaMemcpyDeviceToDevice, st_));
-                if ((rc = apply_op(w, AWb + j * vec, false))) return rc;
-                count_launch(kChebDegree);
-            }
-            // Gram matrix and projection: columns of W^T W and W^T A W.
-            for (int j = 0; j < k; ++j) {
-                launch_project<double>(tabW, k, n_pad_, Wb + j * vec, Recur<double>{}, dG + (size_t)j * k, dout2,
-                                       scratch_, st_);
-                launch_project<double>(tabW, k, n_pad_, AWb + j * vec, Recur<double>{}, dH + (size_t)j * k, dout2,
-                                       scratch_, st_);
-            }
-            count_launch(2 * k);
-            CK(cudaMemcpyAsync(G.data(), dG, sizeof(double) * kk, cudaMemcpyDeviceToHost, st_));
-            CK(cudaMemcpyAsync(H.data(), dH, sizeof(double) * kk, cudaMemcpyDeviceToHost, st_));
-            CK(cudaStreamSynchronize(st_));
-            ++syncs_;
-            for (int i = 0; i < k; ++i)
-                for (int j = 0; j < i; ++j) {
-                    G[i + j * k] = G[j + i * k] = 0.5 * (G[i + j * k] + G[j + i * k]);
-                    H[i + j * k] = H[j + i * k] = 0.5 * (H[i + j * k] + H[j + i * k]);
-                }
-            // G = Q diag(g) Q^T; B = Q g^{-1/2}; (B^T H B) Z = Z diag(theta).
-            // A filtered block that lost rank keeps the pairs of the last
-            // completed pass (or the unrefined ones).
-            std::vector<double> gl(k);
-            if (sym_eig(k, G.data(), k, gl.data()) || !(gl[0] > 1e-14 * gl[k - 1])) break;
-            std::vector<double> B(kk), P(kk), HB(kk);
-            for (int cc = 0; cc < k; ++cc)
-                for (int i = 0; i < k; ++i) B[i + cc * k] = G[i + cc * k] / std::sqrt(gl[cc]);
-            for (int cc = 0; cc < k; ++cc)
-                for (int i = 0; i < k; ++i) {
-                    double acc = 0.0;
-                    for (int j = 0; j < k; ++j) acc += H[i + j * k] * B[j + cc * k];
-                    HB[i + cc * k] = acc;
-                }
-            for (int i = 0; i < k; ++i)
-                for (int cc = 0; cc <= i; ++cc) {
-                    double acc = 0.0;
-                    for (int j = 0; j < k; ++j) acc += B[j + i * k] * HB[j + cc * k];
-                    P[i + cc * k] = P[cc + i * k] = acc;
-                }
-            th.assign(k, 0.0);
-            if (sym_eig(k, P.data(), k, th.data())) break;
-            // Coefficients of the refined vectors, placed so that the i-th
-            // smallest refined value lands where the i-th smallest of the
-            // solver's values was.
-            Cm.assign(kk, 0.0);
-            std::vector<double> hv(2 * kk);
-            for (int i = 0; i < k; ++i) {
-                const int dst = perm[i];
-                for (int r = 0; r < k; ++r) {
-                    double acc = 0.0;
-                    for (int q = 0; q < k; ++q) acc += B[r + q * k] * P[q + i * k];
-                    Cm[r + (size_t)dst * k] = acc;
-                    hv[(size_t)dst * 2 * k + r] = -acc;              // AW part
-                    hv[(size_t)dst * 2 * k + k + r] = th[i] * acc;   // W part
-                }
-                eval_[dst] = th[i];
-            }
-            CK(cudaMemcpyAsync(dC, Cm.data(), sizeof(double) * kk, cudaMemcpyHostToDevice, st_));
-            CK(cudaMemcpyAsync(dh, hv.data(), sizeof(double) * 2 * kk, cudaMemcpyHostToDevice, st_));
-            launch_ritz_out<double>(tabW, k, n_pad_, dC, k, k, X, ldx, nrow_, st_);
-            // r_c = 0 - [AW W] h_c = AW C_c - theta_c W C_c, |r_c|^2 -> dr2[c].
-            for (int cc = 0; cc < k; ++cc)
-                launch_update<double>(tabAWW, 2 * k, n_pad_, zero, Recur<double>{}, dh + (size_t)cc * 2 * k, ay,
-                                      dr2 + cc, scratch_, st_);
-            count_launch(k + 1);
-            CK(cudaMemcpyAsync(r2.data(), dr2, sizeof(double) * k, cudaMemcpyDeviceToHost, st_));
-            CK(cudaStreamSynchronize(st_));
-            ++syncs_;
-            worst = 0.0;
-            for (int i = 0; i < k; ++i) {
-                beta_[i] = std::sqrt(std::max(r2[i], 0.0));
-                worst = std::max(worst, beta_[i]);
-            }
-            refined = true;
-            if (worst <= tol_abs || pass + 1 == kRefinePasses) break;
-            CK(cudaMemcpy2DAsync(Wb, vec * sizeof(double), X, ldx * sizeof(double), nrow_ * sizeof(double), k,
-                                 cudaMemcpyDeviceToDevice, st_));
-        }
-        if (!refined) return 0;
-        if (!user_dev_) {
-            const size_t ue = sizeof(User);
-            CK(cudaMemcpy2DAsync(evec_, ue * lde_, X, ue * n_pad_, ue * nrow_, k, cudaMemcpyDeviceToHost, st_));
-            CK(cudaStreamSynchronize(st_));
-        }
-        *max_res = worst;
-        return 0;
+    using HC = std::conditional_t<kComplex, std::complex<double>, double>;
+    static_assert(sizeof(HC) == sizeof(C), "host and device scalar layouts must agree");
+    constexpr int kChebDegree = 8;
+    constexpr int kRefinePasses = 3;
+    trl_info *info = info_;
+    if (k <= 0 || !(ritz_max_ > ritz_min_)) return 0;
+    const bool low = info->lohi < 0;
+    double th_lo = eval_[0], th_hi = eval_[0];
+    for (int i = 1; i < k; ++i) {
+        th_lo = std::min(th_lo, eval_[i]);
+        th_hi = std::max(th_hi, eval_[i]);
     }
+    double a, b, ref;
+    if (low) {
+        const double top = ritz_max_ + 0.01 * (ritz_max_ - th_lo);
+        a = th_hi + 0.1 * (top - th_hi);
+        b = top;
+        ref = th_lo;
+    } else {
+        const double bot = ritz_min_ - 0.01 * (th_hi - ritz_min_);
+        a = bot;
+        b = th_lo - 0.1 * (th_lo - bot);
+        ref = th_hi;
+    }
+    if (!(b > a)) return 0;
+    const double e = 0.5 * (b - a), c = 0.5 * (b + a);
+    const double sigma1 = e / (ref - c);
+
+    Workspace &ws = workspace();
+    const size_t vec = (size_t)n_pad_;
+    const size_t kk = (size_t)k * k;
+    // Blocks W, AW, four work vectors (Chebyshev pair, operator output, zero),
+    // then G, H, the combination coefficients, the residual coefficients,
+    // |r|^2, a scalar pair and 3k column pointers (all in units of C).
+    const size_t elems = (2 * (size_t)k + 4) * vec + 2 * kk + 2 * kk + (size_t)k + 8 + 3 * (size_t)k;
+    if (!Workspace::ensure(&ws.refine, &ws.refine_bytes, elems * sizeof(C))) return -5;
+    C *base = static_cast<C *>(ws.refine);
+    CK(cudaMemsetAsync(base, 0, elems * sizeof(C), st_));
+    C *Wb = base, *AWb = Wb + k * vec, *y0 = AWb + k * vec, *y1 = y0 + vec, *ay = y1 + vec, *zero = ay + vec;
+    C *dG = zero + vec, *dH = dG + kk, *dh = dH + kk;
+    double *dr2 = reinterpret_cast<double *>(dh + 2 * kk), *dout2 = dr2 + k;
+    C **tabW = reinterpret_cast<C **>(dout2 + 8);
+    C **tabAWW = tabW + k;
+    std::vector<C *> htab(3 * (size_t)k);
+    for (int j = 0; j < k; ++j) {
+        htab[j] = Wb + j * vec;
+        htab[k + j] = AWb + j * vec;
+        htab[2 * k + j] = Wb + j * vec;
+    }
+    CK(cudaMemcpyAsync(tabW, htab.data(), sizeof(C *) * 3 * k, cudaMemcpyHostToDevice, st_));
+    // Converged vectors: the caller's device evec or the host staging.
+    C *X = user_dev_ ? reinterpret_cast<C *>(evec_) : static_cast<C *>(workspace().out);
+    const long ldx = user_dev_ ? lde_ : n_pad_;
+    CK(cudaMemcpy2DAsync(Wb, vec * sizeof(C), X, ldx * sizeof(C), nrow_ * sizeof(C), k, cudaMemcpyDeviceToDevice,
+                         st_));
+    const double tol_abs = info->tol * std::max(info->anrm, 1e-300);
+    std::vector<HC> G(kk), H(kk), hv(2 * kk);
+    std::vector<double> r2(k), th(k), gl(k);
+    std::vector<int> perm(k);
+    std::iota(perm.begin(), perm.end(), 0);
+    std::stable_sort(perm.begin(), perm.end(), [&](int i, int j) { return eval_[i] < eval_[j]; });
+    auto cj = [](const HC &v) {
+        if constexpr (kComplex)
+            return std::conj(v);
+        else
+            return v;
+    };
+    // Symmetric/Hermitian eigen-decomposition of M (k x k) into (w, Z).
+    auto eig = [&](std::vector<HC> &M, std::vector<double> &w, std::vector<HC> &Z) -> int {
+        if constexpr (kComplex) {
+            Z.assign(kk, HC(0.0));
+            return herm_eig(k, M.data(), k, w.data(), Z.data(), k);
+        } else {
+            Z = M;
+            return sym_eig(k, Z.data(), k, w.data());
+        }
+    };
+    double worst = -1.0;
+    bool refined = false;
+    for (int pass = 0; pass < kRefinePasses; ++pass) {
+        for (int j = 0; j < k; ++j) {
+            C *w = Wb + j * vec;
+            // Scaled Chebyshev filter (Zhou & Saad): the wanted end keeps
+            // magnitude ~1, [a, b] is damped by ~1/T_d.
+            int rc = apply_op(w, ay, false);
+            if (rc) return rc;
+            launch_cheb(ay, w, nullptr, n_pad_, sigma1 / e, c, 0.0, y1, st_);
+            const C *prev = w;
+            C *cur = y1, *spare = y0;
+            double s1 = sigma1;
+            for (int t = 2; t <= kChebDegree; ++t) {
+                const double s2 = 1.0 / (2.0 / sigma1 - s1);
+                if ((rc = apply_op(cur, ay, false))) return rc;
+                C *out = prev == w ? spare : const_cast<C *>(prev);
+                launch_cheb(ay, cur, prev, n_pad_, 2.0 * s2 / e, c, -s1 * s2, out, st_);
+                prev = cur;
+                cur = out;
+                s1 = s2;
+            }
+            CK(cudaMemcpyAsync(w, cur, vec * sizeof(C), cudaMemcpyDeviceToDevice, st_));
+            if ((rc = apply_op(w, AWb + j * vec, false))) return rc;
+            count_launch(kChebDegree);
+        }
+        // Columns of W^H W and W^H A W.
+        for (int j = 0; j < k; ++j) {
+            launch_project<C>(tabW, k, n_pad_, Wb + j * vec, Recur<C>{}, dG + (size_t)j * k, dout2, scratch_, st_);
+            launch_project<C>(tabW, k, n_pad_, AWb + j * vec, Recur<C>{}, dH + (size_t)j * k, dout2, scratch_, st_);
+        }
+        count_launch(2 * k);
+        CK(cudaMemcpyAsync(G.data(), dG, sizeof(C) * kk, cudaMemcpyDeviceToHost, st_));
+        CK(cudaMemcpyAsync(H.data(), dH, sizeof(C) * kk, cudaMemcpyDeviceToHost, st_));
+        CK(cudaStreamSynchronize(st_));
+        ++syncs_;
+        for (int i = 0; i < k; ++i)
+            for (int j = 0; j <= i; ++j) {
+                G[i + j * k] = 0.5 * (G[i + j * k] + cj(G[j + i * k]));
+                G[j + i * k] = cj(G[i + j * k]);
+                H[i + j * k] = 0.5 * (H[i + j * k] + cj(H[j + i * k]));
+                H[j + i * k] = cj(H[i + j * k]);
+            }
+        // G = Q diag(g) Q^H; B = Q g^{-1/2}; (B^H H B) Z = Z diag(theta).  A
+        // filtered block that lost rank keeps the pairs of the last completed
+        // pass (or the unrefined ones).
+        std::vector<HC> Q, Z, B(kk), P(kk), HB(kk);
+        if (eig(G, gl, Q) || !(gl[0] > 1e-14 * gl[k - 1])) break;
+        for (int cc = 0; cc < k; ++cc)
+            for (int i = 0; i < k; ++i) B[i + cc * k] = Q[i + cc * k] / std::sqrt(gl[cc]);
+        for (int cc = 0; cc < k; ++cc)
+            for (int i = 0; i < k; ++i) {
+                HC acc = 0.0;
+                for (int j = 0; j < k; ++j) acc += H[i + j * k] * B[j + cc * k];
+                HB[i + cc * k] = acc;
+            }
+        for (int i = 0; i < k; ++i)
+            for (int cc = 0; cc <= i; ++cc) {
+                HC acc = 0.0;
+                for (int j = 0; j < k; ++j) acc += cj(B[j + i * k]) * HB[j + cc * k];
+                P[i + cc * k] = acc;
+                P[cc + i * k] = cj(acc);
+            }
+        if (eig(P, th, Z)) break;
+        // Coefficients of the refined vectors, placed so that the i-th
+        // smallest refined value lands where the i-th smallest of the
+        // solver's values was.
+        std::vector<HC> Cm(kk);
+        for (int i = 0; i < k; ++i) {
+            const int dst = perm[i];
+            for (int r = 0; r < k; ++r) {
+                HC acc = 0.0;
+                for (int q = 0; q < k; ++q) acc += B[r + q * k] * Z[q + i * k];
+                Cm[r + (size_t)dst * k] = acc;
+                hv[(size_t)dst * 2 * k + r] = -acc;             // AW part
+                hv[(size_t)dst * 2 * k + k + r] = th[i] * acc;  // W part
+            }
+            eval_[dst] = th[i];
+        }
+        // X = W Cm.  Real: one recombination launch into X.  Complex: per
+        // column, ay = 0 - W (-Cm_c) with the update kernel, then a copy.
+        if constexpr (kComplex) {
+            std::vector<HC> neg(kk);
+            for (size_t q = 0; q < kk; ++q) neg[q] = -Cm[q];
+            CK(cudaMemcpyAsync(dG, neg.data(), sizeof(C) * kk, cudaMemcpyHostToDevice, st_));
+            for (int cc = 0; cc < k; ++cc) {
+                launch_update<C>(tabW, k, n_pad_, zero, Recur<C>{}, dG + (size_t)cc * k, ay, dout2, scratch_, st_);
+                CK(cudaMemcpyAsync(X + (size_t)cc * ldx, ay, sizeof(C) * nrow_, cudaMemcpyDeviceToDevice, st_));
+            }
+            count_launch(k);
+        } else {
+            CK(cudaMemcpyAsync(dG, Cm.data(), sizeof(C) * kk, cudaMemcpyHostToDevice, st_));
+            launch_ritz_out<double>(tabW, k, n_pad_, reinterpret_cast<const double *>(dG), k, k, X, ldx, nrow_,
+                                    st_);
+            count_launch();
+        }
+        CK(cudaMemcpyAsync(dh, hv.data(), sizeof(C) * 2 * kk, cudaMemcpyHostToDevice, st_));
+        // r_c = 0 - [AW W] h_c = AW C_c - theta_c W C_c, |r_c|^2 -> dr2[c].
+        for (int cc = 0; cc < k; ++cc)
+            launch_update<C>(tabAWW, 2 * k, n_pad_, zero, Recur<C>{}, dh + (size_t)cc * 2 * k, ay, dr2 + cc, scratch_,
+                             st_);
+        count_launch(k);
+        CK(cudaMemcpyAsync(r2.data(), dr2, sizeof(double) * k, cudaMemcpyDeviceToHost, st_));
+        CK(cudaStreamSynchronize(st_));
+        ++syncs_;
+        worst = 0.0;
+        for (int i = 0; i < k; ++i) {
+            beta_[i] = std::sqrt(std::max(r2[i], 0.0));
+            worst = std::max(worst, beta_[i]);
+        }
+        refined = true;
+        if (worst <= tol_abs || pass + 1 == kRefinePasses) break;
+        CK(cudaMemcpy2DAsync(Wb, vec * sizeof(C), X, ldx * sizeof(C), nrow_ * sizeof(C), k, cudaMemcpyDeviceToDevice,
+                             st_));
+    }
+    if (!refined) return 0;
+    if (!user_dev_) {
+        const size_t ue = sizeof(User);
+        CK(cudaMemcpy2DAsync(evec_, ue * lde_, X, ue * n_pad_, ue * nrow_, k, cudaMemcpyDeviceToHost, st_));
+        CK(cudaStreamSynchronize(st_));
+    }
+    *max_res = worst;
+    return 0;
 }
 
 template <class T>

@@ -641,6 +641,14 @@ void launch_cheb(const double *ay, const double *y, const double *yp, long n_pad
                  double *out, cudaStream_t st) {
     k_cheb<<<elementwise_blocks(n_pad), kThreads, 0, st>>>(ay, y, yp, n_pad, a, c, b, out);
 }
+// Complex vectors with real coefficients: the same recurrence on the
+// interleaved real and imaginary parts.
+void launch_cheb(const zd *ay, const zd *y, const zd *yp, long n_pad, double a, double c, double b, zd *out,
+                 cudaStream_t st) {
+    k_cheb<<<elementwise_blocks(2 * n_pad), kThreads, 0, st>>>(
+        reinterpret_cast<const double *>(ay), reinterpret_cast<const double *>(y),
+        reinterpret_cast<const double *>(yp), 2 * n_pad, a, c, b, reinterpret_cast<double *>(out));
+}
 
 #define TRLB_INST(T)                                                                              \
     template void launch_project<T>(T *const *, int, long, const Store<T>::C *, Recur<Store<T>::C>, \

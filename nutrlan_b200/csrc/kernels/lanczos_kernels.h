@@ -89,6 +89,8 @@ void launch_load(const T *src, long n, typename Store<T>::C *dst,
 // step of the scaled Chebyshev filter of the FP64 refinement.
 void launch_cheb(const double *ay, const double *y, const double *yp, long n_pad, double a, double c, double b,
                  double *out, cudaStream_t st);
+void launch_cheb(const zd *ay, const zd *y, const zd *yp, long n_pad, double a, double c, double b, zd *out,
+                 cudaStream_t st);
 
 // Smoothed uniform random vector (the breakdown restart of Gram-Schmidt);
 // rows >= n are set to zero.

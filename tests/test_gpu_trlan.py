@@ -315,3 +315,23 @@ def test_speculative_steps_match_sequential(case, monkeypatch):
     np.testing.assert_array_equal(spec.eval[:spec.nec], seq.eval[:seq.nec])
     assert torch.equal(spec.evec[:spec.nec], seq.evec[:seq.nec])
     assert spec.stats.host_syncs < seq.stats.host_syncs
+
+
+def test_c64_basis_refined_to_tolerance():
+    """Complex Hermitian (Peierls lattice) with c64 basis storage and the
+    default FP64 refinement: eigenvalues within 1e-10 relative of the c128
+    solve, true residuals <= tol * ||A||."""
+    A = ops.peierls_2d(64, phi=1.0 / 16.0)
+    x0 = ops.start_vector(A.n) + 1j * ops.start_vector(A.n, seed=7)
+    with DeviceOperator(A) as op:
+        r128 = solve(op, ned=8, maxlan=48, tol=1e-8, restart=1, maxmv=100000, start=x0)
+        r64 = solve(op, ned=8, maxlan=48, tol=1e-8, restart=1, maxmv=100000, start=x0, basis_bits=32)
+        raw = solve(op, ned=8, maxlan=48, tol=1e-8, restart=1, maxmv=100000, start=x0, basis_bits=32,
+                    refine=False)
+    assert r64.nec >= 8 and r128.nec >= 8
+    np.testing.assert_allclose(np.sort(r64.eval[:8]), np.sort(r128.eval[:8]), rtol=1e-10)
+    res = _residuals(A, r64.eval[:8], r64.evec[:8])
+    assert np.all(res <= 1.01 * 1e-8 * r64.info.anrm), res
+    assert 0.0 < r64.stats.max_true_residual <= 1e-8 * r64.info.anrm
+    res_raw = _residuals(A, raw.eval[:8], raw.evec[:8])
+    assert res_raw.max() > res.max()

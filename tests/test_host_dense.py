@@ -176,3 +176,30 @@ def test_shell_sort_tie_order_matches_reference(lib, reflib):
     lib.trlx_host_sort2(57, P(k2), P(o2))
     np.testing.assert_array_equal(k1, k2)
     np.testing.assert_array_equal(o1, o2)
+
+
+def test_hermitian_jacobi_matches_numpy(lib):
+    """trlx_host_herm_eig (used by the FP64 refinement of complex bases)
+    against numpy.linalg.eigh: eigenvalues, unitary eigenvectors, A Z = Z w,
+    including a degenerate pair."""
+    import ctypes as C
+    f = lib.trlx_host_herm_eig
+    f.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+    f.restype = C.c_int
+    rng = np.random.default_rng(4)
+    for n in (1, 2, 5, 16, 33):
+        M = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+        A = M + M.conj().T
+        if n >= 5:  # a degenerate pair
+            Q = np.linalg.qr(M)[0]
+            d = np.sort(rng.standard_normal(n))
+            d[1] = d[2]
+            A = (Q * d) @ Q.conj().T
+            A = 0.5 * (A + A.conj().T)
+        Af = np.asfortranarray(A)
+        w = np.zeros(n)
+        Z = np.zeros((n, n), dtype=np.complex128, order="F")
+        assert f(n, Af.ctypes.data, n, w.ctypes.data, Z.ctypes.data, n) == 0
+        np.testing.assert_allclose(w, np.linalg.eigvalsh(A), rtol=1e-12, atol=1e-12 * np.abs(w).max())
+        np.testing.assert_allclose(Z.conj().T @ Z, np.eye(n), atol=1e-12)
+        np.testing.assert_allclose(A @ Z, Z * w, atol=1e-11 * max(1.0, np.abs(w).max()))
