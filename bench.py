@@ -53,6 +53,7 @@ WORKLOADS = {
     "batched512": dict(kind="batched", count=512, ned=8, maxlan=32, tol=1e-8),
     "anderson128": dict(kind="anderson", L=128, W=4.0, ned=32, maxlan=128, tol=1e-8),
     "laplace128": dict(kind="laplace", L=128, ned=10, maxlan=64, tol=1.4901e-8),
+    "peierls2048": dict(kind="peierls", L=2048, phi=1.0 / 64.0, W=2.0, ned=16, maxlan=96, tol=1e-8),
 }
 
 
@@ -213,6 +214,198 @@ def run_batched(args, w, world, rank, local, pg):
     b.close()
 
 
+def run_complex(args, w, world, rank, local, pg):
+    """Complex Hermitian configuration (ztrlan): 2D tight binding on an
+    L x L periodic lattice with Peierls phases for flux phi per plaquette,
+    diagonal disorder uniform[-W/2, W/2]; smallest 16, maxlan 96, tol 1e-8.
+    A step is one ztrlan() call bounded to one thick-restart cycle (96
+    Lanczos steps + Ritz vectors); metric: Lanczos steps/s with a c128 basis
+    (c64 basis as a variant)."""
+    from nutrlan_b200 import operators as ops
+    L, ned, maxlan, tol = w["L"], w["ned"], w["maxlan"], w["tol"]
+    seed = 4242 + rank
+    metric = f"Lanczos steps/s (SpMV + full CGS reorth), peierls{L} complex Hermitian, smallest {ned}"
+    config = {"workload": f"peierls{L}: n={L * L}, flux 1/{int(round(1 / w['phi']))}, disorder "
+                          f"U[-{w['W'] / 2:g},{w['W'] / 2:g}], ned={ned}, maxlan={maxlan}, tol={tol}, "
+                          f"complex CSR, basis c128, one thick-restart cycle/step",
+              "global_batch": world, "parallelism": f"replicas x{world}",
+              "l2": "inputs larger than L2 (basis >= 6 GB, CSR 420 MB)"}
+    A = ops.peierls_2d(L, phi=w["phi"], W=w["W"], seed=seed)
+    n = A.n
+    x0 = ops.start_vector(n) + 1j * ops.start_vector(n, seed=99)
+    cpu_sample = args.cpu_sample
+
+    def reference_sample():
+        from oracle import ref
+        ref.build()
+        r = ref.trlan_csr(A, ned=ned, maxlan=cpu_sample, lohi=-1, tol=tol, restart=1, maxmv=cpu_sample,
+                          start=x0, mev=ned + 1)
+        return r["info"].matvec, r["seconds"]
+
+    cpu_desc = (f"reference ztrlan, first {cpu_sample} Lanczos steps (maxlan=maxmv={cpu_sample}) of the "
+                "same solve, OpenBLAS + OpenMP complex CSR callback")
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        times, mvs = [], []
+        for s_ in range(args.warmup + args.steps):
+            mv, dt = reference_sample()
+            if s_ >= args.warmup:
+                times.append(dt)
+                mvs.append(mv)
+        val = sum(mvs) / sum(times)
+        print(json.dumps({"impl": "reference", "metric": metric, "value": val, "unit": "steps/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+                          "config": config,
+                          "cpu_baseline": {"value": val, "unit": "steps/s", "cores": os.cpu_count(),
+                                           "kind": "reference", "sample": cpu_desc},
+                          "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from nutrlan_b200 import load, TrlInfo, TrlxOptions, TrlxStats, DeviceOperator
+    lib = load()
+    mev = ned + 1
+    op = DeviceOperator(A)
+    evec = torch.zeros((mev, n), dtype=torch.complex128, device=dev)
+    x0_dev = torch.as_tensor(x0, device=dev)
+    eval_ = np.zeros(mev)
+    misc = np.zeros(mev, dtype=np.complex128)
+    stats = TrlxStats()
+
+    def options(bits, profile):
+        o = TrlxOptions()
+        lib.trlx_default_options(C.byref(o))
+        o.basis_bits = bits
+        o.profile = profile
+        return o
+
+    def call(info, opts, maxmv, evp, opptr, applier):
+        lib.trl_init_info(C.byref(info), n, maxlan, -1, ned, tol, 1, maxmv, None)
+        info.mvparam = opptr
+        lib.trl_set_iguess(C.byref(info), 0, 1, 0, None)
+        lib.trlx_ztrlan(applier, C.byref(info), n, mev, eval_.ctypes.data, evp, n, misc.ctypes.data, mev,
+                        None, 0, C.byref(opts))
+        if info.stat != 0:
+            raise RuntimeError(f"ztrlan stat {info.stat}")
+        return info.matvec
+
+    def timed(bits, profile):
+        opts = options(bits, profile)
+        info = TrlInfo()
+        for _ in range(args.warmup):
+            evec[0].copy_(x0_dev)
+            call(info, opts, maxlan, evec.data_ptr(), op.handle.value, op.applier)
+        torch.cuda.synchronize()
+        barrier(pg)
+        sampler = ClockSampler(local) if profile else None
+        if sampler:
+            sampler.start()
+        kt, kb, kc = np.zeros(8), np.zeros(8), np.zeros(8)
+        launches, mv = 0, 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            evec[0].copy_(x0_dev)
+            mv += call(info, opts, maxlan, evec.data_ptr(), op.handle.value, op.applier)
+            lib.trlx_get_last_stats(C.byref(stats))
+            kt += np.array(stats.kernel_seconds[:])
+            kb += np.array(stats.kernel_bytes[:])
+            kc += np.array(stats.kernel_count[:])
+            launches += stats.kernel_launches
+        e1.record()
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        dt = reduce_max(pg, e0.elapsed_time(e1) * 1e-3, dev)
+        return reduce_max(pg, mv, dev) * world / dt, dt, kt, kb, kc, launches, clocks
+
+    value, dt, kt, kb, kc, launches, clocks = timed(64, 1)
+    names = ["spmv", "project", "update", "normalize", "ritz", "dot", "other", "x"]
+    dom = int(np.argmax(kt))
+    peak, peak_kind = read_peaks()
+    achieved = kb[dom] / kt[dom] / 1e9 if kt[dom] > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                "alg_bytes_per_launch": kb[dom] / max(kc[dom], 1), "launches": int(kc[dom]),
+                "per_kernel": {names[i]: {"seconds": kt[i], "GB/s": (kb[i] / kt[i] / 1e9) if kt[i] else 0,
+                                          "launches": int(kc[i])} for i in range(7) if kc[i]},
+                "spmv_plus_reorth_GBps": float((kb[0] + kb[1] + kb[2]) / max(kt[0] + kt[1] + kt[2], 1e-30) / 1e9)}
+    variants = {}
+    if not args.no_variants:
+        variants["zcsr_c64"] = timed(32, 0)[0]
+
+    e2e = None
+    if not args.no_e2e:
+        rp, ci, va = (np.ascontiguousarray(A.row_ptr), np.ascontiguousarray(A.col),
+                      np.ascontiguousarray(A.val))
+        hev = np.zeros((mev, n), dtype=np.complex128)
+        opts = options(64, 0)
+
+        def e2e_call():
+            h = C.c_void_p()
+            lib.trlx_zcsr_create(n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, 0, C.byref(h))
+            hev[0] = x0
+            mv = call(TrlInfo(), opts, maxlan, hev.ctypes.data, h.value, op.applier)
+            lib.trlx_operator_destroy(h)
+            return mv
+
+        e2e_call()
+        barrier(pg)
+        t0 = time.perf_counter()
+        mv = sum(e2e_call() for _ in range(args.steps))
+        e_wall = reduce_max(pg, time.perf_counter() - t0, dev)
+        e2e = {"value": reduce_max(pg, mv, dev) * world / e_wall, "unit": "steps/s",
+               "h2d_bytes_per_step": int(rp.nbytes + ci.nbytes + va.nbytes + 16 * n),
+               "d2h_bytes_per_step": int(16 * n * mev + 8 * mev)}
+
+    solve_rec = None
+    if args.full_solve and rank == 0:
+        from nutrlan_b200 import residual_norms
+        solve_rec = {}
+        for bits in (64, 32):
+            info = TrlInfo()
+            evec[0].copy_(x0_dev)
+            torch.cuda.synchronize()
+            ts = time.perf_counter()
+            call(info, options(bits, 0), args.solve_maxmv, evec.data_ptr(), op.handle.value, op.applier)
+            torch.cuda.synchronize()
+            ts = time.perf_counter() - ts
+            k = max(info.nec, 1)
+            res = residual_norms(op, eval_[:k], evec[:k])
+            solve_rec[f"c{2 * bits}"] = {"seconds": ts, "matvecs": info.matvec, "restarts": info.nloop,
+                                         "nec": info.nec, "max_true_residual": float(res.max()),
+                                         "anrm": info.anrm, "evals": [float(v) for v in eval_[:k]]}
+        a_, b_ = np.array(solve_rec["c128"]["evals"]), np.array(solve_rec["c64"]["evals"])
+        kk = min(len(a_), len(b_))
+        solve_rec["c64_vs_c128_max_rel_eval_diff"] = float(np.max(np.abs(np.sort(a_[:kk]) - np.sort(b_[:kk]))
+                                                                  / np.abs(np.sort(a_[:kk]))))
+    op.close()
+    del evec
+    torch.cuda.empty_cache()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            mv, dtc = reference_sample()
+            cpu = {"value": mv / dtc, "unit": "steps/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": cpu_desc, "seconds": dtc}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {e}"}
+    if rank == 0:
+        print(json.dumps({"metric": metric, "value": value, "unit": "steps/s", "n_gpus": world,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+                          "data": "synthetic (seeded disorder and start vector)", "config": config,
+                          "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                          "clocks": clocks, "variants": variants, "solve": solve_rec}), flush=True)
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -262,6 +455,11 @@ def main():
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world, rank, local, pg = dist_setup(args)
+    if w["kind"] == "peierls":
+        run_complex(args, w, world, rank, local, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
     if w["kind"] == "batched":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "batched workload: use the default workload"}))
