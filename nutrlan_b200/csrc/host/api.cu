@@ -223,9 +223,8 @@ void trl_set_iguess(trl_info *info, int nec, int iguess, int ncps, char *cpf) {
     if (cpf != NULL && cpf[0] != '\0') std::strncpy(info->oldcpf, cpf, sizeof(info->oldcpf) - 1);
     info->stat = 0;
     if (std::strlen(info->oldcpf) > 0 && info->guess > 1) {
-        char name[160];
-        std::snprintf(name, sizeof(name), "%s%04d", info->oldcpf, info->my_pe);
-        FILE *fp = std::fopen(name, "r");
+        const std::string name = trlb::pe_filename(info->oldcpf, info->my_pe, info->npes);
+        FILE *fp = std::fopen(name.c_str(), "r");
         if (fp)
             std::fclose(fp);
         else

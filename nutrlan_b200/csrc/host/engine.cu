@@ -23,6 +23,7 @@
 #include <type_traits>
 #include <cstdlib>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "../kernels/lanczos_kernels.h"
@@ -40,6 +41,17 @@ bool is_device_pointer(const void *p) {
         return false;
     }
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+std::string pe_filename(const char *prefix, int rank, int npes) {
+    int ndig = 1;
+    for (int lead = npes; lead > 9; lead /= 10) ++ndig;
+    std::string base(prefix ? prefix : "");
+    const size_t blank = base.find(' ');
+    if (blank != std::string::npos) base.resize(blank);
+    char num[32];
+    std::snprintf(num, sizeof(num), "%0*d", ndig, rank);
+    return base + num;
 }
 
 trlx_stats &last_stats() {
@@ -224,6 +236,12 @@ class Engine {
     int initial_guess(int *jnd);
     int restart_ritz(int locked, int jml, int kept, int jnd);
     int final_vectors(int jnd, int kept);
+    // Checkpoint file of the reference (trl_write_checkpoint /
+    // trl_read_checkpoint, SRC/trlaux.c:780-1014): int nrow, int jnd,
+    // jnd alphas, jnd betas, jnd + 1 vectors of nrow values.
+    template <class ColFn>
+    int write_checkpoint(int jnd, ColFn colptr);
+    int read_checkpoint(int nec, int *jnd_out);
     int refine_fp64(int k, double *max_res);
     bool spec_enabled() const;
     int spec_segment(int *jnd, int S, int kept);
@@ -765,7 +783,11 @@ int Engine<T>::initial_guess(int *jnd_out) {
     }
     // Start vector into r64_.
     if constexpr (kWide) r64_ = reinterpret_cast<C *>(col(nec));
-    if (info_->guess == 1) {
+    int kept0 = nec;  // vectors before the start vector
+    if (info_->guess > 1) {
+        if (int e = read_checkpoint(nec, &kept0)) return e;
+        if constexpr (kWide) r64_ = reinterpret_cast<C *>(col(kept0));
+    } else if (info_->guess == 1) {
         CK(cudaMemcpyAsync(r64_, evec_ + (size_t)nec * lde_, ue * nrow_,
                            user_dev_ ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st_));
     } else {
@@ -813,14 +835,14 @@ int Engine<T>::initial_guess(int *jnd_out) {
         rnrm = std::sqrt(h_scal_[kR2Post]);
     }
     const int nr = info_->nrand, no = info_->north;
-    int stt = cgs(nec, false, &rnrm, nullptr);
-    fl_ += 4 * nrow_ * ((info_->north - no) * nec + info_->nrand - nr) + nrow_;
+    int stt = cgs(kept0, false, &rnrm, nullptr);
+    fl_ += 4 * nrow_ * ((info_->north - no) * kept0 + info_->nrand - nr) + nrow_;
     if (stt) return stt;
     if constexpr (!kWide) {
         // FP64 copy of the start vector becomes q_cur.
         rotate_fp64();
     }
-    *jnd_out = nec;
+    *jnd_out = kept0;
     return 0;
 }
 
@@ -843,6 +865,85 @@ int Engine<T>::restart_ritz(int locked, int jml, int kept, int jnd) {
     for (int j = jnd + 1 + kept; j < P_; ++j) nl.push_back(lslot_[j]);
     lslot_ = nl;
     return upload_table();
+}
+
+template <class T>
+template <class ColFn>
+int Engine<T>::write_checkpoint(int jnd, ColFn colptr) {
+    const std::string name = pe_filename(info_->cpfile, info_->my_pe, info_->npes);
+    FILE *fp = std::fopen(name.c_str(), "wb");
+    if (!fp) {
+        std::printf("TRL_WRITE_CHECKPOINT: failed to open file: %s.\n", name.c_str());
+        return -221;
+    }
+    auto fail = [&](int code) {
+        std::fclose(fp);
+        return code;
+    };
+    const int nrow = nrow_;
+    if (std::fwrite(&nrow, sizeof(int), 1, fp) != 1 || std::fwrite(&jnd, sizeof(int), 1, fp) != 1) return fail(-222);
+    if (jnd > 0 && (std::fwrite(alpha_.data(), sizeof(double), jnd, fp) != (size_t)jnd ||
+                    std::fwrite(beta_.data(), sizeof(double), jnd, fp) != (size_t)jnd))
+        return fail(-222);
+    std::vector<User> h(nrow_);
+    for (int i = 0; i <= jnd; ++i) {
+        const C *src = colptr(i);
+        if (cudaMemcpyAsync(h.data(), src, sizeof(User) * nrow_, cudaMemcpyDeviceToHost, st_) != cudaSuccess ||
+            cudaStreamSynchronize(st_) != cudaSuccess)
+            return fail(-1001);
+        if (std::fwrite(h.data(), sizeof(User), nrow_, fp) != (size_t)nrow_) return fail(-222);
+    }
+    if (std::fclose(fp) != 0) return -223;
+    info_->wrds_out += jnd * (nrow_ + nrow_ + 2) + nrow_ + 2;
+    return 0;
+}
+
+// Restart from a checkpoint (guess > 1): kept vectors into columns
+// nec..nec+jf-1 with their alpha/beta, the last vector of the file becomes
+// the start vector, orthogonalised against the kept ones.  All jf + 1
+// vectors are read whatever mev is (the reference skips the last one when
+// jf >= mev).
+template <class T>
+int Engine<T>::read_checkpoint(int nec, int *jnd_out) {
+    const char *prefix = std::strlen(info_->oldcpf) > 0 ? info_->oldcpf : info_->cpfile;
+    const std::string name = pe_filename(prefix, info_->my_pe, info_->npes);
+    FILE *fp = std::fopen(name.c_str(), "rb");
+    if (!fp) {
+        std::printf("TRL_READ_CHECKPOINT: failed to open check-point file %s.\n", name.c_str());
+        return -212;
+    }
+    auto fail = [&](int code) {
+        std::fclose(fp);
+        return code;
+    };
+    int nr = 0, jf = 0;
+    if (std::fread(&nr, sizeof(int), 1, fp) != 1 || std::fread(&jf, sizeof(int), 1, fp) != 1) return fail(-215);
+    if (nr != nrow_) {
+        std::printf("TRL_READ_CHECKPOINT: Nrow mismatch.\n");
+        return fail(-213);
+    }
+    if (jf < 0 || nec + jf + 1 > maxlan_) {
+        std::printf("TRL_READ_CHECKPOINT: MAXLAN too small.");
+        return fail(-214);
+    }
+    if (jf > 0 && (std::fread(&alpha_[nec], sizeof(double), jf, fp) != (size_t)jf ||
+                   std::fread(&beta_[nec], sizeof(double), jf, fp) != (size_t)jf))
+        return fail(-215);
+    std::vector<User> h(nrow_);
+    for (int i = 0; i <= jf; ++i) {
+        if (std::fread(h.data(), sizeof(User), nrow_, fp) != (size_t)nrow_) return fail(-215);
+        C *dst = kWide ? reinterpret_cast<C *>(col(nec + i)) : r64_;
+        CK(cudaMemcpyAsync(dst, h.data(), sizeof(User) * nrow_, cudaMemcpyHostToDevice, st_));
+        if (!kWide && i < jf) {
+            launch_store<T>(r64_, n_pad_, col(nec + i), st_);
+            count_launch();
+        }
+        CK(cudaStreamSynchronize(st_));
+    }
+    std::fclose(fp);
+    info_->wrds_in = jf * (nrow_ + nrow_ + 2) + nrow_ + 2;
+    *jnd_out = nec + jf;
+    return 0;
 }
 
 // Final Ritz vectors (columns 0..jnd-1, yy_ jnd x kept) straight into the
@@ -872,12 +973,19 @@ int Engine<T>::final_vectors(int jnd, int kept) {
         CK(cudaMemcpy2DAsync(evec_, ue * lde_, tmp, ue * n_pad_, ue * nrow_, kept, cudaMemcpyDeviceToHost, st_));
     }
     // Last Lanczos vector (FP64) into column kept.
+    const C *last = kWide ? reinterpret_cast<const C *>(col(jnd)) : qa64_;
     if (kept < mev_) {
-        const C *last = kWide ? reinterpret_cast<const C *>(col(jnd)) : qa64_;
         CK(cudaMemcpyAsync(evec_ + (size_t)kept * lde_, last, ue * nrow_,
                            user_dev_ ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st_));
     }
     CK(cudaStreamSynchronize(st_));
+    if (info_->cpflag > 0) {
+        // Final state: the Ritz vectors and the last Lanczos vector.
+        return write_checkpoint(kept, [&](int i) -> const C * {
+            if (i == kept) return last;
+            return user_dev_ ? reinterpret_cast<const C *>(evec_) + (size_t)i * lde_ : tmp + (size_t)i * n_pad_;
+        });
+    }
     return 0;
 }
 
@@ -1259,7 +1367,6 @@ void Engine<T>::run() {
     int i1 = info->ned - jnd;
     int next_test = i1 + std::min(i1, std::min(6, info->ned / 2));
     int chkpnt = info->cpflag <= 0 ? info->maxmv + info->maxlan : info->maxmv / info->cpflag;
-    (void)chkpnt;
     int prek = kept;
     int j1 = kept;  // columns that map to the caller's evec on exit
 
@@ -1433,6 +1540,22 @@ void Engine<T>::run() {
             const int ne = std::min(mev_, jnd);
             if (ne > 0) std::memcpy(eval_, lambda_.data(), sizeof(double) * ne);
             j1 = std::min(jnd, mev_);
+            if (info->matvec >= chkpnt) {
+                // Kept vectors 0..jnd-1 and the residual (column jnd; its
+                // FP64 copy is q_cur for a 32-bit basis).
+                const int kj = jnd;
+                stat = write_checkpoint(kj, [&](int i) -> const C * {
+                    if constexpr (kWide) {
+                        return reinterpret_cast<const C *>(col(i));
+                    } else {
+                        if (i == kj) return qa64_;
+                        launch_load<T>(col(i), n_pad_, r64_, st_);
+                        return r64_;
+                    }
+                });
+                if (stat) break;
+                chkpnt += info->maxmv / std::max(info->cpflag, 1);
+            }
         } else {
             kept = std::min(info->nec, std::max(info->ned, mev_ - 1));
             info->nec = kept;

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "../../../include/trlx.h"
 
 namespace trlb {
@@ -31,6 +33,11 @@ void run_ztrlan(ztrl_matvec op, trl_info *info, int nrow, int mev, double *eval,
 void clear_counter(trl_info *info, int nrow, int mev, int lde);
 
 bool is_device_pointer(const void *p);
+
+// Per-process file name of the reference (trl_pe_filename,
+// SRC/trlaux.c:1047): the prefix up to its first blank, then the rank
+// zero-padded to the number of digits of npes.
+std::string pe_filename(const char *prefix, int rank, int npes);
 
 // Frees the calling thread's cached device workspace.
 void release_workspace();
