@@ -54,6 +54,7 @@ WORKLOADS = {
     "anderson128": dict(kind="anderson", L=128, W=4.0, ned=32, maxlan=128, tol=1e-8),
     "laplace128": dict(kind="laplace", L=128, ned=10, maxlan=64, tol=1.4901e-8),
     "peierls2048": dict(kind="peierls", L=2048, phi=1.0 / 64.0, W=2.0, ned=16, maxlan=96, tol=1e-8),
+    "wells256": dict(kind="wells", L=256, ned=16, maxlan=48, tol=1e-8, problems=16),
 }
 
 
@@ -406,6 +407,86 @@ def run_complex(args, w, world, rank, local, pg):
                           "clocks": clocks, "variants": variants, "solve": solve_rec}), flush=True)
 
 
+def learned_seed_ab(problems, seed0=10 ** 6, log=None):
+    """Plain vs learned-seed solves on held-out Gaussian-well operators
+    (256 x 256, smallest 16, maxlan 48, tol 1e-8) with the packaged
+    weights; per-problem wall time includes the network forward pass and
+    the start-vector construction."""
+    from nutrlan_b200.seednet import SeedNet
+    from nutrlan_b200.seed_train import evaluate, summarize
+    net = SeedNet.pretrained()
+    try:
+        recs = evaluate(net, range(seed0, seed0 + problems), 256, maxlan=48, log=log or (lambda *a: None))
+    finally:
+        net.close()
+    out = summarize(recs)
+    out["all_converged"] = bool(all(r["plain_nec"] >= 16 and r["sum_nec"] >= 16 and r["rr_nec"] >= 16
+                                    for r in recs))
+    out["max_true_residual_over_tol"] = float(max(max(r["sum_max_true_res"], r["rr_max_true_res"]) / r["tol_abs"]
+                                                  for r in recs))
+    out["max_eval_rel_diff_vs_plain"] = float(max(max(r["sum_eval_rel_diff"], r["rr_eval_rel_diff"])
+                                                  for r in recs))
+    return out
+
+
+def run_wells(args, w, world, rank, local, pg):
+    """Learned-seed configuration: time to residual <= 1e-8 on held-out
+    Gaussian-well operators, seeded by the packaged network (start vector =
+    sum of its normalised outputs) against the plain solve.  Metric: seeded
+    solves per second (whole job); the plain rate and matvec counts beside it."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference",
+                              "unavailable": "the learned seed has no counterpart in the reference; "
+                                             "its CPU baseline is the plain reference solve in cpu_baseline"}))
+        return
+    n_prob = w["problems"]
+    seed0 = 10 ** 6 + 1000 * rank
+    learned_seed_ab(2, seed0=seed0 + 500)  # warm-up (workspace, library, network)
+    for _ in range(max(args.warmup - 1, 0)):
+        learned_seed_ab(1, seed0=seed0 + 600)
+    barrier(pg)
+    sampler = ClockSampler(local)
+    sampler.start()
+    t0 = time.perf_counter()
+    ab = learned_seed_ab(n_prob, seed0=seed0)
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    seeded_s = reduce_max(pg, ab["sum_s"], dev)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import ref
+        from nutrlan_b200 import operators as ops
+        ref.build()
+        t_cpu, n_cpu, mv = 0.0, 0, 0
+        for s_ in range(seed0, seed0 + 2):
+            A, _ = ops.wells_2d(256, seed=s_)
+            o = ref.trlan_csr(A, ned=16, maxlan=48, tol=1e-8, restart=1, maxmv=100000,
+                              start=ops.start_vector(A.n))
+            t_cpu += o["seconds"]
+            n_cpu += 1
+            mv += o["info"].matvec
+        cpu = {"value": n_cpu / t_cpu, "unit": "solves/s", "cores": os.cpu_count(), "kind": "reference",
+               "sample": f"reference trlan, plain solves of {n_cpu} of the held-out operators "
+                         f"({mv / n_cpu:.0f} matvecs each), OpenBLAS + OpenMP CSR callback"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "learned-seed solves/s to residual <= 1e-8 (Gaussian wells 256x256, smallest 16)",
+            "value": world / seeded_s, "unit": "solves/s", "n_gpus": world, "steps": n_prob,
+            "warmup": args.warmup, "ms_per_step": 1e3 * seeded_s, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 solver, bf16 network",
+            "data": "synthetic (seeded well potentials, held-out seeds)",
+            "config": {"workload": "wells256: n=65536, 8 Gaussian wells, ned=16, maxlan=48, tol=1e-8, "
+                                   "CSR, seed = sum of network outputs (guess=1)",
+                       "problems_per_rank": n_prob, "parallelism": f"replicas x{world}",
+                       "l2": "operator and basis fit in L2 (latency-bound regime)"},
+            "plain_solves_per_s": world / reduce_max(pg, ab["plain_s"], dev),
+            "learned_seed": ab, "cpu_baseline": cpu, "clocks": clocks, "host_wall_s": wall}), flush=True)
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -452,9 +533,16 @@ def main():
     ap.add_argument("--full-solve", action="store_true",
                     help="also run one solve to convergence (time to solution)")
     ap.add_argument("--solve-maxmv", type=int, default=20000)
+    ap.add_argument("--no-learned-seed", action="store_true",
+                    help="skip the learned-seed A/B record of the default line")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world, rank, local, pg = dist_setup(args)
+    if w["kind"] == "wells":
+        run_wells(args, w, world, rank, local, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
     if w["kind"] == "peierls":
         run_complex(args, w, world, rank, local, pg)
         if pg is not None:
@@ -727,6 +815,12 @@ def main():
             cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {e}"}
 
+    seed_ab = None
+    if rank == 0 and world == 1 and not args.no_learned_seed:
+        try:
+            seed_ab = learned_seed_ab(8)
+        except Exception as e:  # noqa: BLE001
+            seed_ab = {"failed": str(e)}
     if rank == 0:
         line = {"metric": metric, "value": value, "unit": "steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -734,6 +828,7 @@ def main():
                 "data": "synthetic (seeded Anderson potential and start vector)", "config": config,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks, "host_wall_s": wall, "variants": variants, "solve": solve_rec,
+                "learned_seed": seed_ab,
                 "matvecs_per_call": int(matvecs // max(args.steps, 1))}
         print(json.dumps(line), flush=True)
     if pg is not None:
