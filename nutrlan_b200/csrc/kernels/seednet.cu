@@ -35,7 +35,6 @@ constexpr int kC = 32;          // channels of every activation tensor
 constexpr int kTaps = 9;
 constexpr int kLayers = 5;
 constexpr int kOut = 16;        // output vectors
-constexpr int kTilePix = 64;    // pixels per CTA in k_conv (4 warps x 16)
 constexpr int kDil[kLayers] = {1, 2, 4, 8, 1};
 constexpr int kCin[kLayers] = {1, 32, 32, 32, 32};
 constexpr int kCout[kLayers] = {32, 32, 32, 32, 16};
@@ -54,65 +53,107 @@ __device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
 }
 
 // ---------------------------------------------------------------------------
+// Shared-memory staging and fragment loads.
+constexpr int kTX = 64;      // pixels of one image row per tile
+constexpr int kMaxDil = 8;   // largest dilation (halo of a tile)
+constexpr int kRowB = 80;    // bytes per staged pixel: 32 channels + 16 B pad (ldmatrix rows hit distinct banks)
+constexpr int kRowH = kRowB / 2;
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int sz = valid ? 16 : 0;  // 0: zero-fill, nothing read
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+__device__ __forceinline__ void ldsm_x4(unsigned (&r)[4], const void *p) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x4_trans(unsigned (&r)[4], const void *p) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+
+// Stages the three input rows y - d, y, y + d of sample b, columns
+// x0 - d .. x0 + kTX - 1 + d (zero outside the image), as [row][col][40]
+// bf16.  `nth` threads cooperate.
+__device__ __forceinline__ void stage_rows(__nv_bfloat16 *xs, const __nv_bfloat16 *in, int b, int y, int x0, int H,
+                                           int W, int d, int tid, int nth) {
+    const int wid = kTX + 2 * d;
+    const int chunks = 3 * wid * 4;
+    for (int c = tid; c < chunks; c += nth) {
+        const int r = c / (wid * 4), rem = c - r * wid * 4, col = rem >> 2, q = rem & 3;
+        const int yy = y + (r - 1) * d, xx = x0 - d + col;
+        const bool ok = yy >= 0 && yy < H && xx >= 0 && xx < W;
+        const __nv_bfloat16 *src = ok ? in + ((((long)b * H + yy) * W + xx) * kC + q * 8) : in;
+        cp_async16(xs + ((size_t)r * wid + col) * kRowH + q * 8, src, ok);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // out[p, co] = act( sum_{tap, ci} in[p + d*off(tap), ci] * w[tap][co][ci] + bias[co] )
 // in: NHWC bf16 (32 ch), w: [tap][co][ci] bf16, out: NHWC bf16 (32 ch) or,
 // when out_f32 != null, FP32 [pixel][16] (first 16 channels).
-// Each warp computes 16 pixels x 32 output channels (4 n8 tiles); A
-// fragments come straight from global/L1 (32-bit channel pairs), B from
-// shared memory.  relu: 1 applies max(0, .).  mask (optional, NHWC bf16):
-// multiply the input by [mask > 0] while loading (ReLU backward fused into
-// the backward-data convolution).
+// A block computes one tile of kTX pixels of one image row for all 32
+// output channels: the three input rows the taps touch (with a halo of d
+// pixels) and all weights are staged in shared memory with cp.async, then
+// each of the 4 warps runs 9 taps x 2 k16 steps x 4 n8 tiles of
+// mma.sync m16n8k16 (bf16 -> f32) on fragments loaded with ldmatrix.
 __global__ void __launch_bounds__(128)
     k_conv(const __nv_bfloat16 *__restrict__ in, const __nv_bfloat16 *__restrict__ w, const float *__restrict__ bias,
            __nv_bfloat16 *out, float *out_f32, int B, int H, int W, int dil, int relu) {
-    __shared__ __align__(16) __nv_bfloat16 ws[kTaps * kC * kC];
-    for (int i = threadIdx.x; i < kTaps * kC * kC / 8; i += blockDim.x)
-        reinterpret_cast<uint4 *>(ws)[i] = reinterpret_cast<const uint4 *>(w)[i];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __nv_bfloat16 *ws = reinterpret_cast<__nv_bfloat16 *>(smem_raw);  // [9][32 co][40]
+    __nv_bfloat16 *xs = ws + kTaps * kC * kRowH;                         // [3][kTX + 2d][40]
+    const int tilesx = W / kTX;
+    const long tile = blockIdx.x;
+    const int xt = (int)(tile % tilesx);
+    const long by = tile / tilesx;
+    const int y = (int)(by % H), b = (int)(by / H);
+    const int x0 = xt * kTX;
+    for (int c = threadIdx.x; c < kTaps * kC * 4; c += blockDim.x)
+        cp_async16(ws + (size_t)(c >> 2) * kRowH + (c & 3) * 8, w + (size_t)(c >> 2) * kC + (c & 3) * 8, true);
+    stage_rows(xs, in, b, y, x0, H, W, dil, threadIdx.x, blockDim.x);
+    cp_async_wait_all();
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
-    const long p0 = (long)blockIdx.x * kTilePix + warp * 16;  // first pixel of this warp
-    const long HW = (long)H * W;
-    // Pixels of rows g and g + 8 of the A fragment.
-    const long pa = p0 + g, pb = p0 + g + 8;
-    const int ba = (int)(pa / HW), ya = (int)((pa % HW) / W), xa = (int)(pa % W);
-    const int bb = (int)(pb / HW), yb = (int)((pb % HW) / W), xb = (int)(pb % W);
+    const int wid = kTX + 2 * dil;
     float acc[4][4];
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[j][q] = 0.f;
-    const unsigned *in32 = reinterpret_cast<const unsigned *>(in);
-    const unsigned *w32 = reinterpret_cast<const unsigned *>(ws);
+    // ldmatrix lane roles: A rows (pixels) lane&7 (+8 for lanes 8-15 / 24-31),
+    // k half lane>>4; B rows (output channels) lane&7 of n-tile pair
+    // member lane>>4, k half (lane>>3)&1.
+    const int a_row = (lane & 7) + ((lane >> 3) & 1) * 8, a_k = (lane >> 4) * 8;
+    const int b_row = (lane & 7) + (lane >> 4) * 8, b_k = ((lane >> 3) & 1) * 8;
 #pragma unroll 1
     for (int tap = 0; tap < kTaps; ++tap) {
-        const int dy = (tap / 3 - 1) * dil, dx = (tap % 3 - 1) * dil;
-        const int ya2 = ya + dy, xa2 = xa + dx, yb2 = yb + dy, xb2 = xb + dx;
-        const bool va = ya2 >= 0 && ya2 < H && xa2 >= 0 && xa2 < W;
-        const bool vb = yb2 >= 0 && yb2 < H && xb2 >= 0 && xb2 < W;
-        const long sa = (((long)ba * H + ya2) * W + xa2) * (kC / 2);  // 32-bit words
-        const long sb = (((long)bb * H + yb2) * W + xb2) * (kC / 2);
+        const int r = tap / 3, dx = (tap % 3 - 1) * dil;
+        const __nv_bfloat16 *xrow = xs + ((size_t)r * wid + dil + dx + warp * 16 + a_row) * kRowH + a_k;
+        const __nv_bfloat16 *wt = ws + (size_t)tap * kC * kRowH;
 #pragma unroll
         for (int k0 = 0; k0 < kC; k0 += 16) {
             unsigned a[4];
-            const int c = k0 / 2 + t;  // word index of channels (k0 + 2t, +1)
-            a[0] = va ? __ldg(in32 + sa + c) : 0u;
-            a[1] = vb ? __ldg(in32 + sb + c) : 0u;
-            a[2] = va ? __ldg(in32 + sa + c + 4) : 0u;
-            a[3] = vb ? __ldg(in32 + sb + c + 4) : 0u;
+            ldsm_x4(a, xrow + k0);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int co = j * 8 + g;
-                unsigned b[2];
-                const int base = (tap * kC + co) * (kC / 2) + k0 / 2 + t;
-                b[0] = w32[base];
-                b[1] = w32[base + 4];
-                mma_bf16(acc[j], a, b);
+            for (int jp = 0; jp < 2; ++jp) {
+                unsigned bb[4];
+                ldsm_x4(bb, wt + (size_t)(jp * 16 + b_row) * kRowH + k0 + b_k);
+                const unsigned b0[2] = {bb[0], bb[1]}, b1[2] = {bb[2], bb[3]};
+                mma_bf16(acc[2 * jp], a, b0);
+                mma_bf16(acc[2 * jp + 1], a, b1);
             }
         }
     }
-    // Epilogue: rows g (pixel pa) and g + 8 (pixel pb); columns 2t, 2t+1 of
-    // each n8 tile j.
+    const long pa = (by * W) + x0 + warp * 16 + g, pb = pa + 8;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const int co = j * 8 + 2 * t;
@@ -126,16 +167,18 @@ __global__ void __launch_bounds__(128)
         }
         if (out_f32) {
             if (co < kOut) {
-                out_f32[pa * kOut + co] = v0;
-                out_f32[pa * kOut + co + 1] = v1;
-                out_f32[pb * kOut + co] = v2;
-                out_f32[pb * kOut + co + 1] = v3;
+                *reinterpret_cast<float2 *>(out_f32 + pa * kOut + co) = make_float2(v0, v1);
+                *reinterpret_cast<float2 *>(out_f32 + pb * kOut + co) = make_float2(v2, v3);
             }
         } else {
             reinterpret_cast<unsigned *>(out)[pa * (kC / 2) + co / 2] = pack_bf16(v0, v1);
             reinterpret_cast<unsigned *>(out)[pb * (kC / 2) + co / 2] = pack_bf16(v2, v3);
         }
     }
+}
+
+size_t conv_smem_bytes(int dil) {
+    return (size_t)kTaps * kC * kRowB + (size_t)3 * (kTX + 2 * dil) * kRowB;
 }
 
 // g_pre = g_post * [act > 0] (ReLU backward), NHWC bf16, elementwise.
@@ -146,101 +189,93 @@ __global__ void k_relu_mask(__nv_bfloat16 *g, const __nv_bfloat16 *act, long n) 
 
 // ---------------------------------------------------------------------------
 // Weight gradient: dW[tap][ci][co] = sum_p in[p + d*off(tap), ci] * g[p, co];
-// db[co] = sum_p g[p, co].  Block b covers pixels [b*chunk, (b+1)*chunk);
-// warp w handles taps w, w+4, w+8 (A rows = ci, k = pixels, B = g).
-// Partials part[b][tap][ci][co] (+ part[b][9][0][co] for the bias).
-constexpr int kWgPix = 2048;
+// db[co] = sum_p g[p, co].  A block of 9 warps walks a range of row tiles
+// (kTX pixels each); per tile the three input rows and the gradient tile are
+// staged with cp.async, and warp w accumulates tap w as a (32 ci) x (32 co)
+// product over the tile's pixels: A = staged input rows transposed (ldmatrix
+// .trans), B = gradient tile (ldmatrix .trans).  Per-block partials
+// part[b][tap][ci][co] (+ part[b][9][0][co] for the bias) are reduced in
+// block order by k_reduce_parts.
+constexpr int kWgWarps = kTaps;
 
-__device__ __forceinline__ unsigned ld_pair(const __nv_bfloat16 *p0, const __nv_bfloat16 *p1, bool v0, bool v1) {
-    __nv_bfloat16 lo = v0 ? *p0 : __float2bfloat16(0.f);
-    __nv_bfloat16 hi = v1 ? *p1 : __float2bfloat16(0.f);
-    __nv_bfloat162 v(lo, hi);
-    return *reinterpret_cast<unsigned *>(&v);
-}
-
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kWgWarps * 32)
     k_conv_wgrad(const __nv_bfloat16 *__restrict__ in, const __nv_bfloat16 *__restrict__ g, float *part, int B, int H,
                  int W, int dil) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __nv_bfloat16 *gs = reinterpret_cast<__nv_bfloat16 *>(smem_raw);  // [kTX][40]
+    __nv_bfloat16 *xs = gs + (size_t)kTX * kRowH;                       // [3][kTX + 2d][40]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int gi = lane >> 2, t = lane & 3;
-    const long HW = (long)H * W, P = (long)B * HW;
-    const long q0 = (long)blockIdx.x * kWgPix, q1 = min(P, q0 + kWgPix);
-    float acc[3][2][4][4];  // [tap slot][m16 tile of ci][n8 tile of co][frag]
+    const int tap = warp, r = tap / 3, dx = (tap % 3 - 1) * dil;
+    const int wid = kTX + 2 * dil;
+    const int tilesx = W / kTX;
+    const long ntiles = (long)B * H * tilesx;
+    float acc[2][4][4];
 #pragma unroll
-    for (int s = 0; s < 3; ++s)
+    for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
-        for (int mi = 0; mi < 2; ++mi)
+        for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) acc[s][mi][j][q] = 0.f;
-    float bsum = 0.f;  // bias gradient of channel `lane` (warp 0)
-    for (long k0 = q0; k0 < q1; k0 += 16) {
-        // B fragments (k = pixel, n = co): pixels k0 + 2t, +1 and +8.
-        const long pk[4] = {k0 + 2 * t, k0 + 2 * t + 1, k0 + 2 * t + 8, k0 + 2 * t + 9};
-        bool pv[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) pv[u] = pk[u] < q1;
-        unsigned bf[4][2];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int co = j * 8 + gi;
-            bf[j][0] = ld_pair(g + pk[0] * kC + co, g + pk[1] * kC + co, pv[0], pv[1]);
-            bf[j][1] = ld_pair(g + pk[2] * kC + co, g + pk[3] * kC + co, pv[2], pv[3]);
-        }
+            for (int q = 0; q < 4; ++q) acc[mi][j][q] = 0.f;
+    float bsum = 0.f;
+    // A (ci x px) from xs rows (px-major): matrices (px lo, ci lo), (px lo,
+    // ci hi), (px hi, ci lo), (px hi, ci hi) -> a0..a3.
+    const int a_px = (lane & 7) + (lane >> 4) * 8, a_ci = ((lane >> 3) & 1) * 8;
+    // B (px x co) from gs: matrices (px lo, co n), (px hi, co n), (px lo,
+    // co n+8), (px hi, co n+8).
+    const int b_px = (lane & 7) + ((lane >> 3) & 1) * 8, b_co = (lane >> 4) * 8;
+    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int xt = (int)(tile % tilesx);
+        const long by = tile / tilesx;
+        const int y = (int)(by % H), b = (int)(by / H);
+        const int x0 = xt * kTX;
+        const __nv_bfloat16 *gsrc = g + ((by * W) + x0) * kC;
+        for (int c = threadIdx.x; c < kTX * 4; c += blockDim.x)
+            cp_async16(gs + (size_t)(c >> 2) * kRowH + (c & 3) * 8, gsrc + (size_t)(c >> 2) * kC + (c & 3) * 8, true);
+        stage_rows(xs, in, b, y, x0, H, W, dil, threadIdx.x, blockDim.x);
+        cp_async_wait_all();
+        __syncthreads();
         if (warp == 0) {
-            // Bias gradient: lane sums channel `lane` over these 16 pixels.
-            for (int u = 0; u < 16; ++u)
-                if (k0 + u < q1) bsum += __bfloat162float(g[(k0 + u) * kC + lane]);
+            float s = 0.f;
+            for (int p = 0; p < kTX; ++p) s += __bfloat162float(gs[(size_t)p * kRowH + lane]);
+            bsum += s;
         }
+        const __nv_bfloat16 *xrow = xs + ((size_t)r * wid + dil + dx) * kRowH;
 #pragma unroll
-        for (int s = 0; s < 3; ++s) {
-            const int tap = warp + 4 * s;
-            if (tap >= kTaps) break;
-            const int dy = (tap / 3 - 1) * dil, dx = (tap % 3 - 1) * dil;
-            // Source pixels of the 4 k positions of this thread, shifted by the tap.
-            const __nv_bfloat16 *src[4];
-            bool sv[4];
+        for (int k0 = 0; k0 < kTX; k0 += 16) {
+            unsigned a[2][4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const long p = pk[u];
-                const int b = (int)(p / HW), y = (int)((p % HW) / W) + dy, x = (int)(p % W) + dx;
-                sv[u] = pv[u] && y >= 0 && y < H && x >= 0 && x < W;
-                src[u] = in + (((long)b * H + y) * W + x) * kC;
-            }
+            for (int mi = 0; mi < 2; ++mi) ldsm_x4_trans(a[mi], xrow + (size_t)(k0 + a_px) * kRowH + mi * 16 + a_ci);
 #pragma unroll
-            for (int mi = 0; mi < 2; ++mi) {
-                // A (m = ci, k = pixel): rows gi, gi + 8 of the ci tile mi.
-                const int ca = mi * 16 + gi, cb = ca + 8;
-                unsigned a[4];
-                a[0] = ld_pair(src[0] + ca, src[1] + ca, sv[0], sv[1]);
-                a[1] = ld_pair(src[0] + cb, src[1] + cb, sv[0], sv[1]);
-                a[2] = ld_pair(src[2] + ca, src[3] + ca, sv[2], sv[3]);
-                a[3] = ld_pair(src[2] + cb, src[3] + cb, sv[2], sv[3]);
+            for (int jp = 0; jp < 2; ++jp) {
+                unsigned bb[4];
+                ldsm_x4_trans(bb, gs + (size_t)(k0 + b_px) * kRowH + jp * 16 + b_co);
+                const unsigned b0[2] = {bb[0], bb[1]}, b1[2] = {bb[2], bb[3]};
 #pragma unroll
-                for (int j = 0; j < 4; ++j) mma_bf16(acc[s][mi][j], a, bf[j]);
+                for (int mi = 0; mi < 2; ++mi) {
+                    mma_bf16(acc[mi][2 * jp], a[mi], b0);
+                    mma_bf16(acc[mi][2 * jp + 1], a[mi], b1);
+                }
             }
         }
+        __syncthreads();
     }
     float *pb = part + (size_t)blockIdx.x * (kTaps + 1) * kC * kC;
+    float *o = pb + (size_t)tap * kC * kC;
 #pragma unroll
-    for (int s = 0; s < 3; ++s) {
-        const int tap = warp + 4 * s;
-        if (tap >= kTaps) break;
+    for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
-        for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int ci0 = mi * 16 + gi, co = j * 8 + 2 * t;
-                float *o = pb + (size_t)tap * kC * kC;
-                o[ci0 * kC + co] = acc[s][mi][j][0];
-                o[ci0 * kC + co + 1] = acc[s][mi][j][1];
-                o[(ci0 + 8) * kC + co] = acc[s][mi][j][2];
-                o[(ci0 + 8) * kC + co + 1] = acc[s][mi][j][3];
-            }
-    }
+        for (int j = 0; j < 4; ++j) {
+            const int ci0 = mi * 16 + gi, co = j * 8 + 2 * t;
+            o[ci0 * kC + co] = acc[mi][j][0];
+            o[ci0 * kC + co + 1] = acc[mi][j][1];
+            o[(ci0 + 8) * kC + co] = acc[mi][j][2];
+            o[(ci0 + 8) * kC + co + 1] = acc[mi][j][3];
+        }
     if (warp == 0) pb[(size_t)kTaps * kC * kC + lane] = bsum;
 }
+
+size_t wgrad_smem_bytes(int dil) { return (size_t)kTX * kRowB + (size_t)3 * (kTX + 2 * dil) * kRowB; }
 
 // Sum partials over blocks in order: grad[i] = sum_b part[b][i].
 __global__ void k_reduce_parts(const float *part, int nb, int stride, int len, float *grad) {
@@ -433,6 +468,12 @@ namespace {
 
 int blocks_for(long n, int t = 256) { return (int)std::min<long>((n + t - 1) / t, 148L * 16); }
 
+// Weight-gradient grid: about two blocks per SM, each walking several tiles.
+int wgrad_blocks(int B, int H, int W) {
+    const long tiles = (long)B * H * (W / kTX);
+    return (int)std::max<long>(1, std::min<long>(tiles, 148L * 2));
+}
+
 void pack_layer(trlx_seednet *net, int l) {
     k_pack<<<36, 256>>>(net->w[l], net->wf[l], net->wb[l]);
 }
@@ -443,14 +484,26 @@ void pack_input(trlx_seednet *net, int B) {
     k_pack_input<<<blocks_for((long)B * HW), 256>>>(net->Vd, net->vmin, HW, (long)B * HW, net->in_scale, net->act[0]);
 }
 
+void conv(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias, __nv_bfloat16 *out, float *out_f32,
+          int B, int H, int W, int dil, int relu) {
+    const size_t smem = conv_smem_bytes(dil);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem_bytes(kMaxDil));
+        cudaFuncSetAttribute(k_conv_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)wgrad_smem_bytes(kMaxDil));
+        attr = true;
+    }
+    const int grid = B * H * (W / kTX);
+    k_conv<<<grid, 128, smem>>>(in, w, bias, out, out_f32, B, H, W, dil, relu);
+}
+
 // Forward pass for B samples already packed in act[0]; output in net->Y.
 void forward(trlx_seednet *net, int B) {
-    const long P = (long)B * net->H * net->W;
-    const int grid = (int)(P / kTilePix);
     for (int l = 0; l < kLayers; ++l) {
         const bool last = l == kLayers - 1;
-        k_conv<<<grid, 128>>>(net->act[l], net->wf[l], net->bias[l], last ? nullptr : net->act[l + 1],
-                              last ? net->Y : nullptr, B, net->H, net->W, kDil[l], last ? 0 : 1);
+        conv(net->act[l], net->wf[l], net->bias[l], last ? nullptr : net->act[l + 1], last ? net->Y : nullptr, B,
+             net->H, net->W, kDil[l], last ? 0 : 1);
     }
 }
 
@@ -513,7 +566,7 @@ int trlx_seednet_create(int H, int W, int max_batch, unsigned long long seed, tr
     alloc((void **)&net->g0, (size_t)P * kC * 2);
     alloc((void **)&net->g1, (size_t)P * kC * 2);
     alloc((void **)&net->Y, (size_t)P * kOut * 4);
-    const long nwg = (P + kWgPix - 1) / kWgPix;
+    const long nwg = wgrad_blocks(max_batch, H, W);
     net->part_len = std::max<size_t>((size_t)nwg * (kTaps + 1) * kC * kC, (size_t)max_batch * ((H * W + kLossPix - 1) / kLossPix) * 512);
     alloc((void **)&net->part, net->part_len * 4);
     alloc((void **)&net->coef, (size_t)max_batch * 512 * 4);
@@ -586,19 +639,18 @@ static int loss_and_grad(trlx_seednet *net, int B, const float *V, const float *
     k_loss_coeffs<<<B, 256>>>(net->part, nch, lam, net->coef, net->loss);
     k_loss_grad<<<blocks_for(P), 256>>>(net->Y, net->Ud, net->coef, HW, P, 1.0f / B, net->g0);
     // Backward through the layers.
-    const int nwg = (int)((P + kWgPix - 1) / kWgPix);
+    const int nwg = wgrad_blocks(B, H, W);
     __nv_bfloat16 *g = net->g0, *gn = net->g1;
     for (int l = kLayers - 1; l >= 0; --l) {
         if (l < kLayers - 1) k_relu_mask<<<blocks_for(P * kC), 256>>>(g, net->act[l + 1], P * kC);
-        k_conv_wgrad<<<nwg, 128>>>(net->act[l], g, net->part, B, H, W, kDil[l]);
+        k_conv_wgrad<<<nwg, kWgWarps * 32, wgrad_smem_bytes(kDil[l])>>>(net->act[l], g, net->part, B, H, W, kDil[l]);
         // Partials have stride (kTaps + 1) * kC * kC; only the weight taps and
         // the kC bias entries after them are written and reduced.
         const int len = kTaps * kC * kC + kC;
         k_reduce_parts<<<(len + 255) / 256, 256>>>(net->part, nwg, (kTaps + 1) * kC * kC, len, net->gw[l]);
         cudaMemcpyAsync(net->gb[l], net->gw[l] + (size_t)kTaps * kC * kC, kC * 4, cudaMemcpyDeviceToDevice);
         if (l > 0) {
-            const int grid = (int)(P / kTilePix);
-            k_conv<<<grid, 128>>>(g, net->wb[l], nullptr, gn, nullptr, B, H, W, kDil[l], 0);
+            conv(g, net->wb[l], nullptr, gn, nullptr, B, H, W, kDil[l], 0);
             std::swap(g, gn);
         }
     }

@@ -181,8 +181,42 @@ def summarize(recs):
     return out
 
 
+def time_steps(batch, steps, L=256, lam=0.1):
+    """Wall time of training steps and forward passes on random potentials
+    and orthonormal targets (for profiling the network kernels)."""
+    import torch
+    net = SeedNet(L, L, max_batch=batch)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    V = -50.0 * torch.rand((batch, L, L), device="cuda", generator=g)
+    U = torch.randn((batch, L * L, NOUT), device="cuda", generator=g)
+    U = U / torch.linalg.vector_norm(U, dim=1, keepdim=True)
+    for _ in range(2):
+        net.train_step(V, U, lam=lam, lr=1e-3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        net.train_step(V, U, lam=lam, lr=1e-3)
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / steps
+    Y = torch.empty((batch, L * L, NOUT), device="cuda")
+    net.forward(V, out=Y)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        net.forward(V, out=Y)
+    torch.cuda.synchronize()
+    df = (time.perf_counter() - t0) / steps
+    flop_fwd = 2.0 * L * L * 9 * (1 * 32 + 3 * 32 * 32 + 32 * 16)
+    net.close()
+    return dict(batch=batch, train_ms=dt * 1e3, samples_per_s=batch / dt,
+                train_tflops=3 * flop_fwd * batch / dt / 1e12, forward_ms=df * 1e3,
+                forward_tflops=flop_fwd * batch / df / 1e12)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--time-steps", type=int, default=0,
+                    help="only time this many training steps / forward passes on random data")
     ap.add_argument("--samples", type=int, default=20000)
     ap.add_argument("--L", type=int, default=256)
     ap.add_argument("--epochs", type=int, default=30)
@@ -195,6 +229,9 @@ def main(argv=None):
     ap.add_argument("--init", default=None, help="start from these weights")
     ap.add_argument("--report", default=None, help="write a JSON report here")
     a = ap.parse_args(argv)
+    if a.time_steps:
+        print(json.dumps(time_steps(a.batch, a.time_steps, a.L)))
+        return
     rep = dict(args=vars(a))
     t0 = time.perf_counter()
     V, U, info = generate(a.samples, a.L, seed0=1, maxlan=a.maxlan)
