@@ -26,6 +26,7 @@
 #include <string>
 #include <vector>
 
+#include "../kernels/coop.h"
 #include "../kernels/lanczos_kernels.h"
 #include "../kernels/spmv.h"
 #include "dense.h"
@@ -291,6 +292,7 @@ class Engine {
     double *d_log_ = nullptr, *h_log_ = nullptr;  // speculative steps: alpha, |r|^2 pre/post, |h|^2
     long long discarded_ = 0;                     // speculative operator applications rerun
     long long spec_accepted_ = 0;
+    long long coop_segments_ = 0;
     Scratch scratch_;
     cudaStream_t st_ = nullptr;
     bool own_stream_ = false;
@@ -1069,7 +1071,29 @@ int Engine<T>::spec_segment(int *jnd_io, int S, int kept) {
     } else {
         const int j0 = *jnd_io;
         cudaEventRecord(ev_[6], st_);
-        for (int s = 1; s <= S; ++s) {
+        // Short CSR problems: the whole run in one cooperative kernel.
+        bool done = false;
+        if (builtin_->kind != 1 && n_pad_ <= (1L << 18)) {
+            const char *e = std::getenv("TRLX_COOP");
+            if (!(e && e[0] == '0')) {
+                const long part_elems = (long)scratch_.max_blocks * (P_ + 2) * (long)(sizeof(zd) / sizeof(C));
+                int pid = pbeg();
+                const int rc = launch_spec_coop<C>(builtin_, reinterpret_cast<C *const *>(d_cols_), n_pad_,
+                                                   maxlan_ + 1, j0, S, beta_[j0 - 1], d_log_,
+                                                   reinterpret_cast<C *>(scratch_.partials), part_elems, d_coef_, st_);
+                if (rc == -1001) return -1001;
+                if (rc == 0) {
+                    double bytes = 0.0;
+                    for (int s = 1; s <= S; ++s) bytes += spmv_bytes(builtin_) + (2.0 * (j0 + s) + 4.0) * nrow_ * cs();
+                    pend(pid, TRLX_K_OTHER, bytes);
+                    info_->matvec += S;
+                    count_launch();
+                    coop_segments_++;
+                    done = true;
+                }
+            }
+        }
+        for (int s = 1; s <= S && !done; ++s) {
             const int j = j0 + s;
             C *qa = reinterpret_cast<C *>(col(j - 1)), *qb = reinterpret_cast<C *>(col(j - 2)),
               *r = reinterpret_cast<C *>(col(j));

@@ -308,6 +308,7 @@ def test_speculative_steps_match_sequential(case, monkeypatch):
         monkeypatch.setenv("TRLX_SPECULATE", "0")
         seq = solve(op, ned=ned, maxlan=maxlan, tol=1e-10, restart=1, maxmv=100000, start=x0, device=True)
         monkeypatch.delenv("TRLX_SPECULATE")
+        monkeypatch.setenv("TRLX_COOP", "0")   # discrete kernels: same arithmetic as sequential
         spec = solve(op, ned=ned, maxlan=maxlan, tol=1e-10, restart=1, maxmv=100000, start=x0, device=True)
     assert seq.stats.speculative_steps == 0 and spec.stats.speculative_steps > 0
     assert spec.info.matvec == seq.info.matvec and spec.info.nloop == seq.info.nloop
@@ -335,3 +336,42 @@ def test_c64_basis_refined_to_tolerance():
     assert 0.0 < r64.stats.max_true_residual <= 1e-8 * r64.info.anrm
     res_raw = _residuals(A, raw.eval[:8], raw.evec[:8])
     assert res_raw.max() > res.max()
+
+
+@pytest.mark.parametrize("case", ["laplace64", "anderson16", "wells128", "peierls32"])
+def test_cooperative_segments_match_sequential(case, monkeypatch):
+    """Runs of speculative steps in one cooperative kernel (short CSR
+    problems): same accepted trajectory as the sequential engine up to the
+    summation order of the reductions — eigenvalues to 1e-12 relative, the
+    same number of converged pairs, residuals <= tol * ||A||, matvecs within
+    2%, and far fewer host synchronisations and launches."""
+    import torch
+    if case == "laplace64":
+        A, ned, maxlan = ops.laplacian_2d(64), 10, 40
+    elif case == "anderson16":
+        A, ned, maxlan = ops.anderson_3d(16), 12, 48
+    elif case == "wells128":
+        A, ned, maxlan = ops.wells_2d(128, seed=3)[0], 16, 48
+    else:
+        A, ned, maxlan = ops.peierls_2d(32, phi=1.0 / 16.0), 8, 40
+    x0 = ops.start_vector(A.n)
+    if np.iscomplexobj(A.val):
+        x0 = x0 + 1j * ops.start_vector(A.n, seed=7)
+    with DeviceOperator(A) as op:
+        monkeypatch.setenv("TRLX_SPECULATE", "0")
+        seq = solve(op, ned=ned, maxlan=maxlan, tol=1e-10, restart=1, maxmv=100000, start=x0, device=True)
+        monkeypatch.delenv("TRLX_SPECULATE")
+        coop = solve(op, ned=ned, maxlan=maxlan, tol=1e-10, restart=1, maxmv=100000, start=x0, device=True)
+    assert coop.stats.speculative_steps > 0
+    assert coop.nec >= ned and seq.nec >= ned
+    a, b = np.sort(coop.eval[:ned]), np.sort(seq.eval[:ned])
+    if case == "laplace64":   # degenerate spectrum: compare distinct values
+        a, b = np.unique(np.round(a, 9)), np.unique(np.round(b, 9))
+        k = min(len(a), len(b))
+        a, b = a[:k], b[:k]
+    np.testing.assert_allclose(a, b, rtol=1e-12)
+    assert abs(coop.info.matvec - seq.info.matvec) <= 0.02 * seq.info.matvec + 2
+    res = _residuals(A, coop.eval[:coop.nec], coop.evec[:coop.nec].cpu().numpy())
+    assert np.all(res <= 1.01 * 1e-10 * coop.info.anrm), res
+    assert coop.stats.host_syncs < seq.stats.host_syncs
+    assert coop.stats.kernel_launches < seq.stats.kernel_launches / 2
