@@ -148,3 +148,36 @@ def seeded_start(seed, pid, n):
     from .operators import uniform01
     s = (int(seed) + 0x9E3779B97F4A7C15 * (pid + 1)) & 0xFFFFFFFFFFFFFFFF
     return 2.0 * uniform01(s, np.arange(n, dtype=np.uint64)) - 1.0
+
+
+def main(argv=None):
+    """Solve a seeded batch of the benchmark family (L uniform in [48, 256],
+    5-point Laplacian + U[0, 2] diagonal) and print throughput; used for
+    profiling the persistent kernel."""
+    import argparse
+    import json
+    import time
+    from . import operators as ops
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--problems", type=int, default=512)
+    ap.add_argument("--threads", type=int, default=0, help="0: autotuned; 256/512/1024")
+    ap.add_argument("--format", type=int, default=-1, help="-1: autotuned; 0 stencil, 1 CSR")
+    ap.add_argument("--repeat", type=int, default=2)
+    a = ap.parse_args(argv)
+    Ls = ops.batched_sizes(a.problems, seed=777)
+    diags = [2.0 * ops.uniform01(1000 + k, np.arange(int(L) * int(L), dtype=np.uint64)) for k, L in enumerate(Ls)]
+    b = Batch.stencil5(Ls, diags)
+    kw = dict(ned=8, maxlan=32, tol=1e-8, restart=1, maxmv=100000, seed=4242, threads=a.threads, fmt=a.format)
+    for _ in range(a.repeat):
+        t0 = time.perf_counter()
+        r = b.solve(**kw)
+        dt = time.perf_counter() - t0
+    print(json.dumps({"problems": a.problems, "seconds": dt, "problems_per_s": a.problems / dt,
+                      "matvecs": int(r.info[:, 2].sum()), "solved": int((r.info[:, 1] >= 8).sum()),
+                      "bucket_threads": list(r.config.bucket_threads),
+                      "bucket_format": list(r.config.bucket_format)}))
+    b.close()
+
+
+if __name__ == "__main__":
+    main()
