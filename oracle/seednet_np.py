@@ -5,6 +5,7 @@ module restates the math that ``nutrlan_b200/csrc/kernels/seednet.cu``
 implements so that the GPU forward pass, the loss and every gradient can be
 checked on the CPU:
 
+* input (V - min V) / 50 per sample (FP32, then bfloat16);
 * 5 layers of 3x3 convolutions, dilations (1, 2, 4, 8, 1), channels
   1 -> 32 -> 32 -> 32 -> 32 -> 16, ReLU after the first four, zero "same"
   padding; out[y, x, co] = sum_{tap, ci} in[y + d*dy, x + d*dx, ci] *
@@ -78,7 +79,8 @@ def forward(params, V, emulate=True):
     layers = unpack(params)
     V = np.asarray(V, dtype=np.float32)
     x = np.zeros(V.shape + (NC,))
-    x[..., 0] = rnd(V * IN_SCALE)
+    vmin = V.min(axis=(1, 2), keepdims=True)
+    x[..., 0] = rnd((V - vmin) * IN_SCALE)
     acts = [x]
     for l, (W, b) in enumerate(layers):
         Wq = rnd(W)
