@@ -14,12 +14,13 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_functions():
     names = set()
-    for h in ("trlan.h", "ztrlan.h", "trlx.h"):
+    for h in ("trlan.h", "ztrlan.h", "trlx.h", "ftrlan.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"\b([a-z_][a-z0-9_]*)\s*\(", text):
             name = m.group(1)
-            if name.startswith(("trl", "ztrl")) and name not in ("trl_matvec", "trl_uo", "ztrl_matvec"):
+            if name.startswith(("trl", "ztrl")) and name not in ("trl_matvec", "trl_uo", "ztrl_matvec", "trl_fmatvec",
+                                                                 "ztrl_fmatvec"):
                 names.add(name)
     return names
 
