@@ -375,3 +375,26 @@ def test_cooperative_segments_match_sequential(case, monkeypatch):
     assert np.all(res <= 1.01 * 1e-10 * coop.info.anrm), res
     assert coop.stats.host_syncs < seq.stats.host_syncs
     assert coop.stats.kernel_launches < seq.stats.kernel_launches / 2
+
+
+def test_lohi_zero_whichever_converge_first_matches_reference():
+    """lohi = 0 (eigenvalues at either end, whichever converge first): every
+    converged value is an eigenvalue of the operator (dense check), its
+    residual <= tol * ||A||, and the count of converged pairs and matvecs
+    track the reference run on the same operator and start vector."""
+    A = ops.anderson_3d(12, seed=5)
+    x0 = ops.start_vector(A.n)
+    dense = np.linalg.eigvalsh(A.to_scipy().toarray())
+    with DeviceOperator(A) as op:
+        r = solve(op, ned=8, maxlan=40, lohi=0, tol=1e-9, restart=1, maxmv=20000, start=x0)
+    o = ref.trlan_csr(A, ned=8, maxlan=40, lohi=0, tol=1e-9, restart=1, maxmv=20000, start=x0)
+    assert r.stat == 0 and r.nec >= 8
+    got = r.eval[: r.nec]
+    for v in got:
+        assert np.min(np.abs(dense - v)) <= 1e-10 * max(1.0, abs(v)), v
+    res = _residuals(A, got, r.evec[: r.nec])
+    assert np.all(res <= 1.01 * 1e-9 * r.info.anrm), res
+    # Same ends converged: the sets of converged values agree.
+    ov = np.sort(o["eval"][: o["info"].nec])
+    np.testing.assert_allclose(np.sort(got)[: len(ov)], ov[: len(got)], rtol=1e-10)
+    assert abs(r.info.matvec - o["info"].matvec) <= 0.05 * o["info"].matvec + 4
