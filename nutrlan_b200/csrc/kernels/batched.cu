@@ -17,6 +17,7 @@
 // deterministic per problem regardless of which CTA solved it.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <numeric>
 #include <vector>
 
@@ -24,6 +25,7 @@
 #include "../host/dense_core.h"
 #include "../host/restart_core.h"
 #include "batched.h"
+#include "dense_warp.cuh"
 #include "common.cuh"
 
 namespace trlb {
@@ -308,8 +310,13 @@ __device__ inline int orth(const Params &P, int pid, double *V, int ld, int n, i
 // In place V[:, lck .. lck+kept) <- V[:, lck .. lck+jml) * yy (jml x kept),
 // tile by tile (the CTA owns every row, so no other reader exists).
 __device__ inline void ritz_in_place(double *V, int ld, int n, int lck, int jml, int kept, const double *yy,
-                                     double *tile /* kTile * jml */, const Grp &G) {
-    constexpr int kTile = 32;
+                                     double *tile, long tile_cap /* doubles */, const Grp &G) {
+    // As many rows per tile as the group's free shared memory holds (two
+    // group barriers per tile), rounded down to a multiple of 32 when that
+    // is at least 32; never more than the capacity.
+    int kTile = (int)min((long)n, tile_cap / max(jml, 1));
+    if (kTile >= 32) kTile = kTile / 32 * 32;
+    kTile = max(kTile, 1);
     for (int r0 = 0; r0 < n; r0 += kTile) {
         const int rows = min(kTile, n - r0);
         for (int e = G.tid; e < rows * jml; e += G.nt) {
@@ -348,7 +355,7 @@ __device__ inline void init_info(trl_info *info, int n, int maxlan, int lohi, in
 }
 
 // One complete solve of problem pid by the calling CTA.
-__device__ void solve(const Params &P, int pid, const Grp &G, double *dyn) {
+__device__ void solve(const Params &P, int pid, const Grp &G, double *dyn, long tile_cap) {
     Shared &S = *G.S;
     const Problem pr = P.probs[pid];
     const int n = pr.n, ld = pr.ld, maxlan = P.maxlan, ned = P.ned, mev = ned + 1;
@@ -392,14 +399,16 @@ __device__ void solve(const Params &P, int pid, const Grp &G, double *dyn) {
         update(V, ld, n, jnd, V + (size_t)jnd * ld, false, nullptr, nullptr, 0.0, 0.0, S.beta, G);
         stat = orth(P, pid, V, ld, n, jnd, false, 0.0, kept, G);
         if (stat) break;
-        if (G.tid == 0) {
-            for (int i = 0; i < locked; ++i) {
+        if (G.tid < 32) {
+            const int lane = G.tid;
+            for (int i = lane; i < locked; i += 32) {
                 S.alfrot[i] = S.alpha[i];
                 S.betrot[i] = 0.0;
             }
-            core::arrow_to_tridiag(jnd - locked, &S.alpha[locked], &S.beta[locked], rot, &S.alfrot[locked],
-                                   &S.betrot[locked], dws);
-            S.betrot[jnd - 1] = S.beta[jnd - 1];
+            __syncwarp();
+            warp::arrow_to_tridiag(jnd - locked, &S.alpha[locked], &S.beta[locked], rot, &S.alfrot[locked],
+                                   &S.betrot[locked], dws, lane);
+            if (lane == 0) S.betrot[jnd - 1] = S.beta[jnd - 1];
         }
         G.sync();
         while (jnd < info->klan && info->nec < info->ned) {
@@ -442,65 +451,88 @@ __device__ void solve(const Params &P, int pid, const Grp &G, double *dyn) {
             }
         }
         if (stat) break;
-        // ---- restart or finish (thread 0 decides, all apply) ----------------
-        if (G.tid == 0) {
-            int st = 0;
-            prek = kept;
+        // ---- restart or finish ------------------------------------------------
+        // Lane 0 of warp 0 takes the decisions; the O(maxlan^3) eigenvector
+        // work runs on the whole warp (dense_warp.cuh), then all apply.
+        prek = kept;
+        if (G.tid < 32) {
+            const int lane = G.tid;
+            int st = 0, go = 0, path = 0;
             const int jml = jnd - locked;
             int i2 = kept - locked + 1;
-            if (info->nec < info->ned) {
-                st = core::get_eval(jnd, locked, S.alfrot, S.betrot, S.lambda, S.res, dws);
-                if (!st) core::convergence_test(jnd, S.lambda, S.res, info, S.wrk2);
+            int kk = kept;
+            if (lane == 0) {
+                if (info->nec < info->ned) {
+                    st = core::get_eval(jnd, locked, S.alfrot, S.betrot, S.lambda, S.res, dws);
+                    if (!st) core::convergence_test(jnd, S.lambda, S.res, info, S.wrk2);
+                }
+                if (!st && info->nec < info->ned && info->matvec < info->maxmv) {
+                    go = 1;
+                    core::shuffle_eig(jml, info->klan - locked, &S.lambda[locked], &S.res[locked], info, &kk,
+                                      locked);
+                    path = kk * 3 < jml ? 1 : 2;
+                } else if (!st) {
+                    // Final: sort and compute the wanted eigenvectors.
+                    kk = min(info->nec, max(info->ned, mev - 1));
+                    info->nec = kk;
+                    if (kk == 0) kk = min(mev - 1, info->ned);
+                    core::sort_eig(jnd, info->lohi, kk, info->ref, S.lambda, S.res);
+                    for (int i = 0; i < kk; ++i) S.wrk2[i] = S.lambda[i];
+                    path = kk * 3 < jnd ? 3 : 4;
+                }
             }
-            int go = 0;
-            if (!st && info->nec < info->ned && info->matvec < info->maxmv) {
-                go = 1;
-                core::shuffle_eig(jml, info->klan - locked, &S.lambda[locked], &S.res[locked], info, &kept, locked);
-                int ts = 0;
-                if (kept * 3 < jml) {
-                    ts = core::get_tvec(jml, &S.alfrot[locked], &S.betrot[locked], 0, i2, rot, kept,
-                                        &S.lambda[locked], yy, dws);
-                    if (ts == 0)
-                        for (int i = 0; i < locked + kept; ++i) S.alpha[i] = S.lambda[i];
+            st = __shfl_sync(0xffffffffu, st, 0);
+            go = __shfl_sync(0xffffffffu, go, 0);
+            path = __shfl_sync(0xffffffffu, path, 0);
+            kk = __shfl_sync(0xffffffffu, kk, 0);
+            __syncwarp();
+            int ts = 0;
+            if (!st && go) {
+                if (path == 1) {
+                    ts = warp::get_tvec(jml, &S.alfrot[locked], &S.betrot[locked], 0, i2, rot, kk, &S.lambda[locked],
+                                        yy, dws, lane);
+                    if (ts == 0 && lane == 0)
+                        for (int i = 0; i < locked + kk; ++i) S.alpha[i] = S.lambda[i];
+                    __syncwarp();
                 }
-                if (kept * 3 >= jml || ts != 0) {
-                    for (int i = 0; i < locked + kept; ++i) S.alfrot[i] = S.lambda[i];
-                    ts = core::get_tvec_a(jml, prek - locked, &S.alpha[locked], &S.beta[locked], kept,
-                                          &S.alfrot[locked], yy, dws);
+                if (path == 2 || ts != 0) {
+                    if (lane == 0)
+                        for (int i = 0; i < locked + kk; ++i) S.alfrot[i] = S.lambda[i];
+                    __syncwarp();
+                    ts = warp::get_tvec_a(jml, prek - locked, &S.alpha[locked], &S.beta[locked], kk,
+                                          &S.alfrot[locked], yy, dws, lane);
                 }
-                if (ts) st = ts;
-                if (!st) {
-                    for (int i = 0; i < kept; ++i) S.beta[locked + i] = yy[(size_t)(i + 1) * jml - 1] * S.betrot[jnd - 1];
-                    if (jml > info->ned + (info->ned / 5 + 6))
-                        core::set_locking(jml, kept, &S.alpha[locked], &S.beta[locked], yy, info->anrm, &i2);
-                    else
-                        i2 = 0;
-                    S.ctl[cJnd] = jml;       // columns recombined
-                    S.ctl[cKept] = kept;
-                    S.ctl[cLocked] = i2;     // newly locked
+                if (lane == 0) {
+                    if (ts) st = ts;
+                    if (!st) {
+                        for (int i = 0; i < kk; ++i) S.beta[locked + i] = yy[(size_t)(i + 1) * jml - 1] * S.betrot[jnd - 1];
+                        if (jml > info->ned + (info->ned / 5 + 6))
+                            core::set_locking(jml, kk, &S.alpha[locked], &S.beta[locked], yy, info->anrm, &i2);
+                        else
+                            i2 = 0;
+                        S.ctl[cJnd] = jml;       // columns recombined
+                        S.ctl[cKept] = kk;
+                        S.ctl[cLocked] = i2;     // newly locked
+                    }
                 }
             } else if (!st) {
-                // Final: sort and compute the wanted eigenvectors.
-                kept = min(info->nec, max(info->ned, mev - 1));
-                info->nec = kept;
-                if (kept == 0) kept = min(mev - 1, info->ned);
-                core::sort_eig(jnd, info->lohi, kept, info->ref, S.lambda, S.res);
                 double *ev = S.wrk2;
-                for (int i = 0; i < kept; ++i) ev[i] = S.lambda[i];
-                int ts = 0;
-                if (kept * 3 < jnd) ts = core::get_tvec(jnd, S.alfrot, S.betrot, locked, i2, rot, kept, ev, yy, dws);
-                if (kept * 3 >= jnd || ts != 0)
-                    ts = core::get_tvec_a(jnd, prek, S.alpha, S.beta, kept, ev, yy, dws);
-                if (ts) st = ts;
-                for (int i = 0; i < kept; ++i) {
-                    S.alpha[i] = ev[i];
-                    S.beta[i] = S.betrot[jnd - 1] * yy[(size_t)(1 + i) * jnd - 1];
+                if (path == 3) ts = warp::get_tvec(jnd, S.alfrot, S.betrot, locked, i2, rot, kk, ev, yy, dws, lane);
+                if (path == 4 || ts != 0) ts = warp::get_tvec_a(jnd, prek, S.alpha, S.beta, kk, ev, yy, dws, lane);
+                if (lane == 0) {
+                    if (ts) st = ts;
+                    for (int i = 0; i < kk; ++i) {
+                        S.alpha[i] = ev[i];
+                        S.beta[i] = S.betrot[jnd - 1] * yy[(size_t)(1 + i) * jnd - 1];
+                    }
+                    S.ctl[cJnd] = jnd;
+                    S.ctl[cKept] = kk;
                 }
-                S.ctl[cJnd] = jnd;
-                S.ctl[cKept] = kept;
             }
-            S.ctl[cGo] = go;
-            S.ctl[cFlag] = st;
+            if (lane == 0) {
+                S.ctl[cGo] = go;
+                S.ctl[cFlag] = st;
+            }
         }
         G.sync();
         if (S.ctl[cFlag]) {
@@ -511,7 +543,7 @@ __device__ void solve(const Params &P, int pid, const Grp &G, double *dyn) {
         kept = S.ctl[cKept];
         if (S.ctl[cGo]) {
             // Restart: kept Ritz vectors in place, then the residual vector.
-            ritz_in_place(V, ld, n, locked, jml, kept, yy, tile, G);
+            ritz_in_place(V, ld, n, locked, jml, kept, yy, tile, tile_cap, G);
             const double *rr = V + (size_t)jnd * ld;
             double *dst = V + (size_t)(locked + kept) * ld;
             for (int i = G.tid; i < n; i += G.nt) dst[i] = rr[i];
@@ -564,11 +596,17 @@ __device__ void solve(const Params &P, int pid, const Grp &G, double *dyn) {
 // phase's queue until it is empty, then the whole CTA moves on.
 __global__ void __launch_bounds__(1024, 1) k_batched(Params P) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const size_t per_group = group_bytes_dev(P.maxlan);
     for (int f = 0; f < P.nphases; ++f) {
         const int nt = P.phase_threads[f];
         const int gidx = threadIdx.x / nt;
         const int ngroups = blockDim.x / nt;
+        // Each group gets an equal share of the CTA's shared memory; what
+        // its fixed state leaves free extends the restart tile (which starts
+        // at the dense workspace).
+        const size_t per_group = max(group_bytes_dev(P.maxlan), P.smem_total / (size_t)ngroups / 128 * 128);
+        const size_t head = (sizeof(Shared) + 15) / 16 * 16;
+        const long tile_cap =
+            (long)((per_group - head) / sizeof(double)) - 2L * P.maxlan * P.maxlan;
         if (gidx < ngroups) {
             Grp G{(int)threadIdx.x - gidx * nt, nt, 1 + gidx,
                   reinterpret_cast<Shared *>(smem + gidx * per_group)};
@@ -579,7 +617,7 @@ __global__ void __launch_bounds__(1024, 1) k_batched(Params P) {
                 const int q = G.S->ctl[cGo];
                 G.sync();
                 if (q >= P.phase_end[f]) break;
-                solve(P, P.order[q], G, dyn);
+                solve(P, P.order[q], G, dyn, tile_cap);
             }
         }
         __syncthreads();
@@ -592,19 +630,35 @@ size_t group_bytes(int maxlan) {
 // Shared memory for the largest split used by the launch.
 size_t smem_bytes(int maxlan, int min_threads) { return group_bytes(maxlan) * (1024 / min_threads); }
 
+// What a launch asks for: the split's need, raised to kLaunchSmem so the
+// restart tiles of 1024- and 512-thread groups hold a few hundred rows; the
+// rest of the SM's 256 KB stays L1 cache, which the Gram-Schmidt passes'
+// re-reads of r and the previous vectors rely on.
+constexpr size_t kLaunchSmem = 96 * 1024;
+static size_t launch_smem(int maxlan, int min_threads) {
+    static const size_t want = [] {
+        const char *e = std::getenv("TRLX_BATCH_SMEM_KB");  // tuning only
+        const long kb = e ? std::atol(e) : 0;
+        return kb > 0 ? (size_t)kb * 1024 : kLaunchSmem;
+    }();
+    return std::max(smem_bytes(maxlan, min_threads), want);
+}
+
 int launch(const Params &P, int blocks, cudaStream_t st) {
     int min_threads = 1024;
     for (int f = 0; f < P.nphases; ++f) min_threads = std::min(min_threads, P.phase_threads[f]);
-    const size_t sm = smem_bytes(P.maxlan, min_threads);
+    const size_t sm = launch_smem(P.maxlan, min_threads);
     if (cudaFuncSetAttribute(k_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
         return -1001;
-    k_batched<<<blocks, 1024, sm, st>>>(P);
+    Params Q = P;
+    Q.smem_total = sm;
+    k_batched<<<blocks, 1024, sm, st>>>(Q);
     return cudaGetLastError() == cudaSuccess ? 0 : -1001;
 }
 
 int max_blocks_per_sm(int min_threads, int maxlan) {
     int nb = 0;
-    const size_t sm = smem_bytes(maxlan, min_threads);
+    const size_t sm = launch_smem(maxlan, min_threads);
     cudaFuncSetAttribute(k_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batched, 1024, sm) != cudaSuccess) return 1;
     return std::max(nb, 1);

@@ -46,6 +46,7 @@ struct Params {
     int phase_threads[4];
     int phase_begin[4];
     int phase_end[4];
+    size_t smem_total;  // dynamic shared memory of the launch (set by launch())
 };
 
 size_t group_bytes(int maxlan);
