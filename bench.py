@@ -702,7 +702,13 @@ def main():
 
         def e2e_call():
             handle.value = None
-            lib.trlx_csr_create(n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, 0, C.byref(handle))
+            if args.format == "sell":
+                rc = lib.trlx_sell_create(n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, 1, 0,
+                                          C.byref(handle))
+            else:
+                rc = lib.trlx_csr_create(n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, 0, C.byref(handle))
+            if rc != 0:
+                raise RuntimeError(f"operator creation from host arrays failed ({rc})")
             inf = TrlInfo()
             lib.trl_init_info(C.byref(inf), n, maxlan, -1, ned, tol, 1, steps_per_call, None)
             inf.mvparam = handle.value

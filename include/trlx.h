@@ -32,7 +32,9 @@ int trlx_csr_create(int nrow, const long long *row_ptr, const int *col_idx,
                     const double *val, int where, trlx_operator **out);
 
 /* Real SELL-C-sigma (C = 32) built from CSR input; sigma >= 1 is the
-   row-sorting window (1 keeps the natural order). */
+   row-sorting window (1 keeps the natural order).  The layout is built on
+   the device (the row order of sigma > 1 on the host, from the row
+   pointers); host input arrays are copied to the device first. */
 int trlx_sell_create(int nrow, const long long *row_ptr, const int *col_idx,
                      const double *val, int sigma, int where,
                      trlx_operator **out);
@@ -42,6 +44,8 @@ int trlx_zcsr_create(int nrow, const long long *row_ptr, const int *col_idx,
                      const trl_dcomplex *val, int where,
                      trlx_operator **out);
 
+/* Waits for the device (like cudaFree), then returns the operator's memory
+   to the library's device pool. */
 void trlx_operator_destroy(trlx_operator *op);
 
 /* Number of stored entries (including SELL padding) and rows. */
@@ -258,7 +262,10 @@ typedef struct {
 void trlx_get_last_stats(trlx_stats *stats);
 
 /* Device workspace (basis pool, reduction scratch) is kept per thread
-   between solves and reused when large enough; this frees it. */
+   between solves and reused when large enough; this frees it, together with
+   the pinned host buffers of the staged host<->device copies and the device
+   memory that destroyed operators left in the library's allocation pool
+   (trlx_operator_destroy keeps it there for the next operator). */
 void trlx_release_workspace(void);
 
 /* Version string of the library. */

@@ -31,6 +31,7 @@
 #include "../kernels/spmv.h"
 #include "dense.h"
 #include "engine.h"
+#include "hostcopy.h"
 
 namespace trlb {
 
@@ -130,7 +131,11 @@ Workspace &workspace() {
     return w;
 }
 
-void release_workspace() { workspace().release(); }
+void release_workspace() {
+    workspace().release();
+    release_staging();
+    trim_operator_pools();
+}
 
 __global__ void k_zero_padding(char *pool, int nslots, size_t slot_bytes, size_t from_byte) {
     const size_t tail = slot_bytes - from_byte;
@@ -776,8 +781,8 @@ int Engine<T>::initial_guess(int *jnd_out) {
     // Locked vectors 0..nec-1 from the user's evec.
     for (int j = 0; j < nec; ++j) {
         C *dst = kWide ? reinterpret_cast<C *>(col(j)) : r64_;
-        CK(cudaMemcpyAsync(dst, evec_ + (size_t)j * lde_, ue * nrow_,
-                           user_dev_ ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st_));
+        CK(user_dev_ ? cudaMemcpyAsync(dst, evec_ + (size_t)j * lde_, ue * nrow_, cudaMemcpyDeviceToDevice, st_)
+                     : host_copy(dst, evec_ + (size_t)j * lde_, ue * nrow_, cudaMemcpyHostToDevice, st_));
         if (!kWide) {
             launch_store<T>(r64_, n_pad_, col(j), st_);
             count_launch();
@@ -790,8 +795,8 @@ int Engine<T>::initial_guess(int *jnd_out) {
         if (int e = read_checkpoint(nec, &kept0)) return e;
         if constexpr (kWide) r64_ = reinterpret_cast<C *>(col(kept0));
     } else if (info_->guess == 1) {
-        CK(cudaMemcpyAsync(r64_, evec_ + (size_t)nec * lde_, ue * nrow_,
-                           user_dev_ ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st_));
+        CK(user_dev_ ? cudaMemcpyAsync(r64_, evec_ + (size_t)nec * lde_, ue * nrow_, cudaMemcpyDeviceToDevice, st_)
+                     : host_copy(r64_, evec_ + (size_t)nec * lde_, ue * nrow_, cudaMemcpyHostToDevice, st_));
     } else {
         std::vector<User> ones(nrow_);
         for (auto &v : ones) {
@@ -812,8 +817,7 @@ int Engine<T>::initial_guess(int *jnd_out) {
             }
             fl_ += nran + nran;
         }
-        CK(cudaMemcpyAsync(r64_, ones.data(), ue * nrow_, cudaMemcpyHostToDevice, st_));
-        CK(cudaStreamSynchronize(st_));
+        CK(host_copy(r64_, ones.data(), ue * nrow_, cudaMemcpyHostToDevice, st_));
         if (nran >= nrow_) {
             launch_random<C>(r64_, nrow_, n_pad_, opt_.seed, st_);
             count_launch();
@@ -890,8 +894,7 @@ int Engine<T>::write_checkpoint(int jnd, ColFn colptr) {
     std::vector<User> h(nrow_);
     for (int i = 0; i <= jnd; ++i) {
         const C *src = colptr(i);
-        if (cudaMemcpyAsync(h.data(), src, sizeof(User) * nrow_, cudaMemcpyDeviceToHost, st_) != cudaSuccess ||
-            cudaStreamSynchronize(st_) != cudaSuccess)
+        if (host_copy(h.data(), src, sizeof(User) * nrow_, cudaMemcpyDeviceToHost, st_) != cudaSuccess)
             return fail(-1001);
         if (std::fwrite(h.data(), sizeof(User), nrow_, fp) != (size_t)nrow_) return fail(-222);
     }
@@ -935,7 +938,7 @@ int Engine<T>::read_checkpoint(int nec, int *jnd_out) {
     for (int i = 0; i <= jf; ++i) {
         if (std::fread(h.data(), sizeof(User), nrow_, fp) != (size_t)nrow_) return fail(-215);
         C *dst = kWide ? reinterpret_cast<C *>(col(nec + i)) : r64_;
-        CK(cudaMemcpyAsync(dst, h.data(), sizeof(User) * nrow_, cudaMemcpyHostToDevice, st_));
+        CK(host_copy(dst, h.data(), sizeof(User) * nrow_, cudaMemcpyHostToDevice, st_));
         if (!kWide && i < jf) {
             launch_store<T>(r64_, n_pad_, col(nec + i), st_);
             count_launch();
@@ -972,13 +975,13 @@ int Engine<T>::final_vectors(int jnd, int kept) {
     count_launch();
     const size_t ue = sizeof(User);
     if (!user_dev_ && kept > 0) {
-        CK(cudaMemcpy2DAsync(evec_, ue * lde_, tmp, ue * n_pad_, ue * nrow_, kept, cudaMemcpyDeviceToHost, st_));
+        CK(host_copy_2d(evec_, ue * lde_, tmp, ue * n_pad_, ue * nrow_, kept, cudaMemcpyDeviceToHost, st_));
     }
     // Last Lanczos vector (FP64) into column kept.
     const C *last = kWide ? reinterpret_cast<const C *>(col(jnd)) : qa64_;
     if (kept < mev_) {
-        CK(cudaMemcpyAsync(evec_ + (size_t)kept * lde_, last, ue * nrow_,
-                           user_dev_ ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st_));
+        CK(user_dev_ ? cudaMemcpyAsync(evec_ + (size_t)kept * lde_, last, ue * nrow_, cudaMemcpyDeviceToDevice, st_)
+                     : host_copy(evec_ + (size_t)kept * lde_, last, ue * nrow_, cudaMemcpyDeviceToHost, st_));
     }
     CK(cudaStreamSynchronize(st_));
     if (info_->cpflag > 0) {
@@ -1353,8 +1356,7 @@ int Engine<T>::refine_fp64(int k, double *max_res) {
     if (!refined) return 0;
     if (!user_dev_) {
         const size_t ue = sizeof(User);
-        CK(cudaMemcpy2DAsync(evec_, ue * lde_, X, ue * n_pad_, ue * nrow_, k, cudaMemcpyDeviceToHost, st_));
-        CK(cudaStreamSynchronize(st_));
+        CK(host_copy_2d(evec_, ue * lde_, X, ue * n_pad_, ue * nrow_, k, cudaMemcpyDeviceToHost, st_));
     }
     *max_res = worst;
     return 0;

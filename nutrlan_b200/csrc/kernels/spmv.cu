@@ -7,12 +7,15 @@
 // value/index load of a warp is one 128/256-byte segment.  Both fuse the
 // Lanczos alpha = x^H y into the same pass.
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
 #include "../../../include/trlx.h"
 #include "spmv.h"
+#include "../host/hostcopy.h"
 
 namespace trlb {
 
@@ -262,6 +265,77 @@ double spmv_bytes(const trlx_operator *A) {
     return b;
 }
 
+// ---- SELL-C-32 construction ------------------------------------------------
+// Stored row r of slice s = r / 32 is original row perm[r] (r without a
+// permutation).  Slice s holds width(s) = max row length of its 32 rows
+// entries per row, column-major: entry k of stored row s*32+l at
+// slice_ptr[s] + 32k + l.  Padding entries have value 0 and the column of
+// their own row (row 0 for the rows past nrow), so they read a valid x.
+
+namespace {
+
+__global__ void k_slice_width(int nrow, int nslice, const long long *__restrict__ rp,
+                              const int *__restrict__ perm, int *__restrict__ width) {
+    const int lane = threadIdx.x & 31;
+    const long warps = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long s = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nslice; s += warps) {
+        const long r = s * 32 + lane;
+        long long len = 0;
+        if (r < nrow) {
+            const long o = perm ? perm[r] : r;
+            len = rp[o + 1] - rp[o];
+        }
+        for (int d = 16; d; d >>= 1) len = max(len, __shfl_xor_sync(0xffffffffu, len, d));
+        if (lane == 0) width[s] = (int)len;
+    }
+}
+
+__global__ void k_sell_fill(int nrow, int nslice, const long long *__restrict__ rp, const int *__restrict__ ci,
+                            const double *__restrict__ va, const int *__restrict__ perm,
+                            const long long *__restrict__ sp, int *__restrict__ sc, double *__restrict__ sv) {
+    const int lane = threadIdx.x & 31;
+    const long warps = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long s = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nslice; s += warps) {
+        const long r = s * 32 + lane;
+        const long o = r < nrow ? (perm ? perm[r] : r) : -1;
+        const long long beg = o >= 0 ? rp[o] : 0;
+        const long long len = o >= 0 ? rp[o + 1] - beg : 0;
+        const long long base = sp[s];
+        const long long w = (sp[s + 1] - base) >> 5;
+        const int pad_col = o >= 0 ? (int)o : 0;
+        for (long long k = 0; k < w; ++k) {
+            const long long d = base + 32 * k + lane;
+            if (k < len) {
+                sc[d] = ci[beg + k];
+                sv[d] = va[beg + k];
+            } else {
+                sc[d] = pad_col;
+                sv[d] = 0.0;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+int sell_build_grid(int nslice) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+    const long need = ((long)nslice + 7) / 8;  // 8 warps (slices) per 256-thread block
+    return (int)std::max<long>(1, std::min<long>(need, (long)sms * 8));
+}
+
+void launch_slice_width(int nrow, int nslice, const long long *rp, const int *perm, int *width, int grid) {
+    k_slice_width<<<grid, 256>>>(nrow, nslice, rp, perm, width);
+}
+
+void launch_sell_fill(int nrow, int nslice, const long long *rp, const int *ci, const double *va, const int *perm,
+                      const long long *sp, int *sc, double *sv, int grid) {
+    k_sell_fill<<<grid, 256>>>(nrow, nslice, rp, ci, va, perm, sp, sc, sv);
+}
+
 }  // namespace trlb
 
 // ---------------------------------------------------------------------------
@@ -269,16 +343,81 @@ double spmv_bytes(const trlx_operator *A) {
 // ---------------------------------------------------------------------------
 namespace {
 
+// Device memory of the built-in operators comes from a per-device
+// stream-ordered pool that keeps what is freed (release threshold
+// unlimited): creating and destroying operators of similar size again and
+// again then reuses the same memory instead of going through the driver's
+// allocation path, where GB-sized cudaMalloc/cudaFree calls on a busy host
+// now and then take hundreds of milliseconds.  trlx_release_workspace()
+// returns the unused pool memory.  Devices without pool support use
+// cudaMalloc/cudaFree.
+constexpr int kMaxDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kMaxDevices] = {};
+int g_pool_state[kMaxDevices] = {};  // 0 not tried, 1 pool, -1 no pool
+
+cudaMemPool_t op_pool(int dev) {
+    if (dev < 0 || dev >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    if (g_pool_state[dev] == 0) {
+        g_pool_state[dev] = -1;
+        int supported = 0;
+        cudaDeviceGetAttribute(&supported, cudaDevAttrMemoryPoolsSupported, dev);
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if (supported && cudaMemPoolCreate(&pool, &props) == cudaSuccess) {
+            uint64_t keep = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            g_pool[dev] = pool;
+            g_pool_state[dev] = 1;
+        } else {
+            cudaGetLastError();
+        }
+    }
+    return g_pool[dev];
+}
+
+int current_device() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return dev;
+}
+
+// Allocation on the current device, ordered on the legacy default stream
+// (every use of operator memory comes after a synchronisation).
+cudaError_t op_alloc(void **p, size_t bytes) {
+    cudaMemPool_t pool = op_pool(current_device());
+    cudaError_t e = pool ? cudaMallocFromPoolAsync(p, bytes, pool, 0) : cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+    }
+    return e;
+}
+
+// Free on the current device (the one the memory was allocated on).
+void op_free(void *p) {
+    if (!p) return;
+    if (op_pool(current_device()))
+        cudaFreeAsync(p, 0);
+    else
+        cudaFree(p);
+}
+
 template <class X>
 int to_device(const X *src, size_t count, int where, X **dst) {
     if (count == 0) {
         *dst = nullptr;
         return 0;
     }
-    if (cudaMalloc(reinterpret_cast<void **>(dst), count * sizeof(X)) != cudaSuccess) return -2;
-    cudaMemcpyKind kind = where == TRLX_DEVICE_ARRAYS ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    if (cudaMemcpy(*dst, src, count * sizeof(X), kind) != cudaSuccess) return -3;
-    return 0;
+    if (op_alloc(reinterpret_cast<void **>(dst), count * sizeof(X)) != cudaSuccess) return -2;
+    cudaError_t e = where == TRLX_DEVICE_ARRAYS
+                        ? cudaMemcpy(*dst, src, count * sizeof(X), cudaMemcpyDeviceToDevice)
+                        : trlb::host_copy(*dst, src, count * sizeof(X), cudaMemcpyHostToDevice, 0);
+    return e == cudaSuccess ? 0 : -3;
 }
 
 template <class X>
@@ -355,69 +494,80 @@ extern "C" int trlx_sell_create(int nrow, const long long *row_ptr, const int *c
                                 const double *val, int sigma, int where, trlx_operator **out) {
     if (!out || check_csr(nrow, row_ptr, col_idx, val)) return -1;
     if (sigma < 1) sigma = 1;
-    std::vector<long long> rp = to_host(row_ptr, (size_t)nrow + 1, where);
-    const long long nnz = rp[nrow];
-    std::vector<int> ci = to_host(col_idx, (size_t)nnz, where);
-    std::vector<double> va = to_host(val, (size_t)nnz, where);
-    // Within windows of sigma rows, order rows by decreasing length.
-    std::vector<int> order(nrow);
-    std::iota(order.begin(), order.end(), 0);
+    const bool dev = where == TRLX_DEVICE_ARRAYS;
+    long long nnz = 0;
+    if (dev)
+        cudaMemcpy(&nnz, row_ptr + nrow, sizeof(long long), cudaMemcpyDeviceToHost);
+    else
+        nnz = row_ptr[nrow];
+    // Within windows of sigma rows, order rows by decreasing length (stable):
+    // host work on the row pointers only.
+    std::vector<int> order;
     if (sigma > 1) {
+        std::vector<long long> rp = to_host(row_ptr, (size_t)nrow + 1, where);
+        order.resize(nrow);
+        std::iota(order.begin(), order.end(), 0);
         for (long w0 = 0; w0 < nrow; w0 += sigma) {
             long w1 = std::min<long>(nrow, w0 + sigma);
             std::stable_sort(order.begin() + w0, order.begin() + w1, [&](int a, int b) {
                 return (rp[a + 1] - rp[a]) > (rp[b + 1] - rp[b]);
             });
         }
-    }
-    const int nslice = (nrow + 31) / 32;
-    std::vector<long long> sp(nslice + 1, 0);
-    for (int s = 0; s < nslice; ++s) {
-        long long w = 0;
-        for (int l = 0; l < 32; ++l) {
-            long r = (long)s * 32 + l;
-            if (r < nrow) w = std::max(w, rp[order[r] + 1] - rp[order[r]]);
-        }
-        sp[s + 1] = sp[s] + w * 32;
-    }
-    const long long total = sp[nslice];
-    std::vector<int> sc(total, 0);
-    std::vector<double> sv(total, 0.0);
-    for (int s = 0; s < nslice; ++s) {
-        const long long w = (sp[s + 1] - sp[s]) / 32;
-        for (int l = 0; l < 32; ++l) {
-            long r = (long)s * 32 + l;
-            int orig = r < nrow ? order[r] : -1;
-            long long len = orig >= 0 ? rp[orig + 1] - rp[orig] : 0;
-            for (long long k = 0; k < w; ++k) {
-                long long dst = sp[s] + k * 32 + l;
-                if (k < len) {
-                    sc[dst] = ci[rp[orig] + k];
-                    sv[dst] = va[rp[orig] + k];
-                } else {
-                    // Padding: zero value, column of the row itself (always valid).
-                    sc[dst] = orig >= 0 ? orig : 0;
-                    sv[dst] = 0.0;
-                }
-            }
-        }
+        bool identity = true;
+        for (int i = 0; i < nrow && identity; ++i) identity = (order[i] == i);
+        if (identity) order.clear();
     }
     auto *A = new trlx_operator();
     A->kind = 1;
     A->nrow = nrow;
-    A->nnz = total;
-    A->nslice = nslice;
+    A->nslice = (nrow + 31) / 32;
     A->sigma = sigma;
     cudaGetDevice(&A->device);
-    int rc = to_device(sp.data(), sp.size(), TRLX_HOST_ARRAYS, &A->slice_ptr);
-    if (!rc) rc = to_device(sc.data(), sc.size(), TRLX_HOST_ARRAYS, &A->col);
+    // CSR arrays on the device (the caller's own when they already are).
+    long long *d_rp = dev ? const_cast<long long *>(row_ptr) : nullptr;
+    int *d_ci = dev ? const_cast<int *>(col_idx) : nullptr;
+    double *d_va = dev ? const_cast<double *>(val) : nullptr;
+    int *d_w = nullptr;
+    int rc = 0;
+    if (!dev) {
+        rc = to_device(row_ptr, (size_t)nrow + 1, where, &d_rp);
+        if (!rc) rc = to_device(col_idx, (size_t)nnz, where, &d_ci);
+        if (!rc) rc = to_device(val, (size_t)nnz, where, &d_va);
+    }
+    if (!rc && !order.empty()) rc = to_device(order.data(), order.size(), TRLX_HOST_ARRAYS, &A->perm);
+    // Slice widths on the device, their prefix sum on the host (nrow/32 values).
+    const int nslice = A->nslice;
+    const int grid = trlb::sell_build_grid(nslice);
+    std::vector<long long> sp(nslice + 1, 0);
+    if (!rc && op_alloc(reinterpret_cast<void **>(&d_w), sizeof(int) * nslice) != cudaSuccess) rc = -2;
+    if (!rc) {
+        trlb::launch_slice_width(nrow, nslice, d_rp, A->perm, d_w, grid);
+        std::vector<int> w(nslice);
+        if (cudaMemcpy(w.data(), d_w, sizeof(int) * nslice, cudaMemcpyDeviceToHost) != cudaSuccess) rc = -3;
+        for (int s = 0; s < nslice && !rc; ++s) sp[s + 1] = sp[s] + 32LL * w[s];
+    }
+    if (!rc) rc = to_device(sp.data(), sp.size(), TRLX_HOST_ARRAYS, &A->slice_ptr);
+    const long long total = sp[nslice];
+    A->nnz = total;
     double *dv = nullptr;
-    if (!rc) rc = to_device(sv.data(), sv.size(), TRLX_HOST_ARRAYS, &dv);
+    if (!rc && (op_alloc(reinterpret_cast<void **>(&A->col), sizeof(int) * std::max<long long>(total, 1)) !=
+                    cudaSuccess ||
+                op_alloc(reinterpret_cast<void **>(&dv), sizeof(double) * std::max<long long>(total, 1)) !=
+                    cudaSuccess))
+        rc = -2;
     A->val = dv;
-    bool identity = true;
-    for (int i = 0; i < nrow && identity; ++i) identity = (order[i] == i);
-    if (!rc && !identity) rc = to_device(order.data(), order.size(), TRLX_HOST_ARRAYS, &A->perm);
+    if (!rc) {
+        trlb::launch_sell_fill(nrow, nslice, d_rp, d_ci, d_va, A->perm, A->slice_ptr, A->col, dv, grid);
+        if (cudaDeviceSynchronize() != cudaSuccess) rc = -3;
+    }
+    op_free(d_w);
+    if (!dev) {
+        op_free(d_rp);
+        op_free(d_ci);
+        op_free(d_va);
+    }
     if (rc) {
+        cudaGetLastError();
         trlx_operator_destroy(A);
         return rc;
     }
@@ -427,13 +577,30 @@ extern "C" int trlx_sell_create(int nrow, const long long *row_ptr, const int *c
 
 extern "C" void trlx_operator_destroy(trlx_operator *A) {
     if (!A) return;
-    cudaFree(A->row_ptr);
-    cudaFree(A->col);
-    cudaFree(A->val);
-    cudaFree(A->slice_ptr);
-    cudaFree(A->perm);
+    // Like cudaFree: work still running on any stream of the device may read
+    // the operator, so wait for the device before the memory is reused.
+    int prev = current_device();
+    if (A->device >= 0 && A->device != prev) cudaSetDevice(A->device);
+    cudaDeviceSynchronize();
+    op_free(A->row_ptr);
+    op_free(A->col);
+    op_free(A->val);
+    op_free(A->slice_ptr);
+    op_free(A->perm);
+    cudaStreamSynchronize(0);
+    if (A->device >= 0 && A->device != prev) cudaSetDevice(prev);
     delete A;
 }
+
+namespace trlb {
+
+void trim_operator_pools() {
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    for (int d = 0; d < kMaxDevices; ++d)
+        if (g_pool[d]) cudaMemPoolTrimTo(g_pool[d], 0);
+}
+
+}  // namespace trlb
 
 extern "C" long long trlx_operator_nnz(const trlx_operator *A) { return A ? A->nnz : 0; }
 extern "C" int trlx_operator_nrow(const trlx_operator *A) { return A ? A->nrow : 0; }

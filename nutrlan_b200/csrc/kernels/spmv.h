@@ -40,4 +40,7 @@ void spmv_plain(const trlx_operator *A, const void *x, void *y, cudaStream_t st)
 // Algorithmic bytes of one product (values + indices + row pointers + x + y).
 double spmv_bytes(const trlx_operator *A);
 
+// Returns the unused memory of the operators' device pools.
+void trim_operator_pools();
+
 }  // namespace trlb
