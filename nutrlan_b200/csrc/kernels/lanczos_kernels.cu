@@ -448,6 +448,126 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------
+// Real bases: the same product on the FP64 tensor-core instruction
+// (mma.sync.m8n8k4.f64).  A block of 8 warps computes BM x BN outputs; each
+// warp owns a 32 x 32 tile (4 x 4 mma tiles of 8 x 8, 32 accumulators per
+// thread), so 8 fragment loads from shared memory feed 16 mma (4096 FMAs).
+// K advances 16 columns per shared-memory stage (4 mma k-steps) with the
+// next stage prefetched into registers.  Shared tiles are k-major with a row
+// pitch of (rows + 8) doubles: a warp's fragment loads (8 rows x 4 k) then
+// touch every bank exactly twice, the minimum for 256 bytes.
+// Fragment layout of m8n8k4 .f64 (g = lane / 4, t = lane % 4):
+// A (row-major 8x4): a = A[g][t]; B (col-major 4x8): b = B[t][g];
+// C/D (8x8): c0, c1 = C[g][2t], C[g][2t+1].
+template <int BN>
+struct MmaShape {
+    static constexpr int WC = BN / 32;      // warps along columns
+    static constexpr int WR = 8 / WC;       // warps along rows
+    static constexpr int BM = 32 * WR;      // rows per block (256 or 128)
+};
+
+__device__ __forceinline__ void mma_f64(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <class T, class OutT, int BN>
+__global__ void __launch_bounds__(kThreads)
+    k_ritz_mma(T *const *__restrict__ in_cols, int jml, const double *__restrict__ Y, int ldy, int kept,
+               OutT *const *out_cols, OutT *out, long ldo, long n_valid) {
+    using S = Store<T>;
+    using Sh = MmaShape<BN>;
+    constexpr int BM = Sh::BM, APITCH = BM + 8, BPITCH = BN + 8;
+    constexpr int R = S::R;              // elements per 16-byte load
+    constexpr int CH = BM / R / 16;      // 16-byte chunks per thread per stage
+    constexpr int BPT = BN * kBK / kThreads;
+    __shared__ __align__(16) double As[kBK][APITCH];
+    __shared__ double Bs[kBK][BPITCH];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int g = lane >> 2, tg = lane & 3;
+    const int wr = warp % Sh::WR, wc = warp / Sh::WR;
+    const long i0 = (long)blockIdx.x * BM;
+    const int k0 = blockIdx.y * BN;
+    // Stage loads: 16 threads per column (a_kk = t / 16); thread chunk j
+    // covers rows ((t % 16) + 16 j) * R .. + R, so 16 consecutive threads read
+    // 256 contiguous bytes and write 16 consecutive smem chunks.
+    const int a_kk = t >> 4, a_ch = t & 15;
+    double areg[CH * R];
+    double breg[BPT];
+    auto load_stage = [&](int c0) {
+        const int c = c0 + a_kk;
+        if (c < jml) {
+            const T *col = in_cols[c] + i0;
+#pragma unroll
+            for (int j = 0; j < CH; ++j) {
+                double v[R];
+                S::load(col + (a_ch + 16 * j) * R, v);
+#pragma unroll
+                for (int r = 0; r < R; ++r) areg[j * R + r] = v[r];
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < CH * R; ++q) areg[q] = 0.0;
+        }
+#pragma unroll
+        for (int e = 0; e < BPT; ++e) {
+            const int idx = t + e * kThreads;
+            const int kk = idx / BN, kc = idx % BN;
+            const int cc = c0 + kk, k = k0 + kc;
+            breg[e] = (cc < jml && k < kept) ? Y[(long)cc + (long)k * ldy] : 0.0;
+        }
+    };
+    double acc[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    load_stage(0);
+    for (int c0 = 0; c0 < jml; c0 += kBK) {
+#pragma unroll
+        for (int j = 0; j < CH; ++j)
+#pragma unroll
+            for (int r = 0; r < R; r += 2)
+                *reinterpret_cast<double2 *>(&As[a_kk][(a_ch + 16 * j) * R + r]) =
+                    make_double2(areg[j * R + r], areg[j * R + r + 1]);
+#pragma unroll
+        for (int e = 0; e < BPT; ++e) {
+            const int idx = t + e * kThreads;
+            Bs[idx / BN][idx % BN] = breg[e];
+        }
+        __syncthreads();
+        if (c0 + kBK < jml) load_stage(c0 + kBK);
+#pragma unroll
+        for (int ks = 0; ks < kBK; ks += 4) {
+            double a[4], b[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) a[q] = As[ks + tg][32 * wr + 8 * q + g];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) b[q] = Bs[ks + tg][32 * wc + 8 * q + g];
+#pragma unroll
+            for (int x = 0; x < 4; ++x)
+#pragma unroll
+                for (int y = 0; y < 4; ++y) mma_f64(acc[x][y][0], acc[x][y][1], a[x], b[y]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int y = 0; y < 4; ++y)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int k = k0 + 32 * wc + 8 * y + 2 * tg + i;
+            if (k >= kept) continue;
+            OutT *dst = out_cols ? out_cols[k] : out + (long)k * ldo;
+#pragma unroll
+            for (int x = 0; x < 4; ++x) {
+                const long row = i0 + 32 * wr + 8 * x + g;
+                if (row < n_valid) dst[row] = (OutT)acc[x][y][i];
+            }
+        }
+}
+
+// ---------------------------------------------------------------------------
 template <class T>
 __global__ void k_store(const typename Store<T>::C *src, long n_pad, T *dst) {
     const long stride = (long)gridDim.x * blockDim.x;
@@ -586,6 +706,17 @@ template <class T, class OutT>
 void ritz_dispatch(T *const *in_cols, int jml, long n_pad, const double *Y, int ldy, int kept, OutT *const *out_cols,
                    OutT *out, long ldo, long n_valid, cudaStream_t st) {
     if (kept <= 0) return;
+    if constexpr (std::is_same<typename Store<T>::C, double>::value) {
+        if (kept <= 32) {
+            k_ritz_mma<T, OutT, 32><<<dim3((unsigned)(n_pad / MmaShape<32>::BM), 1), kThreads, 0, st>>>(
+                in_cols, jml, Y, ldy, kept, out_cols, out, ldo, n_valid);
+        } else {
+            dim3 grid((unsigned)(n_pad / MmaShape<64>::BM), (unsigned)((kept + 63) / 64));
+            k_ritz_mma<T, OutT, 64><<<grid, kThreads, 0, st>>>(in_cols, jml, Y, ldy, kept, out_cols, out, ldo,
+                                                                n_valid);
+        }
+        return;
+    }
     const unsigned gx = (unsigned)(n_pad / kBM);
     if (kept <= 32) {
         k_ritz<T, OutT, 32><<<dim3(gx, 1), kThreads, 0, st>>>(in_cols, jml, Y, ldy, kept, out_cols, out, ldo, n_valid);

@@ -398,3 +398,22 @@ def test_lohi_zero_whichever_converge_first_matches_reference():
     ov = np.sort(o["eval"][: o["info"].nec])
     np.testing.assert_allclose(np.sort(got)[: len(ov)], ov[: len(got)], rtol=1e-10)
     assert abs(r.info.matvec - o["info"].matvec) <= 0.05 * o["info"].matvec + 4
+
+
+@pytest.mark.parametrize("bits", [64, 32])
+def test_wide_restart_tiles_match_scipy(bits):
+    """ned = 40: restarts keep more than 32 vectors and the final Ritz vectors
+    are 40+ columns, so the recombination V·Y runs on its 64-column tiles (the
+    other tests keep <= 32).  Eigenvalues equal scipy's to 1e-10 relative and
+    every pair has residual <= tol * ||A|| (FP32 basis: after refinement)."""
+    import scipy.sparse.linalg as sla
+    A = ops.anderson_3d(24, seed=17)
+    x0 = ops.start_vector(A.n)
+    want = np.sort(sla.eigsh(A.to_scipy().tocsc(), k=40, which="SA", tol=1e-12)[0])
+    with DeviceOperator(A, fmt="sell") as op:
+        r = solve(op, ned=40, maxlan=100, tol=1e-8, restart=1, maxmv=100000, start=x0, basis_bits=bits)
+    assert r.nec >= 40
+    got = np.sort(r.eval[:40])
+    np.testing.assert_allclose(got, want, rtol=1e-10, atol=1e-10 * np.max(np.abs(want)))
+    res = _residuals(A, r.eval[: r.nec], r.evec[: r.nec])
+    assert np.all(res <= 1.01 * 1e-8 * r.info.anrm), res
