@@ -121,6 +121,72 @@ void trlx_ztrlan(ztrl_matvec op, trl_info *info, int nrow, int mev,
                  const trlx_options *opts);
 
 /* ---------------------------------------------------------------------------
+ * Several GPUs, block rows (the reference's parallel model, SRC/trl_comm_mpi.c):
+ * every rank owns nloc contiguous rows of every vector (rank r's rows follow
+ * rank r-1's) and calls trlan/trlx_trlan with its own nloc and evec rows.
+ * The dot products, norms and Gram-Schmidt projections are summed over the
+ * ranks of the communicator that trlx_init_info_comm stores in
+ * info->mpicomp (the reference keeps its MPI communicator there); the small
+ * projected problem is solved on every rank from identical sums, so every
+ * rank takes the same decisions.  The operator sees this rank's rows: a
+ * user `op` exchanges what it needs itself (as in the reference); the
+ * distributed built-in operators below do it for CSR input.
+ * ------------------------------------------------------------------------- */
+typedef struct trlx_comm trlx_comm;
+
+#define TRLX_SUM 0
+#define TRLX_MAX 1
+#define TRLX_MIN 2
+
+/* Host-callback communicator: fn must replace buf[0:count] (host memory) by
+   its elementwise sum / max / min (TRLX_SUM/MAX/MIN) over all ranks, with
+   the same result on every rank, and return 0 (MPI_Allreduce, a gloo
+   process group, ...).  Device values are staged through pinned host memory
+   around each call; halo exchanges travel as one sum over a board of all
+   ranks' messages. */
+typedef int (*trlx_allreduce_fn)(double *buf, long long count, int op, void *ctx);
+int trlx_comm_create_host(int nranks, int rank, trlx_allreduce_fn fn, void *ctx,
+                          trlx_comm **out);
+
+/* NCCL communicator (libnccl.so.2, or $TRLX_NCCL_LIB, loaded at run time;
+   -1011 when it cannot be loaded): rank 0 calls trlx_comm_nccl_id, the 128
+   bytes reach every rank by any channel, and every rank calls
+   trlx_comm_create_nccl with its device current.  Sums are queued on the
+   solver's stream; halo exchanges are grouped point-to-point messages. */
+int trlx_comm_nccl_id(unsigned char id[128]);
+int trlx_comm_create_nccl(int nranks, int rank, const unsigned char id[128],
+                          trlx_comm **out);
+
+int trlx_comm_rank(const trlx_comm *comm);
+int trlx_comm_size(const trlx_comm *comm);
+/* Sum / max / min of host doubles over the ranks. */
+int trlx_comm_allreduce(trlx_comm *comm, double *buf, long long count, int op);
+/* Destroy after every solve and operator using the communicator. */
+void trlx_comm_destroy(trlx_comm *comm);
+
+/* trl_init_info for this rank's nloc rows, then ntot = sum of nloc over the
+   ranks, my_pe / npes from the communicator and info->mpicomp = comm
+   (reference trl_init_info, SRC/trl_comm_mpi.c).  maxmv <= 0 takes the
+   reference default from the global ntot.  Returns 0 or an error code. */
+int trlx_init_info_comm(trl_info *info, trlx_comm *comm, int nloc, int mxlan,
+                        int lohi, int ned, double tol, int restart, int maxmv);
+
+/* This rank's block of a distributed matrix: nloc rows (row_ptr has nloc+1
+   entries, starting at 0) whose column indices are GLOBAL.  Rank r's rows
+   start after the rows of ranks 0..r-1 (sizes gathered over comm).  Columns
+   owned by other ranks become a halo received before every product; the
+   local part is stored as CSR or SELL-C-sigma.  Collective: every rank
+   calls it. */
+int trlx_dist_csr_create(trlx_comm *comm, int nloc, const long long *row_ptr,
+                         const int *col_idx, const double *val, int where,
+                         trlx_operator **out);
+int trlx_dist_sell_create(trlx_comm *comm, int nloc, const long long *row_ptr,
+                          const int *col_idx, const double *val, int sigma,
+                          int where, trlx_operator **out);
+/* Halo entries this rank receives per product (0 for other operators). */
+long long trlx_operator_halo(const trlx_operator *op);
+
+/* ---------------------------------------------------------------------------
  * Batched solver: many independent real symmetric problems of uneven size,
  * smallest (lohi < 0) eigenpairs of each, solved by ONE persistent kernel
  * launch.  Each problem is solved by a group of 256, 512 or 1024 threads of

@@ -34,6 +34,10 @@ class TrlxStats(C.Structure):
                 for i, name in enumerate(self.KERNEL_CLASSES) if self.kernel_count[i]}
 
 
+# int (*)(double *buf, long long count, int op, void *ctx)
+ALLREDUCE_FN = C.CFUNCTYPE(c_int, C.POINTER(C.c_double), C.c_longlong, c_int, c_void_p)
+
+
 class TrlxOptions(C.Structure):
     _fields_ = [("basis_bits", c_int), ("seed", C.c_ulonglong),
                 ("stream", c_void_p), ("refine", c_int), ("profile", c_int)]
@@ -71,6 +75,30 @@ def _declare(lib):
     lib.trlx_operator_nnz.restype = C.c_longlong
     lib.trlx_operator_nrow.argtypes = [c_void_p]
     lib.trlx_operator_nrow.restype = c_int
+    # Block-row communicators and distributed operators.
+    lib.trlx_comm_create_host.argtypes = [c_int, c_int, ALLREDUCE_FN, c_void_p, P(c_void_p)]
+    lib.trlx_comm_create_host.restype = c_int
+    lib.trlx_comm_nccl_id.argtypes = [c_void_p]
+    lib.trlx_comm_nccl_id.restype = c_int
+    lib.trlx_comm_create_nccl.argtypes = [c_int, c_int, c_void_p, P(c_void_p)]
+    lib.trlx_comm_create_nccl.restype = c_int
+    for name in ("trlx_comm_rank", "trlx_comm_size"):
+        getattr(lib, name).argtypes = [c_void_p]
+        getattr(lib, name).restype = c_int
+    lib.trlx_comm_allreduce.argtypes = [c_void_p, c_void_p, C.c_longlong, c_int]
+    lib.trlx_comm_allreduce.restype = c_int
+    lib.trlx_comm_destroy.argtypes = [c_void_p]
+    lib.trlx_comm_destroy.restype = None
+    lib.trlx_init_info_comm.argtypes = [P(TrlInfo), c_void_p, c_int, c_int, c_int, c_int, C.c_double, c_int,
+                                        c_int]
+    lib.trlx_init_info_comm.restype = c_int
+    lib.trlx_dist_csr_create.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int, P(c_void_p)]
+    lib.trlx_dist_csr_create.restype = c_int
+    lib.trlx_dist_sell_create.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int, c_int,
+                                          P(c_void_p)]
+    lib.trlx_dist_sell_create.restype = c_int
+    lib.trlx_operator_halo.argtypes = [c_void_p]
+    lib.trlx_operator_halo.restype = C.c_longlong
     lib.trlx_host_get_eval.argtypes = [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]
     lib.trlx_host_get_eval.restype = c_int
     lib.trlx_host_tridiag_eig_last.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p]

@@ -30,6 +30,7 @@
 #include "../kernels/lanczos_kernels.h"
 #include "../kernels/spmv.h"
 #include "dense.h"
+#include "comm.h"
 #include "engine.h"
 #include "hostcopy.h"
 
@@ -281,6 +282,25 @@ class Engine {
     bool user_dev_ = false;
     const trlx_operator *builtin_ = nullptr;
     bool host_op_ = false;
+    // Block-row solve: sums over the ranks of the communicator stored in
+    // info->mpicomp by trlx_init_info_comm (nullptr: one GPU).
+    Comm *comm_ = nullptr;
+    int gsum(double *d, size_t n) { return comm_ ? comm_->sum_device(d, n, st_) : 0; }
+    template <class V>
+    int gsum_c(V *d, size_t n) {
+        return gsum(reinterpret_cast<double *>(d), n * (sizeof(V) / sizeof(double)));
+    }
+    // After a projection summed over the ranks, |h|^2 comes from the summed h.
+    int project_sums(int m) {
+        if (!comm_) return 0;
+        if (int e = gsum_c(d_coef_, (size_t)m)) return e;
+        if (int e = gsum(d_scal_ + kR2Pre, 1)) return e;
+        launch_sumsq(reinterpret_cast<const double *>(d_coef_), (long)m * (long)(sizeof(C) / sizeof(double)),
+                     d_scal_ + kH2, st_);
+        count_launch();
+        return 0;
+    }
+    uint64_t rank_seed(uint64_t s) const { return s + 0x9E3779B97F4A7C15ull * (uint64_t)(comm_ ? comm_->rank : 0); }
 
     // device state
     long n_pad_ = 0;
@@ -414,6 +434,11 @@ int Engine<T>::setup() {
         }
     }
     host_op_ = !builtin_ && !user_dev_;
+    if (info_->mpicomp) comm_ = static_cast<trlx_comm *>(info_->mpicomp)->impl;
+    if (builtin_ && builtin_->halo && !comm_) {
+        std::fprintf(stderr, "TRLAN-B200: distributed operator without a communicator in info.\n");
+        return -6;
+    }
 
     if (opt_.stream) {
         st_ = opt_.stream;
@@ -538,12 +563,20 @@ int Engine<T>::apply_op(const C *x, C *y, bool want_alpha) {
     double *aout = want_alpha ? d_scal_ + kAlpha : nullptr;
     if (builtin_) {
         int pid = pbeg();
-        if constexpr (kComplex)
+        if constexpr (kComplex) {
             spmv_fused_cplx(builtin_, x, y, n_pad_, aout, &scratch_, st_);
-        else
-            spmv_fused_real(builtin_, x, y, n_pad_, aout, &scratch_, st_);
+        } else {
+            const double *xin = x;
+            if (builtin_->halo) {
+                if (int e = halo_exchange(builtin_, x, st_, &xin)) return e;
+                count_launch();
+            }
+            spmv_fused_real(builtin_, xin, y, n_pad_, aout, &scratch_, st_);
+        }
         pend(pid, TRLX_K_SPMV, spmv_bytes(builtin_));
         count_launch();
+        if (aout)
+            if (int e = gsum(aout, 1)) return e;
     } else if (!host_op_) {
         // The user's operator sees device pointers; our stream is a blocking
         // stream, so work it issues on the legacy default stream is ordered.
@@ -557,6 +590,7 @@ int Engine<T>::apply_op(const C *x, C *y, bool want_alpha) {
             launch_dot<C>(x, y, n_pad_, aout, scratch_, st_);
             pend(pid, TRLX_K_DOT, 2.0 * nrow_ * cs());
             count_launch();
+            if (int e = gsum(aout, 1)) return e;
         }
     } else {
         CK(cudaMemcpyAsync(hx_, x, sizeof(User) * nrow_, cudaMemcpyDeviceToHost, st_));
@@ -568,6 +602,7 @@ int Engine<T>::apply_op(const C *x, C *y, bool want_alpha) {
             launch_dot<C>(x, y, n_pad_, aout, scratch_, st_);
             pend(pid, TRLX_K_DOT, 2.0 * nrow_ * cs());
             count_launch();
+            if (int e = gsum(aout, 1)) return e;
         }
     }
     info_->matvec++;
@@ -618,10 +653,12 @@ int Engine<T>::cgs(int m, bool pass_done, double *rnrm, bool *irnd_used) {
                 int p1 = pbeg();
                 launch_project<T>(d_cols_, m, n_pad_, r64_, none, d_coef_, d_scal_ + kR2Pre, scratch_, st_);
                 pend(p1, TRLX_K_PROJECT, (double)m * nrow_ * sv() + nrow_ * cs());
+                if (int e = project_sums(m)) return e;
                 int p2 = pbeg();
                 launch_update<T>(d_cols_, m, n_pad_, r64_, none, d_coef_, r64_, d_scal_ + kR2Post, scratch_, st_);
                 pend(p2, TRLX_K_UPDATE, (double)m * nrow_ * sv() + 2.0 * nrow_ * cs());
                 count_launch(2);
+                if (int e = gsum(d_scal_ + kR2Post, 1)) return e;
                 if (int e = sync_scalars()) return e;
             }
             first = false;
@@ -637,6 +674,7 @@ int Engine<T>::cgs(int m, bool pass_done, double *rnrm, bool *irnd_used) {
                     }
                     launch_dot<C>(r64_, r64_, n_pad_, d_scal_ + kR2Post, scratch_, st_);
                     count_launch();
+                    if (int e = gsum(d_scal_ + kR2Post, 1)) return e;
                     if (int e = sync_scalars()) return e;
                 }
             }
@@ -654,7 +692,7 @@ int Engine<T>::cgs(int m, bool pass_done, double *rnrm, bool *irnd_used) {
                 cnt = 0;
                 irnd++;
                 info_->nrand++;
-                launch_random<C>(r64_, nrow_, n_pad_, opt_.seed + 7919ull * (uint64_t)info_->nrand, st_);
+                launch_random<C>(r64_, nrow_, n_pad_, rank_seed(opt_.seed + 7919ull * (uint64_t)info_->nrand), st_);
                 count_launch();
             }
         }
@@ -691,10 +729,12 @@ int Engine<T>::orth(int m, bool recur, double beta_prev, int kept) {
     int p1 = pbeg();
     launch_project<T>(d_cols_, m, n_pad_, r64_, rec, d_coef_, d_scal_ + kR2Pre, scratch_, st_);
     pend(p1, TRLX_K_PROJECT, (double)m * nrow_ * sv() + nrow_ * cs() + recb);
+    if (int e = project_sums(m)) return e;
     int p2 = pbeg();
     launch_update<T>(d_cols_, m, n_pad_, r64_, rec, d_coef_, r64_, d_scal_ + kR2Post, scratch_, st_);
     pend(p2, TRLX_K_UPDATE, (double)m * nrow_ * sv() + 2.0 * nrow_ * cs() + recb);
     count_launch(2);
+    if (int e = gsum(d_scal_ + kR2Post, 1)) return e;
     if (int e = sync_scalars()) return e;
     alpha_[jnd - 1] = h_scal_[kAlpha];
     const double normrr2 = h_scal_[kR2Pre];
@@ -819,24 +859,26 @@ int Engine<T>::initial_guess(int *jnd_out) {
         }
         CK(host_copy(r64_, ones.data(), ue * nrow_, cudaMemcpyHostToDevice, st_));
         if (nran >= nrow_) {
-            launch_random<C>(r64_, nrow_, n_pad_, opt_.seed, st_);
+            launch_random<C>(r64_, nrow_, n_pad_, rank_seed(opt_.seed), st_);
             count_launch();
             info_->nrand++;
         }
     }
     launch_dot<C>(r64_, r64_, n_pad_, d_scal_ + kR2Post, scratch_, st_);
     count_launch();
+    if (int e = gsum(d_scal_ + kR2Post, 1)) return e;
     if (int e = sync_scalars()) return e;
     double normr2 = h_scal_[kR2Post];
     double rnrm = 0.0;
     if (normr2 >= DBL_MIN && normr2 <= DBL_MAX) {
         rnrm = std::sqrt(normr2);
     } else {
-        launch_random<C>(r64_, nrow_, n_pad_, opt_.seed ^ 0xA5A5A5A5ull, st_);
+        launch_random<C>(r64_, nrow_, n_pad_, rank_seed(opt_.seed ^ 0xA5A5A5A5ull), st_);
         count_launch();
         info_->nrand++;
         launch_dot<C>(r64_, r64_, n_pad_, d_scal_ + kR2Post, scratch_, st_);
         count_launch();
+        if (int e = gsum(d_scal_ + kR2Post, 1)) return e;
         if (int e = sync_scalars()) return e;
         rnrm = std::sqrt(h_scal_[kR2Post]);
     }
@@ -1014,7 +1056,7 @@ bool Engine<T>::spec_enabled() const {
     if constexpr (!kWide) {
         return false;
     } else {
-        if (!builtin_ || uo_ || n_pad_ > (1L << 21)) return false;
+        if (!builtin_ || uo_ || comm_ || builtin_->halo || n_pad_ > (1L << 21)) return false;
         const char *e = std::getenv("TRLX_SPECULATE");
         return !(e && e[0] == '0');
     }
@@ -1270,6 +1312,8 @@ int Engine<T>::refine_fp64(int k, double *max_res) {
             launch_project<C>(tabW, k, n_pad_, AWb + j * vec, Recur<C>{}, dH + (size_t)j * k, dout2, scratch_, st_);
         }
         count_launch(2 * k);
+        if (int e = gsum_c(dG, kk)) return e;
+        if (int e = gsum_c(dH, kk)) return e;
         CK(cudaMemcpyAsync(G.data(), dG, sizeof(C) * kk, cudaMemcpyDeviceToHost, st_));
         CK(cudaMemcpyAsync(H.data(), dH, sizeof(C) * kk, cudaMemcpyDeviceToHost, st_));
         CK(cudaStreamSynchronize(st_));
@@ -1340,6 +1384,7 @@ int Engine<T>::refine_fp64(int k, double *max_res) {
             launch_update<C>(tabAWW, 2 * k, n_pad_, zero, Recur<C>{}, dh + (size_t)cc * 2 * k, ay, dr2 + cc, scratch_,
                              st_);
         count_launch(k);
+        if (int e = gsum(dr2, (size_t)k)) return e;
         CK(cudaMemcpyAsync(r2.data(), dr2, sizeof(double) * k, cudaMemcpyDeviceToHost, st_));
         CK(cudaStreamSynchronize(st_));
         ++syncs_;

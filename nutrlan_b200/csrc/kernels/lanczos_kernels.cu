@@ -768,6 +768,18 @@ __global__ void k_cheb(const double *__restrict__ ay, const double *__restrict__
     }
 }
 
+__global__ void __launch_bounds__(kThreads) k_sumsq(const double *__restrict__ v, long n, double *out) {
+    __shared__ double red[32];
+    double s = 0.0;
+    for (long i = threadIdx.x; i < n; i += kThreads) s = fma(v[i], v[i], s);
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) *out = s;
+}
+
+void launch_sumsq(const double *v, long n, double *out, cudaStream_t st) {
+    k_sumsq<<<1, kThreads, 0, st>>>(v, n, out);
+}
+
 void launch_cheb(const double *ay, const double *y, const double *yp, long n_pad, double a, double c, double b,
                  double *out, cudaStream_t st) {
     k_cheb<<<elementwise_blocks(n_pad), kThreads, 0, st>>>(ay, y, yp, n_pad, a, c, b, out);

@@ -85,6 +85,9 @@ template <class T>
 void launch_load(const T *src, long n, typename Store<T>::C *dst,
                  cudaStream_t st);
 
+// *out = sum of v[i]^2 for i < n (short vectors: one block, fixed order).
+void launch_sumsq(const double *v, long n, double *out, cudaStream_t st);
+
 // out = a * (ay - c * y) + b * yp (yp may be null; out may alias yp): one
 // step of the scaled Chebyshev filter of the FP64 refinement.
 void launch_cheb(const double *ay, const double *y, const double *yp, long n_pad, double a, double c, double b,

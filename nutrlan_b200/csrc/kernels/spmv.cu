@@ -15,6 +15,7 @@
 
 #include "../../../include/trlx.h"
 #include "spmv.h"
+#include "../host/comm.h"
 #include "../host/hostcopy.h"
 
 namespace trlb {
@@ -248,6 +249,12 @@ void spmv_fused_cplx(const trlx_operator *A, const zd *x, zd *y, long n_pad, dou
 
 void spmv_plain(const trlx_operator *A, const void *x, void *y, cudaStream_t st) {
     // n_pad == nrow: no padding rows written.
+    if (A->halo) {
+        const double *xe = nullptr;
+        if (halo_exchange(A, static_cast<const double *>(x), st, &xe) != 0) return;
+        spmv_fused_real(A, xe, static_cast<double *>(y), A->nrow, nullptr, nullptr, st);
+        return;
+    }
     if (A->kind == 2)
         spmv_fused_cplx(A, static_cast<const zd *>(x), static_cast<zd *>(y), A->nrow, nullptr, nullptr, st);
     else
@@ -263,6 +270,43 @@ double spmv_bytes(const trlx_operator *A) {
     else
         b += 8.0 * (A->nrow + 1.0);
     return b;
+}
+
+// ---- block-row distribution -------------------------------------------------
+struct Halo {
+    Comm *comm = nullptr;  // borrowed from the trlx_comm given at creation
+    long long row0 = 0;    // global index of this rank's first row
+    int nhalo = 0;
+    long long nsend = 0;
+    int *send_idx = nullptr;     // local rows other ranks need, grouped by receiver
+    double *send_buf = nullptr;  // nsend values
+    double *x_ext = nullptr;     // this rank's rows, then the halo
+    long ext_len = 0;
+    std::vector<long> soff, roff, counts;  // per peer offsets; size x size lengths
+};
+
+namespace {
+
+__global__ void k_gather(const double *__restrict__ x, const int *__restrict__ idx, long long n,
+                         double *__restrict__ out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = x[idx[i]];
+}
+
+}  // namespace
+
+int halo_exchange(const trlx_operator *A, const double *x, cudaStream_t st, const double **x_ext) {
+    Halo *h = A->halo;
+    if (h->nsend > 0) {
+        const int nb = (int)std::min<long long>((h->nsend + 255) / 256, 148LL * 8);
+        k_gather<<<nb, 256, 0, st>>>(x, h->send_idx, h->nsend, h->send_buf);
+    }
+    if (cudaMemcpyAsync(h->x_ext, x, sizeof(double) * (size_t)A->nrow, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return -1001;
+    if (int e = h->comm->exchange(h->send_buf, h->soff, h->x_ext + A->nrow, h->roff, h->counts, st)) return e;
+    *x_ext = h->x_ext;
+    return 0;
 }
 
 // ---- SELL-C-32 construction ------------------------------------------------
@@ -587,6 +631,12 @@ extern "C" void trlx_operator_destroy(trlx_operator *A) {
     op_free(A->val);
     op_free(A->slice_ptr);
     op_free(A->perm);
+    if (A->halo) {
+        op_free(A->halo->send_idx);
+        op_free(A->halo->send_buf);
+        op_free(A->halo->x_ext);
+        delete A->halo;
+    }
     cudaStreamSynchronize(0);
     if (A->device >= 0 && A->device != prev) cudaSetDevice(prev);
     delete A;
@@ -604,6 +654,127 @@ void trim_operator_pools() {
 
 extern "C" long long trlx_operator_nnz(const trlx_operator *A) { return A ? A->nnz : 0; }
 extern "C" int trlx_operator_nrow(const trlx_operator *A) { return A ? A->nrow : 0; }
+
+extern "C" long long trlx_operator_halo(const trlx_operator *A) { return A && A->halo ? A->halo->nhalo : 0; }
+
+namespace {
+
+// Block-row operator of this rank (reference model: SRC/trl_comm_mpi.c
+// distributes rows the same way; its user operator does the exchange).
+// Every rank takes part in every collective below, also on bad input, so
+// that no rank is left waiting.
+int dist_create(trlx_comm *comm, int nloc, const long long *row_ptr, const int *col_idx, const double *val,
+                int sigma, bool sell, int where, trlx_operator **out) {
+    if (!out || !comm || !comm->impl || nloc <= 0 || !row_ptr || !col_idx || !val) return -1;
+    trlb::Comm *cm = comm->impl;
+    const int P = cm->size, me = cm->rank;
+    // Row ranges of all ranks.
+    std::vector<double> cnt(P, 0.0);
+    cnt[me] = nloc;
+    if (int e = cm->reduce_host(cnt.data(), P, trlb::kOpSum)) return e;
+    std::vector<long long> start(P + 1, 0);
+    for (int p = 0; p < P; ++p) start[p + 1] = start[p] + (long long)cnt[p];
+    const long long row0 = start[me], ntot = start[P];
+    std::vector<long long> rp = to_host(row_ptr, (size_t)nloc + 1, where);
+    int bad = rp[0] != 0 || rp[nloc] < 0;
+    const long long nnz = bad ? 0 : rp[nloc];
+    std::vector<int> ci = to_host(col_idx, (size_t)nnz, where);
+    std::vector<double> va = to_host(val, (size_t)nnz, where);
+    // Columns owned by other ranks, ascending (hence grouped by owner).
+    std::vector<int> ext;
+    for (long long k = 0; k < nnz; ++k) {
+        const long long c = ci[k];
+        if (c < 0 || c >= ntot)
+            bad = 1;
+        else if (c < row0 || c >= row0 + nloc)
+            ext.push_back((int)c);
+    }
+    double flag = bad;
+    if (int e = cm->reduce_host(&flag, 1, trlb::kOpMax)) return e;
+    if (flag != 0.0) return -1;
+    std::sort(ext.begin(), ext.end());
+    ext.erase(std::unique(ext.begin(), ext.end()), ext.end());
+    const int nhalo = (int)ext.size();
+    std::vector<long> roff(P + 1, 0);
+    for (int c : ext) {
+        const int p = (int)(std::upper_bound(start.begin(), start.end(), (long long)c) - start.begin()) - 1;
+        roff[p + 1]++;
+    }
+    for (int p = 0; p < P; ++p) roff[p + 1] += roff[p];
+    // counts[p * P + q]: values p sends to q.
+    std::vector<double> cm_counts((size_t)P * P, 0.0);
+    for (int p = 0; p < P; ++p) cm_counts[(size_t)p * P + me] = (double)(roff[p + 1] - roff[p]);
+    if (int e = cm->reduce_host(cm_counts.data(), cm_counts.size(), trlb::kOpSum)) return e;
+    std::vector<long> counts(cm_counts.size());
+    for (size_t k = 0; k < counts.size(); ++k) counts[k] = (long)cm_counts[k];
+    // The requested global indices, on a board with one segment per
+    // (owner, requester) pair.
+    std::vector<long> bo(counts.size() + 1, 0);
+    for (size_t k = 0; k < counts.size(); ++k) bo[k + 1] = bo[k] + counts[k];
+    std::vector<double> board((size_t)bo.back(), 0.0);
+    for (int p = 0; p < P; ++p)
+        for (long k = roff[p]; k < roff[p + 1]; ++k) board[(size_t)bo[(size_t)p * P + me] + (k - roff[p])] = ext[k];
+    if (int e = cm->reduce_host(board.data(), board.size(), trlb::kOpSum)) return e;
+    std::vector<long> soff(P + 1, 0);
+    std::vector<int> sidx;
+    for (int q = 0; q < P; ++q) {
+        const long c = counts[(size_t)me * P + q];
+        for (long k = 0; k < c; ++k)
+            sidx.push_back((int)((long long)board[(size_t)bo[(size_t)me * P + q] + k] - row0));
+        soff[q + 1] = soff[q] + c;
+    }
+    // Local numbering: own rows first, then the halo in receive order.
+    for (long long k = 0; k < nnz; ++k) {
+        const long long c = ci[k];
+        if (c >= row0 && c < row0 + nloc)
+            ci[k] = (int)(c - row0);
+        else
+            ci[k] = nloc + (int)(std::lower_bound(ext.begin(), ext.end(), (int)c) - ext.begin());
+    }
+    trlx_operator *A = nullptr;
+    int rc = sell ? trlx_sell_create(nloc, rp.data(), ci.data(), va.data(), sigma, TRLX_HOST_ARRAYS, &A)
+                  : trlx_csr_create(nloc, rp.data(), ci.data(), va.data(), TRLX_HOST_ARRAYS, &A);
+    if (rc) return rc;
+    auto *h = new trlb::Halo();
+    A->halo = h;
+    h->comm = cm;
+    h->row0 = row0;
+    h->nhalo = nhalo;
+    h->nsend = (long long)sidx.size();
+    h->soff = soff;
+    h->roff = roff;
+    h->counts = counts;
+    const long n_pad = ((long)nloc + 255) / 256 * 256;
+    h->ext_len = std::max<long>(n_pad, (long)nloc + nhalo);
+    if (h->nsend > 0) {
+        rc = to_device(sidx.data(), sidx.size(), TRLX_HOST_ARRAYS, &h->send_idx);
+        if (!rc && op_alloc(reinterpret_cast<void **>(&h->send_buf), sizeof(double) * sidx.size()) != cudaSuccess)
+            rc = -2;
+    }
+    if (!rc && op_alloc(reinterpret_cast<void **>(&h->x_ext), sizeof(double) * h->ext_len) != cudaSuccess) rc = -2;
+    // Entries past nloc + nhalo are only ever multiplied by zero; keep them zero.
+    if (!rc && (cudaMemsetAsync(h->x_ext, 0, sizeof(double) * h->ext_len, 0) != cudaSuccess ||
+                cudaStreamSynchronize(0) != cudaSuccess))
+        rc = -3;
+    if (rc) {
+        trlx_operator_destroy(A);
+        return rc;
+    }
+    *out = A;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int trlx_dist_csr_create(trlx_comm *comm, int nloc, const long long *row_ptr, const int *col_idx,
+                                    const double *val, int where, trlx_operator **out) {
+    return dist_create(comm, nloc, row_ptr, col_idx, val, 1, false, where, out);
+}
+
+extern "C" int trlx_dist_sell_create(trlx_comm *comm, int nloc, const long long *row_ptr, const int *col_idx,
+                                     const double *val, int sigma, int where, trlx_operator **out) {
+    return dist_create(comm, nloc, row_ptr, col_idx, val, sigma, true, where, out);
+}
 
 extern "C" void trlx_matvec(const int nrow, const int ncol, const double *x, const int ldx, double *y,
                             const int ldy, void *mvparam) {

@@ -9,6 +9,10 @@
 
 #include "lanczos_kernels.h"
 
+namespace trlb {
+struct Halo;
+}
+
 struct trlx_operator {
     int kind = 0;  // 0 real CSR, 1 real SELL-C-32, 2 complex CSR
     int nrow = 0;
@@ -23,6 +27,10 @@ struct trlx_operator {
     long long *slice_ptr = nullptr;  // offset of slice s (entries), nslice+1
     int *perm = nullptr;             // stored row -> original row (nullptr = identity)
     int device = -1;
+    // Block-row distribution (trlx_dist_*_create): columns [0, nrow) are
+    // this rank's rows, [nrow, nrow + halo entries) values received from
+    // other ranks before every product.
+    trlb::Halo *halo = nullptr;
 };
 
 namespace trlb {
@@ -42,5 +50,11 @@ double spmv_bytes(const trlx_operator *A);
 
 // Returns the unused memory of the operators' device pools.
 void trim_operator_pools();
+
+// Distributed operators: gathers the values other ranks need from x (this
+// rank's n_pad-row vector), exchanges halos over the operator's
+// communicator and returns in *x_ext the vector to multiply (x's rows, then
+// the halo), all ordered on st.  0 or an error code.
+int halo_exchange(const trlx_operator *A, const double *x, cudaStream_t st, const double **x_ext);
 
 }  // namespace trlb
