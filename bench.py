@@ -487,6 +487,107 @@ def run_wells(args, w, world, rank, local, pg):
             "learned_seed": ab, "cpu_baseline": cpu, "clocks": clocks, "host_wall_s": wall}), flush=True)
 
 
+def run_dist(args, w, world, rank, local, pg):
+    """One Anderson/Laplace solve split into block rows over the ranks (the
+    reference's parallel model): NCCL sums and halo exchanges between the
+    GPUs.  Strong scaling: the global problem is the named workload; value =
+    Lanczos steps of the one global solve per second (max over ranks)."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from nutrlan_b200 import operators as ops
+    from nutrlan_b200.dist import Comm, DistOperator, row_blocks, local_rows, solve as dsolve
+    A = build_operator(w, 2024)
+    n = A.n
+    ned, maxlan, tol = w["ned"], w["maxlan"], w["tol"]
+    mev = ned + 1
+    row0, nloc = row_blocks(n, world)[rank]
+    rp, ci, va = local_rows(A, row0, nloc)
+    x0 = ops.start_vector(n)[row0:row0 + nloc]
+    comm = Comm.from_process_group() if pg is not None else Comm.nccl(1, 0, Comm.nccl_unique_id())
+    op = DistOperator(comm, rp, ci, va, fmt=args.format)
+    evec = torch.zeros((mev, nloc), dtype=torch.float64, device=dev)
+
+    def one_call(profile=True):
+        r = dsolve(comm, op, ned, maxlan, tol=tol, maxmv=maxlan, start=x0, evec=evec,
+                   basis_bits=args.basis_bits, profile=profile)
+        if r.stat != 0:
+            raise RuntimeError(f"trlan stat {r.stat}")
+        return r
+
+    for _ in range(args.warmup):
+        one_call()
+    torch.cuda.synchronize()
+    barrier(pg)
+    sampler = ClockSampler(local)
+    sampler.start()
+    kt, kb, kc = np.zeros(8), np.zeros(8), np.zeros(8)
+    launches = mv = 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        r = one_call()
+        st = r.stats
+        kt += np.array(st.kernel_seconds[:])
+        kb += np.array(st.kernel_bytes[:])
+        kc += np.array(st.kernel_count[:])
+        launches += st.kernel_launches
+        mv += r.info.matvec
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    elapsed = reduce_max(pg, e0.elapsed_time(e1) * 1e-3, dev)
+    value = mv / elapsed
+    names = ["spmv", "project", "update", "normalize", "ritz", "dot", "other", "x"]
+    dom = int(np.argmax(kt))
+    peak, peak_kind = read_peaks()
+    achieved = kb[dom] / kt[dom] / 1e9 if kt[dom] > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                "alg_bytes_per_launch": kb[dom] / max(kc[dom], 1), "launches": int(kc[dom]),
+                "note": "rank 0's kernels on its own rows"}
+    e2e = None
+    if not args.no_e2e:
+        hev = np.zeros((mev, nloc))
+
+        def e2e_call():
+            with DistOperator(comm, rp, ci, va, fmt=args.format) as hop:
+                r = dsolve(comm, hop, ned, maxlan, tol=tol, maxmv=maxlan, start=x0, basis_bits=args.basis_bits,
+                           evec=hev)
+                return r.info.matvec
+
+        e2e_call()
+        barrier(pg)
+        t0 = time.perf_counter()
+        emv = sum(e2e_call() for _ in range(args.steps))
+        e_wall = reduce_max(pg, time.perf_counter() - t0, dev)
+        e2e = {"value": emv / e_wall, "unit": "steps/s",
+               "h2d_bytes_per_step": int(rp.nbytes + ci.nbytes + va.nbytes + 8 * nloc),
+               "d2h_bytes_per_step": int(8 * nloc * mev + 8 * mev)}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cmv, cdt = run_reference_sample(A, w, ops.start_vector(n), args.cpu_sample)
+        cpu = {"value": cmv / cdt, "unit": "steps/s", "cores": os.cpu_count(), "kind": "reference",
+               "sample": f"reference trlan, first {args.cpu_sample} Lanczos steps of the same solve"}
+    op.close()
+    comm.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"Lanczos steps/s (SpMV + full CGS reorth), {args.workload}, smallest {ned}",
+            "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64" if args.basis_bits == 64 else "f32 basis / f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"{args.workload}: n={n}, ned={ned}, maxlan={maxlan}, tol={tol}, "
+                                   f"{args.format.upper()} block rows, basis fp{args.basis_bits}, "
+                                   "one thick-restart cycle/step",
+                       "parallelism": f"block rows x{world} (NCCL sums + halo exchange)",
+                       "l2": "inputs larger than L2"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clocks}), flush=True)
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -535,6 +636,9 @@ def main():
     ap.add_argument("--solve-maxmv", type=int, default=20000)
     ap.add_argument("--no-learned-seed", action="store_true",
                     help="skip the learned-seed A/B record of the default line")
+    ap.add_argument("--dist", action="store_true",
+                    help="one solve split into block rows over the ranks (NCCL), strong scaling; "
+                         "default for --gpus N: independent replicas")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world, rank, local, pg = dist_setup(args)
@@ -545,6 +649,11 @@ def main():
         return
     if w["kind"] == "peierls":
         run_complex(args, w, world, rank, local, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    if args.dist and args.impl == "b200" and w["kind"] in ("anderson", "laplace"):
+        run_dist(args, w, world, rank, local, pg)
         if pg is not None:
             pg.destroy_process_group()
         return

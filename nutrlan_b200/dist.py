@@ -195,8 +195,9 @@ def solve(comm, op, ned, maxlan, lohi=-1, tol=1.4901e-8, restart=1, maxmv=0, sta
           basis_bits=64, seed=0, refine=None, profile=False, evec=None):
     """trlan on this rank's rows (``op``: a DistOperator, or anything with
     ``n``, ``handle`` and ``applier`` of a built-in operator).  ``start`` is
-    this rank's rows of the start vector; ``evec`` (optional) a torch CUDA
-    tensor of mev x n for device-resident eigenvectors.  A collective: every
+    this rank's rows of the start vector; ``evec`` (optional) a C-contiguous
+    mev x n float64 torch CUDA tensor (device-resident eigenvectors) or numpy
+    array.  A collective: every
     rank calls it with the same parameters."""
     lib = load()
     n = op.n
@@ -207,7 +208,7 @@ def solve(comm, op, ned, maxlan, lohi=-1, tol=1.4901e-8, restart=1, maxmv=0, sta
         raise RuntimeError(f"trlx_init_info_comm failed ({rc})")
     info.mvparam = op.handle.value
     eval_ = np.zeros(mev)
-    if evec is not None:
+    if evec is not None and hasattr(evec, "data_ptr"):
         import torch
         ev = evec
         if start is not None:
@@ -215,7 +216,7 @@ def solve(comm, op, ned, maxlan, lohi=-1, tol=1.4901e-8, restart=1, maxmv=0, sta
         torch.cuda.synchronize()
         ptr = ev.data_ptr()
     else:
-        ev = np.zeros((mev, n))
+        ev = evec if evec is not None else np.zeros((mev, n))
         if start is not None:
             ev[0] = start
         ptr = ev.ctypes.data
