@@ -454,8 +454,9 @@ __global__ void __launch_bounds__(kThreads)
 // thread), so 8 fragment loads from shared memory feed 16 mma (4096 FMAs).
 // K advances 16 columns per shared-memory stage (4 mma k-steps) with the
 // next stage prefetched into registers.  Shared tiles are k-major with a row
-// pitch of (rows + 8) doubles: a warp's fragment loads (8 rows x 4 k) then
-// touch every bank exactly twice, the minimum for 256 bytes.
+// pitch of (rows + 4) doubles.  A warp's 64-bit fragment loads are served per
+// half-warp (4 rows x 4 k); with a pitch of 4 mod 16 doubles the four k rows
+// start 8 banks apart, so each half-warp is one conflict-free wavefront.
 // Fragment layout of m8n8k4 .f64 (g = lane / 4, t = lane % 4):
 // A (row-major 8x4): a = A[g][t]; B (col-major 4x8): b = B[t][g];
 // C/D (8x8): c0, c1 = C[g][2t], C[g][2t+1].
@@ -478,7 +479,8 @@ __global__ void __launch_bounds__(kThreads)
                OutT *const *out_cols, OutT *out, long ldo, long n_valid) {
     using S = Store<T>;
     using Sh = MmaShape<BN>;
-    constexpr int BM = Sh::BM, APITCH = BM + 8, BPITCH = BN + 8;
+    constexpr int BM = Sh::BM, APITCH = BM + 4, BPITCH = BN + 4;
+    static_assert(APITCH % 16 == 4 && BPITCH % 16 == 4 && (APITCH * 8) % 16 == 0, "bank-spread pitches");
     constexpr int R = S::R;              // elements per 16-byte load
     constexpr int CH = BM / R / 16;      // 16-byte chunks per thread per stage
     constexpr int BPT = BN * kBK / kThreads;
