@@ -125,21 +125,50 @@ __device__ inline double apply_op(const Params &P, const Problem &pr, const doub
 }
 
 // h[c] = V[:,c].r (c < m) with r = y - alpha x - beta xp when rec; S.scal[kR2Pre] = |r|^2,
-// S.scal[kH2] = |h|^2.
+// S.scal[kH2] = |h|^2.  Rows are taken in pairs with 16-byte loads (basis
+// columns are 256-byte aligned, ld a multiple of 32); an odd last row is
+// handled by thread 0.  Padding rows (n .. ld) are never read.
+__device__ inline double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
+
 __device__ inline void project(const double *V, int ld, int n, int m, const double *y, bool rec, const double *x,
                                const double *xp, double alpha, double beta, const Grp &G) {
     Shared &S = *G.S;
     double r2 = 0.0;
+    const int np = n >> 1;
+    const bool tail = (n & 1) && G.tid == 0;
     for (int c0 = 0; c0 < m; c0 += 8) {
         double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         const int mm = min(8, m - c0);
-        for (int i = G.tid; i < n; i += G.nt) {
+        const double *Vc = V + (size_t)c0 * ld;
+        for (int p = G.tid; p < np; p += G.nt) {
+            const int i = 2 * p;
+            const double2 yv = ld2(y + i);
+            double r0 = yv.x, r1 = yv.y;
+            if (rec) {
+                const double2 xv = ld2(x + i), pv = ld2(xp + i);
+                r0 -= alpha * xv.x + beta * pv.x;
+                r1 -= alpha * xv.y + beta * pv.y;
+            }
+            if (c0 == 0) {
+                r2 += r0 * r0;
+                r2 += r1 * r1;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (k < mm) {
+                    const double2 v = ld2(Vc + (size_t)k * ld + i);
+                    acc[k] = fma(v.x, r0, acc[k]);
+                    acc[k] = fma(v.y, r1, acc[k]);
+                }
+        }
+        if (tail) {
+            const int i = n - 1;
             double ri = y[i];
             if (rec) ri -= alpha * x[i] + beta * xp[i];
             if (c0 == 0) r2 += ri * ri;
 #pragma unroll
             for (int k = 0; k < 8; ++k)
-                if (k < mm) acc[k] = fma(V[(size_t)(c0 + k) * ld + i], ri, acc[k]);
+                if (k < mm) acc[k] = fma(Vc[(size_t)k * ld + i], ri, acc[k]);
         }
         block_reduce<8>(acc, &S.h[c0], G);
     }
@@ -160,11 +189,45 @@ __device__ inline void project(const double *V, int ld, int n, int m, const doub
 }
 
 // r = (y - alpha x - beta xp) - V h (in place in y); S.scal[kR2] = |r|^2.
+// Row pairs as in project; the column loop issues eight 16-byte loads before
+// their FMAs (each element's FMA chain keeps the column order).
 __device__ inline void update(const double *V, int ld, int n, int m, double *y, bool rec, const double *x,
                               const double *xp, double alpha, double beta, const double *h, const Grp &G) {
+    constexpr int UC = 8;
     Shared &S = *G.S;
     double r2 = 0.0;
-    for (int i = G.tid; i < n; i += G.nt) {
+    const int np = n >> 1;
+    for (int p = G.tid; p < np; p += G.nt) {
+        const int i = 2 * p;
+        const double2 yv = ld2(y + i);
+        double r0 = yv.x, r1 = yv.y;
+        if (rec) {
+            const double2 xv = ld2(x + i), pv = ld2(xp + i);
+            r0 -= alpha * xv.x + beta * pv.x;
+            r1 -= alpha * xv.y + beta * pv.y;
+        }
+        int c = 0;
+        for (; c + UC <= m; c += UC) {
+            double2 v[UC];
+#pragma unroll
+            for (int k = 0; k < UC; ++k) v[k] = ld2(V + (size_t)(c + k) * ld + i);
+#pragma unroll
+            for (int k = 0; k < UC; ++k) {
+                r0 = fma(-v[k].x, h[c + k], r0);
+                r1 = fma(-v[k].y, h[c + k], r1);
+            }
+        }
+        for (; c < m; ++c) {
+            const double2 v = ld2(V + (size_t)c * ld + i);
+            r0 = fma(-v.x, h[c], r0);
+            r1 = fma(-v.y, h[c], r1);
+        }
+        *reinterpret_cast<double2 *>(y + i) = make_double2(r0, r1);
+        r2 += r0 * r0;
+        r2 += r1 * r1;
+    }
+    if ((n & 1) && G.tid == 0) {
+        const int i = n - 1;
         double ri = y[i];
         if (rec) ri -= alpha * x[i] + beta * xp[i];
         for (int c = 0; c < m; ++c) ri = fma(-V[(size_t)c * ld + i], h[c], ri);
