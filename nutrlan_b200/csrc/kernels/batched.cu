@@ -380,18 +380,45 @@ __device__ inline void ritz_in_place(double *V, int ld, int n, int lck, int jml,
     int kTile = (int)min((long)n, tile_cap / max(jml, 1));
     if (kTile >= 32) kTile = kTile / 32 * 32;
     kTile = max(kTile, 1);
+    // Tile fill: row pairs with 16-byte loads when the tile height is even
+    // (r0, rr even: aligned in the basis column and in the tile).  Products:
+    // each thread forms two output columns from one read of the tile value;
+    // every output sums over c in ascending order.
+    const bool pairs = (kTile & 1) == 0;
+    const int kp = kept / 2;
     for (int r0 = 0; r0 < n; r0 += kTile) {
         const int rows = min(kTile, n - r0);
-        for (int e = G.tid; e < rows * jml; e += G.nt) {
-            const int rr = e % rows, c = e / rows;
+        const int rp = pairs ? rows / 2 : 0;
+        for (int e = G.tid; e < rp * jml; e += G.nt) {
+            const int pr = e % rp, c = e / rp;
+            const double2 v = ld2(V + (size_t)(lck + c) * ld + r0 + 2 * pr);
+            *reinterpret_cast<double2 *>(tile + c * kTile + 2 * pr) = v;
+        }
+        const int rest = rows - 2 * rp;  // rows not covered by pairs
+        for (int e = G.tid; e < rest * jml; e += G.nt) {
+            const int rr = 2 * rp + e % rest, c = e / rest;
             tile[c * kTile + rr] = V[(size_t)(lck + c) * ld + r0 + rr];
         }
         G.sync();
-        for (int e = G.tid; e < rows * kept; e += G.nt) {
-            const int rr = e % rows, k = e / rows;
-            double s = 0.0;
-            for (int c = 0; c < jml; ++c) s = fma(tile[c * kTile + rr], yy[(size_t)k * jml + c], s);
-            V[(size_t)(lck + k) * ld + r0 + rr] = s;
+        for (int e = G.tid; e < rows * kp; e += G.nt) {
+            const int rr = e % rows, k = 2 * (e / rows);
+            const double *y0 = yy + (size_t)k * jml, *y1 = y0 + jml;
+            double s0 = 0.0, s1 = 0.0;
+            for (int c = 0; c < jml; ++c) {
+                const double t = tile[c * kTile + rr];
+                s0 = fma(t, y0[c], s0);
+                s1 = fma(t, y1[c], s1);
+            }
+            V[(size_t)(lck + k) * ld + r0 + rr] = s0;
+            V[(size_t)(lck + k + 1) * ld + r0 + rr] = s1;
+        }
+        if (kept & 1) {
+            const int k = kept - 1;
+            for (int rr = G.tid; rr < rows; rr += G.nt) {
+                double s = 0.0;
+                for (int c = 0; c < jml; ++c) s = fma(tile[c * kTile + rr], yy[(size_t)k * jml + c], s);
+                V[(size_t)(lck + k) * ld + r0 + rr] = s;
+            }
         }
         G.sync();
     }
