@@ -124,13 +124,15 @@ __device__ inline double apply_op(const Params &P, const Problem &pr, const doub
     return block_sum1(a, G);
 }
 
-// h[c] = V[:,c].r (c < m) with r = y - alpha x - beta xp when rec; S.scal[kR2Pre] = |r|^2,
+// h[c] = V[:,c].r (c < m) with r = y - alpha x - beta xp when rec, and r
+// written back into y by the first column pass (the later passes and the
+// update then read one vector instead of three); S.scal[kR2Pre] = |r|^2,
 // S.scal[kH2] = |h|^2.  Rows are taken in pairs with 16-byte loads (basis
 // columns are 256-byte aligned, ld a multiple of 32); an odd last row is
 // handled by thread 0.  Padding rows (n .. ld) are never read.
 __device__ inline double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
 
-__device__ inline void project(const double *V, int ld, int n, int m, const double *y, bool rec, const double *x,
+__device__ inline void project(const double *V, int ld, int n, int m, double *y, bool rec, const double *x,
                                const double *xp, double alpha, double beta, const Grp &G) {
     Shared &S = *G.S;
     double r2 = 0.0;
@@ -144,10 +146,11 @@ __device__ inline void project(const double *V, int ld, int n, int m, const doub
             const int i = 2 * p;
             const double2 yv = ld2(y + i);
             double r0 = yv.x, r1 = yv.y;
-            if (rec) {
+            if (rec && c0 == 0) {
                 const double2 xv = ld2(x + i), pv = ld2(xp + i);
                 r0 -= alpha * xv.x + beta * pv.x;
                 r1 -= alpha * xv.y + beta * pv.y;
+                *reinterpret_cast<double2 *>(y + i) = make_double2(r0, r1);
             }
             if (c0 == 0) {
                 r2 += r0 * r0;
@@ -164,7 +167,10 @@ __device__ inline void project(const double *V, int ld, int n, int m, const doub
         if (tail) {
             const int i = n - 1;
             double ri = y[i];
-            if (rec) ri -= alpha * x[i] + beta * xp[i];
+            if (rec && c0 == 0) {
+                ri -= alpha * x[i] + beta * xp[i];
+                y[i] = ri;
+            }
             if (c0 == 0) r2 += ri * ri;
 #pragma unroll
             for (int k = 0; k < 8; ++k)
@@ -341,7 +347,7 @@ __device__ inline int orth(const Params &P, int pid, double *V, int ld, int n, i
     }
     double beta_new;
     if (usecgs) {
-        update(V, ld, n, m, r, recur, x, xp, a, beta_prev, S.h, G);
+        update(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, S.h, G);
         double rnrm = sqrt(normrr2);
         const int st = cgs(P, pid, V, ld, n, m, true, &rnrm, G);
         if (st) return st;
@@ -352,7 +358,7 @@ __device__ inline int orth(const Params &P, int pid, double *V, int ld, int n, i
             for (int c = 0; c < m; ++c) S.g[c] = (c >= m - min(2, m)) ? S.h[c] : 0.0;
         }
         G.sync();
-        update(V, ld, n, m, r, recur, x, xp, a, beta_prev, S.g, G);
+        update(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, S.g, G);
         if (G.tid == 0) S.alpha[jnd - 1] += S.h[m - 1];
         beta_new = sqrt(normrr2);
         G.sync();
