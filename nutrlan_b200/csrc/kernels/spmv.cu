@@ -294,7 +294,59 @@ __global__ void k_gather(const double *__restrict__ x, const int *__restrict__ i
         out[i] = x[idx[i]];
 }
 
+// Columns outside [lo, hi) (another rank's rows): counted, and with out set
+// stored at atomically taken positions (the host sorts them); columns
+// outside [0, ntot) raise *bad.
+__global__ void k_halo_scan(const int *__restrict__ ci, long long nnz, long long lo, long long hi, long long ntot,
+                            unsigned long long *count, int *out, unsigned long long cap, int *bad) {
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nnz;
+         k += (long long)gridDim.x * blockDim.x) {
+        const long long c = ci[k];
+        if (c < 0 || c >= ntot) {
+            *bad = 1;
+        } else if (c < lo || c >= hi) {
+            const unsigned long long pos = atomicAdd(count, 1ull);
+            if (out && pos < cap) out[pos] = (int)c;
+        }
+    }
+}
+
+// Local numbering: own rows to c - lo, halo columns to nloc + their position
+// in the sorted halo list ext (binary search).
+__global__ void k_halo_renumber(const int *__restrict__ ci, long long nnz, long long lo, long long hi, int nloc,
+                                const int *__restrict__ ext, int next, int *__restrict__ out) {
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nnz;
+         k += (long long)gridDim.x * blockDim.x) {
+        const long long c = ci[k];
+        if (c >= lo && c < hi) {
+            out[k] = (int)(c - lo);
+        } else {
+            int a = 0, b = next;
+            while (a < b) {
+                const int mid = (a + b) >> 1;
+                if (ext[mid] < c)
+                    a = mid + 1;
+                else
+                    b = mid;
+            }
+            out[k] = nloc + a;
+        }
+    }
+}
+
 }  // namespace
+
+void launch_halo_scan(const int *ci, long long nnz, long long lo, long long hi, long long ntot,
+                      unsigned long long *count, int *out, unsigned long long cap, int *bad) {
+    const int nb = (int)std::max<long long>(1, std::min<long long>((nnz + 255) / 256, 148LL * 16));
+    k_halo_scan<<<nb, 256>>>(ci, nnz, lo, hi, ntot, count, out, cap, bad);
+}
+
+void launch_halo_renumber(const int *ci, long long nnz, long long lo, long long hi, int nloc, const int *ext,
+                          int next, int *out) {
+    const int nb = (int)std::max<long long>(1, std::min<long long>((nnz + 255) / 256, 148LL * 16));
+    k_halo_renumber<<<nb, 256>>>(ci, nnz, lo, hi, nloc, ext, next, out);
+}
 
 int halo_exchange(const trlx_operator *A, const double *x, cudaStream_t st, const double **x_ext) {
     Halo *h = A->halo;
@@ -668,30 +720,77 @@ int dist_create(trlx_comm *comm, int nloc, const long long *row_ptr, const int *
     if (!out || !comm || !comm->impl || nloc <= 0 || !row_ptr || !col_idx || !val) return -1;
     trlb::Comm *cm = comm->impl;
     const int P = cm->size, me = cm->rank;
+    const bool dev = where == TRLX_DEVICE_ARRAYS;
     // Row ranges of all ranks.
     std::vector<double> cnt(P, 0.0);
     cnt[me] = nloc;
     if (int e = cm->reduce_host(cnt.data(), P, trlb::kOpSum)) return e;
     std::vector<long long> start(P + 1, 0);
     for (int p = 0; p < P; ++p) start[p + 1] = start[p] + (long long)cnt[p];
-    const long long row0 = start[me], ntot = start[P];
+    const long long row0 = start[me], ntot = start[P], row1 = row0 + nloc;
     std::vector<long long> rp = to_host(row_ptr, (size_t)nloc + 1, where);
     int bad = rp[0] != 0 || rp[nloc] < 0;
     const long long nnz = bad ? 0 : rp[nloc];
-    std::vector<int> ci = to_host(col_idx, (size_t)nnz, where);
-    std::vector<double> va = to_host(val, (size_t)nnz, where);
-    // Columns owned by other ranks, ascending (hence grouped by owner).
+    // Column indices and values on the device (the caller's device arrays
+    // are read, never changed); the scan over all entries runs there.
+    int *d_ci = dev ? const_cast<int *>(col_idx) : nullptr;
+    double *d_va = dev ? const_cast<double *>(val) : nullptr;
+    int *d_new = nullptr, *d_ext = nullptr, *d_raw = nullptr;
+    long long *d_rp = nullptr;
+    unsigned long long *d_cnt = nullptr;
+    auto cleanup = [&] {
+        if (!dev) {
+            op_free(d_ci);
+            op_free(d_va);
+        }
+        op_free(d_new);
+        op_free(d_ext);
+        op_free(d_raw);
+        op_free(d_rp);
+        op_free(d_cnt);
+    };
     std::vector<int> ext;
-    for (long long k = 0; k < nnz; ++k) {
-        const long long c = ci[k];
-        if (c < 0 || c >= ntot)
-            bad = 1;
-        else if (c < row0 || c >= row0 + nloc)
-            ext.push_back((int)c);
+    if (!bad && nnz > 0) {
+        int rc = 0;
+        if (!dev) {
+            rc = to_device(col_idx, (size_t)nnz, where, &d_ci);
+            if (!rc) rc = to_device(val, (size_t)nnz, where, &d_va);
+        }
+        // d_cnt[0]: out-of-range count, d_cnt[1] (as int): bad column flag.
+        if (!rc && op_alloc(reinterpret_cast<void **>(&d_cnt), 2 * sizeof(unsigned long long)) != cudaSuccess)
+            rc = -2;
+        unsigned long long hc[2] = {0, 0};
+        if (!rc && cudaMemset(d_cnt, 0, sizeof(hc)) != cudaSuccess) rc = -3;
+        int *d_bad = reinterpret_cast<int *>(d_cnt + 1);
+        if (!rc) {
+            trlb::launch_halo_scan(d_ci, nnz, row0, row1, ntot, d_cnt, nullptr, 0, d_bad);
+            if (cudaMemcpy(hc, d_cnt, sizeof(hc), cudaMemcpyDeviceToHost) != cudaSuccess) rc = -3;
+        }
+        const unsigned long long nraw = hc[0];
+        if (!rc && (int)hc[1] != 0) bad = 1;
+        if (!rc && !bad && nraw > 0) {
+            if (op_alloc(reinterpret_cast<void **>(&d_raw), sizeof(int) * nraw) != cudaSuccess) rc = -2;
+            if (!rc && cudaMemset(d_cnt, 0, sizeof(unsigned long long)) != cudaSuccess) rc = -3;
+            if (!rc) {
+                trlb::launch_halo_scan(d_ci, nnz, row0, row1, ntot, d_cnt, d_raw, nraw, d_bad);
+                ext.resize(nraw);
+                if (cudaMemcpy(ext.data(), d_raw, sizeof(int) * nraw, cudaMemcpyDeviceToHost) != cudaSuccess)
+                    rc = -3;
+            }
+        }
+        if (rc) bad = 1;
     }
+    // Every rank takes part in every collective below, also on bad input.
     double flag = bad;
-    if (int e = cm->reduce_host(&flag, 1, trlb::kOpMax)) return e;
-    if (flag != 0.0) return -1;
+    if (int e = cm->reduce_host(&flag, 1, trlb::kOpMax)) {
+        cleanup();
+        return e;
+    }
+    if (flag != 0.0) {
+        cleanup();
+        return -1;
+    }
+    // Columns owned by other ranks, ascending (hence grouped by owner).
     std::sort(ext.begin(), ext.end());
     ext.erase(std::unique(ext.begin(), ext.end()), ext.end());
     const int nhalo = (int)ext.size();
@@ -704,7 +803,10 @@ int dist_create(trlx_comm *comm, int nloc, const long long *row_ptr, const int *
     // counts[p * P + q]: values p sends to q.
     std::vector<double> cm_counts((size_t)P * P, 0.0);
     for (int p = 0; p < P; ++p) cm_counts[(size_t)p * P + me] = (double)(roff[p + 1] - roff[p]);
-    if (int e = cm->reduce_host(cm_counts.data(), cm_counts.size(), trlb::kOpSum)) return e;
+    if (int e = cm->reduce_host(cm_counts.data(), cm_counts.size(), trlb::kOpSum)) {
+        cleanup();
+        return e;
+    }
     std::vector<long> counts(cm_counts.size());
     for (size_t k = 0; k < counts.size(); ++k) counts[k] = (long)cm_counts[k];
     // The requested global indices, on a board with one segment per
@@ -714,7 +816,10 @@ int dist_create(trlx_comm *comm, int nloc, const long long *row_ptr, const int *
     std::vector<double> board((size_t)bo.back(), 0.0);
     for (int p = 0; p < P; ++p)
         for (long k = roff[p]; k < roff[p + 1]; ++k) board[(size_t)bo[(size_t)p * P + me] + (k - roff[p])] = ext[k];
-    if (int e = cm->reduce_host(board.data(), board.size(), trlb::kOpSum)) return e;
+    if (int e = cm->reduce_host(board.data(), board.size(), trlb::kOpSum)) {
+        cleanup();
+        return e;
+    }
     std::vector<long> soff(P + 1, 0);
     std::vector<int> sidx;
     for (int q = 0; q < P; ++q) {
@@ -723,17 +828,19 @@ int dist_create(trlx_comm *comm, int nloc, const long long *row_ptr, const int *
             sidx.push_back((int)((long long)board[(size_t)bo[(size_t)me * P + q] + k] - row0));
         soff[q + 1] = soff[q] + c;
     }
-    // Local numbering: own rows first, then the halo in receive order.
-    for (long long k = 0; k < nnz; ++k) {
-        const long long c = ci[k];
-        if (c >= row0 && c < row0 + nloc)
-            ci[k] = (int)(c - row0);
-        else
-            ci[k] = nloc + (int)(std::lower_bound(ext.begin(), ext.end(), (int)c) - ext.begin());
+    // Local numbering on the device: own rows first, then the halo in
+    // receive order; the local operator is built from device arrays.
+    int rc = to_device(rp.data(), rp.size(), TRLX_HOST_ARRAYS, &d_rp);
+    if (!rc && nnz > 0) {
+        if (op_alloc(reinterpret_cast<void **>(&d_new), sizeof(int) * (size_t)nnz) != cudaSuccess) rc = -2;
+        if (!rc && nhalo > 0) rc = to_device(ext.data(), ext.size(), TRLX_HOST_ARRAYS, &d_ext);
+        if (!rc) trlb::launch_halo_renumber(d_ci, nnz, row0, row1, nloc, d_ext, nhalo, d_new);
     }
     trlx_operator *A = nullptr;
-    int rc = sell ? trlx_sell_create(nloc, rp.data(), ci.data(), va.data(), sigma, TRLX_HOST_ARRAYS, &A)
-                  : trlx_csr_create(nloc, rp.data(), ci.data(), va.data(), TRLX_HOST_ARRAYS, &A);
+    if (!rc)
+        rc = sell ? trlx_sell_create(nloc, d_rp, d_new, d_va, sigma, TRLX_DEVICE_ARRAYS, &A)
+                  : trlx_csr_create(nloc, d_rp, d_new, d_va, TRLX_DEVICE_ARRAYS, &A);
+    cleanup();
     if (rc) return rc;
     auto *h = new trlb::Halo();
     A->halo = h;
