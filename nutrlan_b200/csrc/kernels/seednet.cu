@@ -177,6 +177,11 @@ __global__ void __launch_bounds__(128)
     }
 }
 
+// tcgen05 convolution (kernels/seednet_tc.cu).
+bool conv_tc(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias, __nv_bfloat16 *out, float *out_f32,
+             int B, int H, int W, int dil, int relu);
+int conv_tc_status();
+
 size_t conv_smem_bytes(int dil) {
     return (size_t)kTaps * kC * kRowB + (size_t)3 * (kTX + 2 * dil) * kRowB;
 }
@@ -486,6 +491,9 @@ void pack_input(trlx_seednet *net, int B) {
 
 void conv(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias, __nv_bfloat16 *out, float *out_f32,
           int B, int H, int W, int dil, int relu) {
+    // The tcgen05 kernel (kernels/seednet_tc.cu) where the shape allows;
+    // TRLX_SEEDNET_CONV=mma keeps every layer on k_conv.
+    if (conv_tc(in, w, bias, out, out_f32, B, H, W, dil, relu)) return;
     const size_t smem = conv_smem_bytes(dil);
     static bool attr = false;
     if (!attr) {
@@ -621,7 +629,8 @@ int trlx_seednet_forward(trlx_seednet *net, int B, const float *V, float *out) {
     pack_input(net, B);
     forward(net, B);
     if (out && cudaMemcpy(out, net->Y, P * kOut * 4, cudaMemcpyDefault) != cudaSuccess) return -1001;
-    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1001;
+    if (cudaDeviceSynchronize() != cudaSuccess) return -1001;
+    return conv_tc_status();
 }
 
 // Loss and gradients of a batch (no update); loss_out[b] per sample,
@@ -655,7 +664,8 @@ static int loss_and_grad(trlx_seednet *net, int B, const float *V, const float *
         }
     }
     if (loss_out) cudaMemcpy(loss_out, net->loss, B * 4, cudaMemcpyDeviceToHost);
-    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1001;
+    if (cudaDeviceSynchronize() != cudaSuccess) return -1001;
+    return conv_tc_status();
 }
 
 int trlx_seednet_gradients(trlx_seednet *net, int B, const float *V, const float *U, float lam, float *loss_out,

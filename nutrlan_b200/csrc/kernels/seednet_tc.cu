@@ -1,0 +1,343 @@
+// Seed-network convolution on the 5th-generation tensor cores (tcgen05).
+//
+// The same implicit GEMM as k_conv (pixels x 288 taps*channels x 32 output
+// channels, BF16 in, FP32 accumulate, bias + optional ReLU), Blackwell-style:
+//   * one persistent CTA of 4 warps per SM walks tiles of 128 pixels
+//     (TW x TH pixels of one sample: a full 128-pixel row segment, or 2 rows
+//     of 64, ...);
+//   * the 3x3 taps of a tile are 9 TMA loads of 128 pixels x 32 channels
+//     (64 B per pixel, 64-byte swizzle) from the NHWC activations, at
+//     coordinates shifted by the dilated tap offset: the "same" zero padding
+//     is the TMA's out-of-bounds fill.  Tiles are double-buffered;
+//   * the weights ([tap][co][ci], 9 x 32 x 64 B, same swizzle) are one TMA
+//     load per CTA;
+//   * one thread issues 18 tcgen05.mma (M = 128, N = 32, K = 16, kind::f16
+//     with BF16 operands) from shared-memory descriptors into a TMEM
+//     accumulator of 32 columns and commits to an mbarrier;
+//   * the 4 warps read the accumulator with tcgen05.ld (warp w: TMEM lanes =
+//     pixels 32w .. 32w+31, 32 channels each), add the bias, apply the ReLU
+//     and store BF16 NHWC (or the first 16 channels as FP32 for the last
+//     layer).
+// Every mbarrier wait is bounded; a wait that runs out sets a device flag
+// (read by the seed-network entry points) and the kernel still runs to its
+// end, so the TMEM allocation is always released.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+
+namespace trlb {
+namespace seednet {
+namespace {
+
+constexpr int kTM = 128;                      // pixels per tile (MMA M)
+constexpr int kCh = 32;                       // channels (MMA N and K per tap)
+constexpr int kTapsTC = 9;
+constexpr int kRow = kCh * 2;                 // bytes per pixel / weight row
+constexpr int kTapA = kTM * kRow;             // 8 KB per tap tile
+constexpr int kStageA = kTapsTC * kTapA;      // 72 KB per pixel tile
+constexpr int kTapW = kCh * kRow;             // 2 KB per tap of weights
+constexpr int kWBytes = kTapsTC * kTapW;      // 18 KB
+constexpr int kOffA = kWBytes;                // 1 KB aligned
+constexpr int kOffBar = kOffA + 2 * kStageA;  // mbarriers after the buffers
+constexpr size_t kSmemTC = kOffBar + 64 + 1024;  // + alignment slack
+constexpr long kWaitLimit = 1L << 24;
+
+__device__ int g_tc_error = 0;
+
+__device__ __forceinline__ unsigned saddr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void bar_init(uint64_t *b, unsigned n) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(n) : "memory");
+}
+__device__ __forceinline__ void bar_expect(uint64_t *b, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bar_try(uint64_t *b, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(saddr(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait; on timeout records the failure and returns.
+__device__ __forceinline__ void bar_wait(uint64_t *b, unsigned parity) {
+    for (long i = 0; !bar_try(b, parity); ++i) {
+        if (i > kWaitLimit) {
+            atomicExch(&g_tc_error, 1);
+            return;
+        }
+    }
+}
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1, int c2,
+                                            int c3) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
+        "[%2];" ::"r"(saddr(dst)),
+        "l"(map), "r"(saddr(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+        "[%2];" ::"r"(saddr(dst)),
+        "l"(map), "r"(saddr(bar)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major operand, rows of 64 B in 8-row
+// groups 512 B apart, 64-byte swizzle (layout type 4), descriptor version 1.
+__device__ __forceinline__ uint64_t smem_desc(unsigned addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);        // start address
+    d |= (uint64_t)1 << 16;                        // leading byte offset (unused with swizzle)
+    d |= (uint64_t)((512 >> 4) & 0x3FFF) << 32;    // stride byte offset: 8 rows x 64 B
+    d |= (uint64_t)1 << 46;                        // version
+    d |= (uint64_t)4 << 61;                        // SWIZZLE_64B
+    return d;
+}
+// Instruction descriptor: D FP32, A and B BF16, both K-major, N = 32, M = 128.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kCh >> 3) << 17) |
+                            ((uint32_t)(kTM >> 4) << 24);
+
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
+        "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ unsigned pack2(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<unsigned *>(&v);
+}
+
+__global__ void __launch_bounds__(128, 1)
+    k_conv_tc(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap twt,
+              const float *__restrict__ bias, __nv_bfloat16 *out, float *out_f32, int H, int W, int TW, int TH,
+              int dil, int relu, int ntiles) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *sm = reinterpret_cast<unsigned char *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char *ws = sm;
+    unsigned char *as = sm + kOffA;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + kOffBar);  // full[0], full[1], weights, mma
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 4);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tiles_x = W / TW, tiles_y = H / TH;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tslot)),
+                     "r"(32)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int k = 0; k < 4; ++k) bar_init(bars + k, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    auto issue = [&](int tile, int stage) {
+        const int tx = tile % tiles_x, rest = tile / tiles_x;
+        const int ty = rest % tiles_y, b = rest / tiles_y;
+        const int x0 = tx * TW, y0 = ty * TH;
+        uint64_t *bar = bars + stage;
+        bar_expect(bar, kStageA);
+        for (int tap = 0; tap < kTapsTC; ++tap) {
+            const int dy = (tap / 3 - 1) * dil, dx = (tap % 3 - 1) * dil;
+            tma_load_4d(as + stage * kStageA + tap * kTapA, &tin, bar, 0, x0 + dx, y0 + dy, b);
+        }
+    };
+    if (tid == 0) {
+        bar_expect(bars + 2, kWBytes);
+        tma_load_3d(ws, &twt, bars + 2, 0, 0, 0);
+        if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+        if ((int)(blockIdx.x + gridDim.x) < ntiles) issue(blockIdx.x + gridDim.x, 1);
+    }
+    float bv[kCh];
+#pragma unroll
+    for (int c = 0; c < kCh; ++c) bv[c] = bias ? bias[c] : 0.f;
+
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        const int stage = it & 1;
+        if (tid == 0) {
+            if (it == 0) bar_wait(bars + 2, 0);
+            bar_wait(bars + stage, (unsigned)((it >> 1) & 1));
+            tc_fence_after();
+            const unsigned a0 = saddr(as + stage * kStageA), w0 = saddr(ws);
+#pragma unroll 1
+            for (int tap = 0; tap < kTapsTC; ++tap)
+#pragma unroll
+                for (int k = 0; k < 2; ++k)
+                    mma_f16(tmem, smem_desc(a0 + tap * kTapA + k * 32), smem_desc(w0 + tap * kTapW + k * 32),
+                            (tap | k) != 0);
+            mma_commit(bars + 3);
+        }
+        bar_wait(bars + 3, (unsigned)(it & 1));
+        tc_fence_after();
+        // The MMAs finished reading this stage: refill it two tiles ahead.
+        if (tid == 0 && tile + 2 * (int)gridDim.x < ntiles) issue(tile + 2 * gridDim.x, stage);
+        uint32_t r[32];
+        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16), r);
+        const int tx = tile % tiles_x, rest = tile / tiles_x;
+        const int ty = rest % tiles_y, b = rest / tiles_y;
+        const int i = warp * 32 + lane;
+        const long p = ((long)b * H + ty * TH + i / TW) * W + tx * TW + i % TW;
+        float v[kCh];
+#pragma unroll
+        for (int c = 0; c < kCh; ++c) {
+            v[c] = __uint_as_float(r[c]) + bv[c];
+            if (relu) v[c] = fmaxf(v[c], 0.f);
+        }
+        if (out_f32) {
+            float4 *o = reinterpret_cast<float4 *>(out_f32 + p * 16);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        } else {
+            uint4 *o = reinterpret_cast<uint4 *>(out + p * kCh);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                o[q] = make_uint4(pack2(v[8 * q], v[8 * q + 1]), pack2(v[8 * q + 2], v[8 * q + 3]),
+                                  pack2(v[8 * q + 4], v[8 * q + 5]), pack2(v[8 * q + 6], v[8 * q + 7]));
+        }
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32) : "memory");
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encoder() {
+    static EncodeTiled fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (EncodeTiled) nullptr;
+        }
+        return reinterpret_cast<EncodeTiled>(p);
+    }();
+    return fn;
+}
+
+// Reports once why the tcgen05 kernel is not used (the mma.sync kernel runs).
+void tc_note(const char *why) {
+    static bool said = false;
+    if (!said) std::fprintf(stderr, "TRLAN-B200: seed network on the mma.sync convolution: %s\n", why);
+    said = true;
+}
+
+bool tc_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("TRLX_SEEDNET_CONV");
+        if (e && e[0] == 'm') return false;  // "mma": the mma.sync kernel
+        if (!encoder()) {
+            tc_note("cuTensorMapEncodeTiled not available");
+            return false;
+        }
+        const cudaError_t err =
+            cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTC);
+        if (err != cudaSuccess) {
+            tc_note(cudaGetErrorString(err));
+            cudaGetLastError();
+            return false;
+        }
+        return true;
+    }();
+    return on;
+}
+
+}  // namespace
+
+// Runs the convolution on the tcgen05 kernel when the shape allows (tiles of
+// 128 pixels: W a multiple of min(W, 128) and H of 128 / min(W, 128)) and
+// returns true; false leaves it to the caller's kernel.
+bool conv_tc(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias, __nv_bfloat16 *out, float *out_f32,
+             int B, int H, int W, int dil, int relu) {
+    if (!tc_enabled()) return false;
+    const int TW = W < kTM ? W : kTM;
+    if (TW < 8 || kTM % TW != 0 || W % TW != 0) return false;
+    const int TH = kTM / TW;
+    if (H % TH != 0) return false;
+    if (((uintptr_t)in & 15) || ((uintptr_t)w & 15)) {
+        tc_note("operands not 16-byte aligned");
+        return false;
+    }
+    CUtensorMap tin, twt;
+    const cuuint64_t din[4] = {(cuuint64_t)kCh, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+    const cuuint64_t sin[3] = {(cuuint64_t)kRow, (cuuint64_t)W * kRow, (cuuint64_t)H * W * kRow};
+    const cuuint32_t bin[4] = {(cuuint32_t)kCh, (cuuint32_t)TW, (cuuint32_t)TH, 1};
+    const cuuint32_t ones[4] = {1, 1, 1, 1};
+    if (encoder()(&tin, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(in), din, sin, bin, ones,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+        tc_note("activation tensor map rejected");
+        return false;
+    }
+    const cuuint64_t dw[3] = {(cuuint64_t)kCh, (cuuint64_t)kCh, (cuuint64_t)kTapsTC};
+    const cuuint64_t sw[2] = {(cuuint64_t)kRow, (cuuint64_t)kTapW};
+    const cuuint32_t bw[3] = {(cuuint32_t)kCh, (cuuint32_t)kCh, (cuuint32_t)kTapsTC};
+    if (encoder()(&twt, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16 *>(w), dw, sw, bw, ones,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+        tc_note("weight tensor map rejected");
+        return false;
+    }
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    const int ntiles = B * (H / TH) * (W / TW);
+    const int grid = ntiles < sms ? ntiles : sms;
+    k_conv_tc<<<grid, 128, kSmemTC>>>(tin, twt, bias, out, out_f32, H, W, TW, TH, dil, relu, ntiles);
+    return true;
+}
+
+// Reads and clears the flag of a timed-out wait in k_conv_tc (a sync point).
+int conv_tc_status() {
+    int v = 0, zero = 0;
+    if (cudaMemcpyFromSymbol(&v, g_tc_error, sizeof(int)) != cudaSuccess) return -1001;
+    if (v) cudaMemcpyToSymbol(g_tc_error, &zero, sizeof(int));
+    return v ? -1012 : 0;
+}
+
+}  // namespace seednet
+}  // namespace trlb
