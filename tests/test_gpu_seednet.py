@@ -178,3 +178,45 @@ def test_learned_seed_on_held_out_wells():
     print("untrained", su)
     assert np.median([r["seed_res_median"] for r in rt]) < 0.3 * np.median([r["seed_res_median"] for r in ru])
     assert st["rr_matvec"] < su["rr_matvec"] and st["sum_matvec"] < su["sum_matvec"], (st, su)
+
+
+_CONV_CHILD = r"""
+import sys, numpy as np
+sys.path.insert(0, {root!r})
+from nutrlan_b200.seednet import SeedNet
+from oracle import seednet_np as sn
+H, W, B = {H}, {W}, 2
+net = SeedNet(H, W, max_batch=B)
+net.weights = sn.init_params(5).astype(np.float32)
+rng = np.random.default_rng(6)
+V = (-50.0 * rng.random((B, H, W))).astype(np.float32)
+U = np.stack([np.linalg.qr(rng.standard_normal((H * W, 16)))[0] for _ in range(B)]).astype(np.float32)
+Y = net.forward(V)
+loss, g = net.gradients(V, U, 1.0)
+np.savez({out!r}, Y=Y, g=g, loss=loss)
+net.close()
+"""
+
+
+@pytest.mark.parametrize("H,W", [(16, 64), (64, 128)])
+def test_tcgen05_convolution_equals_mma_sync(tmp_path, H, W):
+    """The tcgen05 convolution (TMA tap tiles, TMEM accumulator) against the
+    mma.sync convolution (TRLX_SEEDNET_CONV=mma, in a child process): the
+    network output, the loss and every weight gradient agree to 1e-6
+    relative (both accumulate the same K = 16 steps in FP32)."""
+    import subprocess, sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = {}
+    for mode in ("mma", "tc"):
+        env = dict(os.environ)
+        env.pop("TRLX_SEEDNET_CONV", None)
+        if mode == "mma":
+            env["TRLX_SEEDNET_CONV"] = "mma"
+        out = str(tmp_path / f"{mode}.npz")
+        r = subprocess.run([sys.executable, "-c", _CONV_CHILD.format(root=root, H=H, W=W, out=out)], env=env,
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+        assert "mma.sync convolution" not in r.stderr or mode == "mma", r.stderr
+        res[mode] = np.load(out)
+    for key in ("Y", "loss", "g"):
+        assert _rel(res["tc"][key], res["mma"][key]) <= 1e-6, key
