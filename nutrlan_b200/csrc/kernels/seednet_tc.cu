@@ -42,7 +42,7 @@ constexpr int kTapW = kCh * kRow;             // 2 KB per tap of weights
 constexpr int kWBytes = kTapsTC * kTapW;      // 18 KB
 constexpr int kOffA = kWBytes;                // 1 KB aligned
 constexpr int kOffBar = kOffA + 2 * kStageA;  // mbarriers after the buffers
-constexpr size_t kSmemTC = kOffBar + 64 + 1024;  // + alignment slack
+constexpr size_t kSmemTC = kOffBar + 128 + 1024;  // 7 mbarriers + TMEM slot + alignment slack
 constexpr long kWaitLimit = 1L << 24;
 
 __device__ int g_tc_error = 0;
@@ -135,7 +135,15 @@ __device__ __forceinline__ unsigned pack2(float lo, float hi) {
     return *reinterpret_cast<unsigned *>(&v);
 }
 
-__global__ void __launch_bounds__(128, 1)
+// Warp roles: warps 0-3 read the accumulator (warp w owns TMEM lanes = tile
+// pixels 32w .. 32w+31), one lane of warp 4 issues the TMA loads and the
+// MMAs.  Two accumulators of 32 TMEM columns alternate between tiles, so the
+// MMAs of tile i+1 run while tile i's epilogue reads its accumulator.
+// Barriers: full[s] (tile loaded into stage s), done[a] (MMAs into
+// accumulator a finished: the epilogue may read it and stage s may be
+// refilled), empty[a] (the 4 epilogue warps finished reading accumulator
+// a), weights.
+__global__ void __launch_bounds__(160, 1)
     k_conv_tc(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap twt,
               const float *__restrict__ bias, __nv_bfloat16 *out, float *out_f32, int H, int W, int TW, int TH,
               int dil, int relu, int ntiles) {
@@ -143,98 +151,117 @@ __global__ void __launch_bounds__(128, 1)
     unsigned char *sm = reinterpret_cast<unsigned char *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char *ws = sm;
     unsigned char *as = sm + kOffA;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + kOffBar);  // full[0], full[1], weights, mma
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 4);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + kOffBar);
+    uint64_t *full = bars, *done = bars + 2, *empty = bars + 4, *wbar = bars + 6;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 7);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tiles_x = W / TW, tiles_y = H / TH;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tslot)),
-                     "r"(32)
+                     "r"(64)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
         for (int k = 0; k < 4; ++k) bar_init(bars + k, 1);
+        bar_init(empty, 4);
+        bar_init(empty + 1, 4);
+        bar_init(wbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tslot;
+    const int my_tiles = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
 
-    auto issue = [&](int tile, int stage) {
-        const int tx = tile % tiles_x, rest = tile / tiles_x;
-        const int ty = rest % tiles_y, b = rest / tiles_y;
-        const int x0 = tx * TW, y0 = ty * TH;
-        uint64_t *bar = bars + stage;
-        bar_expect(bar, kStageA);
-        for (int tap = 0; tap < kTapsTC; ++tap) {
-            const int dy = (tap / 3 - 1) * dil, dx = (tap % 3 - 1) * dil;
-            tma_load_4d(as + stage * kStageA + tap * kTapA, &tin, bar, 0, x0 + dx, y0 + dy, b);
-        }
-    };
-    if (tid == 0) {
-        bar_expect(bars + 2, kWBytes);
-        tma_load_3d(ws, &twt, bars + 2, 0, 0, 0);
-        if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
-        if ((int)(blockIdx.x + gridDim.x) < ntiles) issue(blockIdx.x + gridDim.x, 1);
-    }
-    float bv[kCh];
-#pragma unroll
-    for (int c = 0; c < kCh; ++c) bv[c] = bias ? bias[c] : 0.f;
-
-    int it = 0;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-        const int stage = it & 1;
-        if (tid == 0) {
-            if (it == 0) bar_wait(bars + 2, 0);
-            bar_wait(bars + stage, (unsigned)((it >> 1) & 1));
-            tc_fence_after();
-            const unsigned a0 = saddr(as + stage * kStageA), w0 = saddr(ws);
+    if (warp == 4) {
+        if (lane == 0) {
+            auto issue = [&](int it) {
+                const int tile = blockIdx.x + it * gridDim.x;
+                const int tx = tile % tiles_x, rest = tile / tiles_x;
+                const int ty = rest % tiles_y, b = rest / tiles_y;
+                const int x0 = tx * TW, y0 = ty * TH, st = it & 1;
+                bar_expect(full + st, kStageA);
+                for (int tap = 0; tap < kTapsTC; ++tap) {
+                    const int dy = (tap / 3 - 1) * dil, dx = (tap % 3 - 1) * dil;
+                    tma_load_4d(as + st * kStageA + tap * kTapA, &tin, full + st, 0, x0 + dx, y0 + dy, b);
+                }
+            };
+            // Every load issued here is waited for below (no copy is in
+            // flight when the CTA exits).
+            if (my_tiles > 0) {
+                bar_expect(wbar, kWBytes);
+                tma_load_3d(ws, &twt, wbar, 0, 0, 0);
+                issue(0);
+            }
+            if (my_tiles > 1) issue(1);
+            if (my_tiles > 0) bar_wait(wbar, 0);
+            const unsigned w0 = saddr(ws);
+            for (int it = 0; it < my_tiles; ++it) {
+                const int st = it & 1, acc = it & 1;
+                bar_wait(full + st, (unsigned)((it >> 1) & 1));
+                if (it >= 2) bar_wait(empty + acc, (unsigned)(((it >> 1) - 1) & 1));
+                tc_fence_after();
+                const unsigned a0 = saddr(as + st * kStageA);
+                const uint32_t d = tmem + (uint32_t)(acc * kCh);
 #pragma unroll 1
-            for (int tap = 0; tap < kTapsTC; ++tap)
+                for (int tap = 0; tap < kTapsTC; ++tap)
 #pragma unroll
-                for (int k = 0; k < 2; ++k)
-                    mma_f16(tmem, smem_desc(a0 + tap * kTapA + k * 32), smem_desc(w0 + tap * kTapW + k * 32),
-                            (tap | k) != 0);
-            mma_commit(bars + 3);
+                    for (int k = 0; k < 2; ++k)
+                        mma_f16(d, smem_desc(a0 + tap * kTapA + k * 32), smem_desc(w0 + tap * kTapW + k * 32),
+                                (tap | k) != 0);
+                mma_commit(done + acc);
+                if (it + 2 < my_tiles) {
+                    // The MMAs have read stage st once they complete.
+                    bar_wait(done + acc, (unsigned)((it >> 1) & 1));
+                    issue(it + 2);
+                }
+            }
         }
-        bar_wait(bars + 3, (unsigned)(it & 1));
-        tc_fence_after();
-        // The MMAs finished reading this stage: refill it two tiles ahead.
-        if (tid == 0 && tile + 2 * (int)gridDim.x < ntiles) issue(tile + 2 * gridDim.x, stage);
-        uint32_t r[32];
-        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16), r);
-        const int tx = tile % tiles_x, rest = tile / tiles_x;
-        const int ty = rest % tiles_y, b = rest / tiles_y;
-        const int i = warp * 32 + lane;
-        const long p = ((long)b * H + ty * TH + i / TW) * W + tx * TW + i % TW;
-        float v[kCh];
+    } else {
+        float bv[kCh];
 #pragma unroll
-        for (int c = 0; c < kCh; ++c) {
-            v[c] = __uint_as_float(r[c]) + bv[c];
-            if (relu) v[c] = fmaxf(v[c], 0.f);
+        for (int c = 0; c < kCh; ++c) bv[c] = bias ? bias[c] : 0.f;
+        for (int it = 0; it < my_tiles; ++it) {
+            const int acc = it & 1;
+            const int tile = blockIdx.x + it * gridDim.x;
+            bar_wait(done + acc, (unsigned)((it >> 1) & 1));
+            tc_fence_after();
+            uint32_t r[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(acc * kCh), r);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(empty + acc)) : "memory");
+            const int tx = tile % tiles_x, rest = tile / tiles_x;
+            const int ty = rest % tiles_y, b = rest / tiles_y;
+            const int i = warp * 32 + lane;
+            const long p = ((long)b * H + ty * TH + i / TW) * W + tx * TW + i % TW;
+            float v[kCh];
+#pragma unroll
+            for (int c = 0; c < kCh; ++c) {
+                v[c] = __uint_as_float(r[c]) + bv[c];
+                if (relu) v[c] = fmaxf(v[c], 0.f);
+            }
+            if (out_f32) {
+                float4 *o = reinterpret_cast<float4 *>(out_f32 + p * 16);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            } else {
+                uint4 *o = reinterpret_cast<uint4 *>(out + p * kCh);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    o[q] = make_uint4(pack2(v[8 * q], v[8 * q + 1]), pack2(v[8 * q + 2], v[8 * q + 3]),
+                                      pack2(v[8 * q + 4], v[8 * q + 5]), pack2(v[8 * q + 6], v[8 * q + 7]));
+            }
         }
-        if (out_f32) {
-            float4 *o = reinterpret_cast<float4 *>(out_f32 + p * 16);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-        } else {
-            uint4 *o = reinterpret_cast<uint4 *>(out + p * kCh);
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                o[q] = make_uint4(pack2(v[8 * q], v[8 * q + 1]), pack2(v[8 * q + 2], v[8 * q + 3]),
-                                  pack2(v[8 * q + 4], v[8 * q + 5]), pack2(v[8 * q + 6], v[8 * q + 7]));
-        }
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
     }
     tc_fence_before();
     __syncthreads();
+    tc_fence_after();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
 }
 
 using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -327,7 +354,7 @@ bool conv_tc(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
     }
     const int ntiles = B * (H / TH) * (W / TW);
     const int grid = ntiles < sms ? ntiles : sms;
-    k_conv_tc<<<grid, 128, kSmemTC>>>(tin, twt, bias, out, out_f32, H, W, TW, TH, dil, relu, ntiles);
+    k_conv_tc<<<grid, 160, kSmemTC>>>(tin, twt, bias, out, out_f32, H, W, TW, TH, dil, relu, ntiles);
     return true;
 }
 
