@@ -289,24 +289,35 @@ void tc_note(const char *why) {
     said = true;
 }
 
+// Per device (the shared-memory attribute is set on the current device):
+// 0 not tried, 1 usable, -1 not usable.
+constexpr int kMaxDev = 64;
+int g_dev_state[kMaxDev] = {};
+
 bool tc_enabled() {
-    static const bool on = [] {
+    static const bool allowed = [] {
         const char *e = std::getenv("TRLX_SEEDNET_CONV");
         if (e && e[0] == 'm') return false;  // "mma": the mma.sync kernel
         if (!encoder()) {
             tc_note("cuTensorMapEncodeTiled not available");
             return false;
         }
+        return true;
+    }();
+    if (!allowed) return false;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kMaxDev) return false;
+    if (g_dev_state[dev] == 0) {
         const cudaError_t err =
             cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTC);
         if (err != cudaSuccess) {
             tc_note(cudaGetErrorString(err));
             cudaGetLastError();
-            return false;
         }
-        return true;
-    }();
-    return on;
+        g_dev_state[dev] = err == cudaSuccess ? 1 : -1;
+    }
+    return g_dev_state[dev] == 1;
 }
 
 }  // namespace
@@ -355,6 +366,11 @@ bool conv_tc(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
     const int ntiles = B * (H / TH) * (W / TW);
     const int grid = ntiles < sms ? ntiles : sms;
     k_conv_tc<<<grid, 160, kSmemTC>>>(tin, twt, bias, out, out_f32, H, W, TW, TH, dil, relu, ntiles);
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) {  // not launched: the caller's kernel runs instead
+        tc_note(cudaGetErrorString(err));
+        return false;
+    }
     return true;
 }
 
