@@ -181,6 +181,9 @@ __global__ void __launch_bounds__(128)
 bool conv_tc(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias, __nv_bfloat16 *out, float *out_f32,
              int B, int H, int W, int dil, int relu);
 int conv_tc_status();
+// tcgen05 weight gradient: blocks whose partials it wrote, or 0.
+int wgrad_tc(const __nv_bfloat16 *in, const __nv_bfloat16 *g, float *part, int max_blocks, int B, int H, int W,
+             int dil);
 
 size_t conv_smem_bytes(int dil) {
     return (size_t)kTaps * kC * kRowB + (size_t)3 * (kTX + 2 * dil) * kRowB;
@@ -652,11 +655,18 @@ static int loss_and_grad(trlx_seednet *net, int B, const float *V, const float *
     __nv_bfloat16 *g = net->g0, *gn = net->g1;
     for (int l = kLayers - 1; l >= 0; --l) {
         if (l < kLayers - 1) k_relu_mask<<<blocks_for(P * kC), 256>>>(g, net->act[l + 1], P * kC);
-        k_conv_wgrad<<<nwg, kWgWarps * 32, wgrad_smem_bytes(kDil[l])>>>(net->act[l], g, net->part, B, H, W, kDil[l]);
+        // tcgen05 kernel where W allows (TRLX_SEEDNET_CONV=mma: mma.sync).
+        int nb = wgrad_tc(net->act[l], g, net->part, (int)(net->part_len / ((size_t)(kTaps + 1) * kC * kC)), B, H,
+                          W, kDil[l]);
+        if (nb == 0) {
+            k_conv_wgrad<<<nwg, kWgWarps * 32, wgrad_smem_bytes(kDil[l])>>>(net->act[l], g, net->part, B, H, W,
+                                                                              kDil[l]);
+            nb = nwg;
+        }
         // Partials have stride (kTaps + 1) * kC * kC; only the weight taps and
         // the kC bias entries after them are written and reduced.
         const int len = kTaps * kC * kC + kC;
-        k_reduce_parts<<<(len + 255) / 256, 256>>>(net->part, nwg, (kTaps + 1) * kC * kC, len, net->gw[l]);
+        k_reduce_parts<<<(len + 255) / 256, 256>>>(net->part, nb, (kTaps + 1) * kC * kC, len, net->gw[l]);
         cudaMemcpyAsync(net->gb[l], net->gw[l] + (size_t)kTaps * kC * kC, kC * 4, cudaMemcpyDeviceToDevice);
         if (l > 0) {
             conv(g, net->wb[l], nullptr, gn, nullptr, B, H, W, kDil[l], 0);

@@ -264,6 +264,147 @@ __global__ void __launch_bounds__(160, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
 }
 
+// ---------------------------------------------------------------------------
+// Weight gradient on tcgen05: dW[tap][ci][co] = sum_p in[p + off(tap)][ci] *
+// g[p][co] and db[co] = sum_p g[p][co], as a GEMM over pixels (K) with the
+// taps stacked along M: accumulator group j (M = 128 rows = 4 slots x 32
+// ci) covers taps 4j .. 4j+3; the third group holds tap 8, a slot of ones
+// (its rows give db) and two zero slots.  Both operands are MN-major (ci or
+// co contiguous, 64 B per pixel, 64-byte swizzle): a stage is one 64-pixel
+// row segment, i.e. 9 TMA loads of the shifted input (zero fill outside the
+// image) and one of g, 4 KB each, into slots 4 KB apart (the descriptors'
+// leading byte offset between M atoms; 8-pixel K atoms are 512 B apart).
+// One CTA per SM accumulates its segments in TMEM (3 x 32 columns), then
+// writes the per-block partials part[block][tap][ci][co] (+ [9][0][co] =
+// db) that k_reduce_parts sums in block order.
+constexpr int kWSeg = 64;                                   // pixels per stage (K)
+constexpr int kWSlot = kWSeg * kRow;                        // 4 KB
+constexpr int kWSlots = 12;                                 // 9 taps, ones, 2 zero
+constexpr int kWStage = (kWSlots + 1) * kWSlot;             // + g tile: 52 KB
+constexpr int kWStages = 3;
+constexpr int kWOffBar = kWStages * kWStage;
+constexpr size_t kSmemWG = kWOffBar + 128 + 1024;
+constexpr uint32_t kIdescMN = kIdesc | (1u << 15) | (1u << 16);  // A and B MN-major
+
+__device__ __forceinline__ uint64_t smem_desc_mn(unsigned addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);               // start address
+    d |= (uint64_t)((kWSlot >> 4) & 0x3FFF) << 16;       // leading byte offset: next 32-wide M atom
+    d |= (uint64_t)((512 >> 4) & 0x3FFF) << 32;          // stride byte offset: next 8 pixels of K
+    d |= (uint64_t)1 << 46;                              // version
+    d |= (uint64_t)4 << 61;                              // SWIZZLE_64B
+    return d;
+}
+__device__ __forceinline__ void mma_f16_mn(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(kIdescMN), "r"(accumulate)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(160, 1)
+    k_wgrad_tc(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tg, float *part, int H,
+               int W, int dil, int nseg) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *sm = reinterpret_cast<unsigned char *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + kWOffBar);
+    uint64_t *full = bars, *done = bars + kWStages, *fin = bars + 2 * kWStages;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * kWStages + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int segs_x = W / kWSeg;
+    const int my = (int)blockIdx.x < nseg ? (nseg - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    // Constant slots of every stage: ones (slot 9), zeros (10, 11).
+    for (int st = 0; st < kWStages; ++st) {
+        uint4 *o = reinterpret_cast<uint4 *>(sm + st * kWStage + 9 * kWSlot);
+        const unsigned one2 = 0x3F803F80u;  // two bf16 1.0
+        for (int i = tid; i < 3 * kWSlot / 16; i += blockDim.x)
+            o[i] = i < kWSlot / 16 ? make_uint4(one2, one2, one2, one2) : make_uint4(0u, 0u, 0u, 0u);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tslot)),
+                     "r"(128)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int k = 0; k < 2 * kWStages + 1; ++k) bar_init(bars + k, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (warp == 4) {
+        if (lane == 0) {
+            auto issue = [&](int it) {
+                const int seg = blockIdx.x + it * gridDim.x;
+                const int sx = seg % segs_x, rest = seg / segs_x;
+                const int y = rest % H, b = rest / H, x0 = sx * kWSeg;
+                const int st = it % kWStages;
+                unsigned char *base = sm + st * kWStage;
+                bar_expect(full + st, 10 * kWSlot);
+                for (int tap = 0; tap < 9; ++tap) {
+                    const int dy = (tap / 3 - 1) * dil, dx = (tap % 3 - 1) * dil;
+                    tma_load_4d(base + tap * kWSlot, &tin, full + st, 0, x0 + dx, y + dy, b);
+                }
+                tma_load_4d(base + kWSlots * kWSlot, &tg, full + st, 0, x0, y, b);
+            };
+            for (int it = 0; it < my && it < kWStages; ++it) issue(it);
+            for (int it = 0; it < my; ++it) {
+                const int st = it % kWStages;
+                const unsigned ph = (unsigned)((it / kWStages) & 1);
+                bar_wait(full + st, ph);
+                tc_fence_after();
+                const unsigned a0 = saddr(sm + st * kWStage), b0 = a0 + kWSlots * kWSlot;
+#pragma unroll 1
+                for (int grp = 0; grp < 3; ++grp)
+#pragma unroll
+                    for (int k = 0; k < kWSeg / 16; ++k)
+                        mma_f16_mn(tmem + (uint32_t)(grp * kCh), smem_desc_mn(a0 + grp * 4 * kWSlot + k * 1024),
+                                   smem_desc_mn(b0 + k * 1024), (it | k) != 0);
+                mma_commit(done + st);
+                if (it + kWStages < my) {
+                    bar_wait(done + st, ph);  // the MMAs have read this stage
+                    issue(it + kWStages);
+                }
+            }
+            mma_commit(fin);
+        }
+    } else if (my > 0) {
+        bar_wait(fin, 0);
+        tc_fence_after();
+        float *pb = part + (size_t)blockIdx.x * (kTapsTC + 1) * kCh * kCh;
+#pragma unroll 1
+        for (int grp = 0; grp < 3; ++grp) {
+            uint32_t r[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(grp * kCh), r);
+            const int slot = grp * 4 + warp;  // row block: tap, or ones (9), or zeros
+            if (slot < 9) {
+                float4 *o = reinterpret_cast<float4 *>(pb + ((size_t)slot * kCh + lane) * kCh);
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    o[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
+                                       __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
+            } else if (slot == 9 && lane == 0) {
+                float4 *o = reinterpret_cast<float4 *>(pb + (size_t)kTapsTC * kCh * kCh);
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    o[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
+                                       __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128) : "memory");
+}
+
 using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -372,6 +513,57 @@ bool conv_tc(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
         return false;
     }
     return true;
+}
+
+// Weight gradient on the tcgen05 kernel when W is a multiple of 64: returns
+// the number of blocks whose partials it wrote (at most max_blocks), or 0 to
+// leave it to the caller's kernel.
+int wgrad_tc(const __nv_bfloat16 *in, const __nv_bfloat16 *g, float *part, int max_blocks, int B, int H, int W,
+             int dil) {
+    if (!tc_enabled() || W % kWSeg != 0) return 0;
+    static int wg_ok[kMaxDev] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kMaxDev) return 0;
+    if (wg_ok[dev] == 0) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemWG);
+        if (e != cudaSuccess) {
+            tc_note(cudaGetErrorString(e));
+            cudaGetLastError();
+        }
+        wg_ok[dev] = e == cudaSuccess ? 1 : -1;
+    }
+    if (wg_ok[dev] != 1) return 0;
+    if (((uintptr_t)in & 15) || ((uintptr_t)g & 15)) return 0;
+    CUtensorMap tin, tgm;
+    const cuuint64_t dims[4] = {(cuuint64_t)kCh, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+    const cuuint64_t strides[3] = {(cuuint64_t)kRow, (cuuint64_t)W * kRow, (cuuint64_t)H * W * kRow};
+    const cuuint32_t box[4] = {(cuuint32_t)kCh, (cuuint32_t)kWSeg, 1, 1};
+    const cuuint32_t ones[4] = {1, 1, 1, 1};
+    if (encoder()(&tin, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(in), dims, strides, box,
+                  ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
+        encoder()(&tgm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(g), dims, strides, box,
+                  ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+        tc_note("weight-gradient tensor map rejected");
+        return 0;
+    }
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+    const int nseg = B * H * (W / kWSeg);
+    int grid = nseg < sms ? nseg : sms;
+    if (grid > max_blocks) grid = max_blocks;
+    if (grid < 1) return 0;
+    k_wgrad_tc<<<grid, 160, kSmemWG>>>(tin, tgm, part, H, W, dil, nseg);
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) {
+        tc_note(cudaGetErrorString(err));
+        return 0;
+    }
+    return grid;
 }
 
 // Reads and clears the flag of a timed-out wait in k_conv_tc (a sync point).

@@ -200,10 +200,12 @@ net.close()
 
 @pytest.mark.parametrize("H,W", [(16, 64), (64, 128)])
 def test_tcgen05_convolution_equals_mma_sync(tmp_path, H, W):
-    """The tcgen05 convolution (TMA tap tiles, TMEM accumulator) against the
-    mma.sync convolution (TRLX_SEEDNET_CONV=mma, in a child process): the
-    network output, the loss and every weight gradient agree to 1e-6
-    relative (both accumulate the same K = 16 steps in FP32)."""
+    """The tcgen05 kernels (convolution and weight gradient: TMA tiles, TMEM
+    accumulators) against the mma.sync kernels (TRLX_SEEDNET_CONV=mma, in a
+    child process): the network output and the loss agree to 1e-6 relative
+    (both accumulate the same K = 16 steps in FP32; bitwise in practice), the
+    weight gradients to 1e-5 (the pixel sums are split over blocks
+    differently)."""
     import subprocess, sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     res = {}
@@ -218,5 +220,6 @@ def test_tcgen05_convolution_equals_mma_sync(tmp_path, H, W):
         assert r.returncode == 0, r.stderr[-2000:]
         assert "mma.sync convolution" not in r.stderr or mode == "mma", r.stderr
         res[mode] = np.load(out)
-    for key in ("Y", "loss", "g"):
+    for key in ("Y", "loss"):
         assert _rel(res["tc"][key], res["mma"][key]) <= 1e-6, key
+    assert _rel(res["tc"]["g"], res["mma"]["g"]) <= 1e-5
