@@ -42,7 +42,7 @@ constexpr int kTapW = kCh * kRow;             // 2 KB per tap of weights
 constexpr int kWBytes = kTapsTC * kTapW;      // 18 KB
 constexpr int kOffA = kWBytes;                // 1 KB aligned
 constexpr int kOffBar = kOffA + 2 * kStageA;  // mbarriers after the buffers
-constexpr size_t kSmemTC = kOffBar + 128 + 1024;  // 7 mbarriers + TMEM slot + alignment slack
+constexpr size_t kSmemTC = kOffBar + 128 + 1024;  // 9 mbarriers + TMEM slot + alignment slack
 constexpr long kWaitLimit = 1L << 24;
 
 __device__ int g_tc_error = 0;
@@ -143,6 +143,16 @@ __device__ __forceinline__ unsigned pack2(float lo, float hi) {
 // accumulator a finished: the epilogue may read it and stage s may be
 // refilled), empty[a] (the 4 epilogue warps finished reading accumulator
 // a), weights.
+// kRows (128-pixel row tiles only): instead of 9 tap tiles, the three input
+// rows y - d, y, y + d are loaded once with a halo of d pixels on each side
+// (box of 128 + 2d pixels), and each tap's A operand is a view starting kx*d
+// rows into its row buffer (the swizzle follows the absolute shared-memory
+// address, as the TMA wrote it; results are bitwise those of the 9-tap
+// form): 3 loads of at most 9 KB per tile instead of 9 of 8 KB, 4 stages in
+// flight, each stage refilled one tile after its MMAs were issued.
+constexpr int kRowBuf = 10 * 1024;  // one staged input row, (128 + 2*8) x 64 B, 1 KB aligned
+
+template <bool kRows>
 __global__ void __launch_bounds__(160, 1)
     k_conv_tc(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap twt,
               const float *__restrict__ bias, __nv_bfloat16 *out, float *out_f32, int H, int W, int TW, int TH,
@@ -151,9 +161,12 @@ __global__ void __launch_bounds__(160, 1)
     unsigned char *sm = reinterpret_cast<unsigned char *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char *ws = sm;
     unsigned char *as = sm + kOffA;
+    // Stages: 2 of 72 KB (9 tap tiles) or 4 of 30 KB (3 staged rows).
+    constexpr int NS = kRows ? 4 : 2;
+    constexpr int SB = kRows ? 3 * kRowBuf : kStageA;
     uint64_t *bars = reinterpret_cast<uint64_t *>(sm + kOffBar);
-    uint64_t *full = bars, *done = bars + 2, *empty = bars + 4, *wbar = bars + 6;
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 7);
+    uint64_t *full = bars, *done = bars + 4, *empty = bars + 6, *wbar = bars + 8;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 9);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tiles_x = W / TW, tiles_y = H / TH;
 
@@ -164,7 +177,7 @@ __global__ void __launch_bounds__(160, 1)
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int k = 0; k < 4; ++k) bar_init(bars + k, 1);
+        for (int k = 0; k < 6; ++k) bar_init(bars + k, 1);  // full[4], done[2]
         bar_init(empty, 4);
         bar_init(empty + 1, 4);
         bar_init(wbar, 1);
@@ -182,11 +195,18 @@ __global__ void __launch_bounds__(160, 1)
                 const int tile = blockIdx.x + it * gridDim.x;
                 const int tx = tile % tiles_x, rest = tile / tiles_x;
                 const int ty = rest % tiles_y, b = rest / tiles_y;
-                const int x0 = tx * TW, y0 = ty * TH, st = it & 1;
-                bar_expect(full + st, kStageA);
-                for (int tap = 0; tap < kTapsTC; ++tap) {
-                    const int dy = (tap / 3 - 1) * dil, dx = (tap % 3 - 1) * dil;
-                    tma_load_4d(as + st * kStageA + tap * kTapA, &tin, full + st, 0, x0 + dx, y0 + dy, b);
+                const int x0 = tx * TW, y0 = ty * TH, st = it % NS;
+                if constexpr (kRows) {
+                    bar_expect(full + st, 3u * (unsigned)(TW + 2 * dil) * kRow);
+                    for (int ky = 0; ky < 3; ++ky)
+                        tma_load_4d(as + st * SB + ky * kRowBuf, &tin, full + st, 0, x0 - dil, y0 + (ky - 1) * dil,
+                                    b);
+                } else {
+                    bar_expect(full + st, kStageA);
+                    for (int tap = 0; tap < kTapsTC; ++tap) {
+                        const int dy = (tap / 3 - 1) * dil, dx = (tap % 3 - 1) * dil;
+                        tma_load_4d(as + st * SB + tap * kTapA, &tin, full + st, 0, x0 + dx, y0 + dy, b);
+                    }
                 }
             };
             // Every load issued here is waited for below (no copy is in
@@ -194,29 +214,39 @@ __global__ void __launch_bounds__(160, 1)
             if (my_tiles > 0) {
                 bar_expect(wbar, kWBytes);
                 tma_load_3d(ws, &twt, wbar, 0, 0, 0);
-                issue(0);
             }
-            if (my_tiles > 1) issue(1);
+            for (int it = 0; it < NS && it < my_tiles; ++it) issue(it);
             if (my_tiles > 0) bar_wait(wbar, 0);
             const unsigned w0 = saddr(ws);
             for (int it = 0; it < my_tiles; ++it) {
-                const int st = it & 1, acc = it & 1;
-                bar_wait(full + st, (unsigned)((it >> 1) & 1));
+                const int st = it % NS, acc = it & 1;
+                bar_wait(full + st, (unsigned)((it / NS) & 1));
                 if (it >= 2) bar_wait(empty + acc, (unsigned)(((it >> 1) - 1) & 1));
                 tc_fence_after();
-                const unsigned a0 = saddr(as + st * kStageA);
+                const unsigned a0 = saddr(as + st * SB);
                 const uint32_t d = tmem + (uint32_t)(acc * kCh);
 #pragma unroll 1
                 for (int tap = 0; tap < kTapsTC; ++tap)
 #pragma unroll
                     for (int k = 0; k < 2; ++k)
-                        mma_f16(d, smem_desc(a0 + tap * kTapA + k * 32), smem_desc(w0 + tap * kTapW + k * 32),
-                                (tap | k) != 0);
+                        mma_f16(d,
+                                smem_desc(kRows ? a0 + (tap / 3) * kRowBuf + (tap % 3) * dil * kRow + k * 32
+                                                : a0 + tap * kTapA + k * 32),
+                                smem_desc(w0 + tap * kTapW + k * 32), (tap | k) != 0);
                 mma_commit(done + acc);
-                if (it + 2 < my_tiles) {
+                if constexpr (NS > 2) {
+                    // Refill the previous tile's stage (its MMAs have most
+                    // likely completed), so this tile's MMAs are not waited
+                    // for here.
+                    const int pv = it - 1;
+                    if (pv >= 0 && pv + NS < my_tiles) {
+                        bar_wait(done + (pv & 1), (unsigned)((pv >> 1) & 1));
+                        issue(pv + NS);
+                    }
+                } else if (it + NS < my_tiles) {
                     // The MMAs have read stage st once they complete.
                     bar_wait(done + acc, (unsigned)((it >> 1) & 1));
-                    issue(it + 2);
+                    issue(it + NS);
                 }
             }
         }
@@ -430,6 +460,16 @@ void tc_note(const char *why) {
     said = true;
 }
 
+// Input rows staged once per tile (the default for 128-pixel row tiles;
+// TRLX_SEEDNET_CONV=tap keeps the 9 tap loads).
+bool rows_mode() {
+    static const bool on = [] {
+        const char *e = std::getenv("TRLX_SEEDNET_CONV");
+        return !(e && e[0] == 't');
+    }();
+    return on;
+}
+
 // Per device (the shared-memory attribute is set on the current device):
 // 0 not tried, 1 usable, -1 not usable.
 constexpr int kMaxDev = 64;
@@ -450,8 +490,10 @@ bool tc_enabled() {
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= kMaxDev) return false;
     if (g_dev_state[dev] == 0) {
-        const cudaError_t err =
-            cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTC);
+        cudaError_t err =
+            cudaFuncSetAttribute(k_conv_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTC);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(k_conv_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTC);
         if (err != cudaSuccess) {
             tc_note(cudaGetErrorString(err));
             cudaGetLastError();
@@ -506,7 +548,20 @@ bool conv_tc(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
     }
     const int ntiles = B * (H / TH) * (W / TW);
     const int grid = ntiles < sms ? ntiles : sms;
-    k_conv_tc<<<grid, 160, kSmemTC>>>(tin, twt, bias, out, out_f32, H, W, TW, TH, dil, relu, ntiles);
+    if (rows_mode() && TW == kTM && dil <= 8) {
+        CUtensorMap trow;
+        const cuuint32_t brow[4] = {(cuuint32_t)kCh, (cuuint32_t)(TW + 2 * dil), 1, 1};
+        if (encoder()(&trow, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(in), din, sin, brow, ones,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS) {
+            k_conv_tc<true><<<grid, 160, kSmemTC>>>(trow, twt, bias, out, out_f32, H, W, TW, TH, dil, relu, ntiles);
+            const cudaError_t e = cudaGetLastError();
+            if (e == cudaSuccess) return true;
+            tc_note(cudaGetErrorString(e));
+            return false;
+        }
+    }
+    k_conv_tc<false><<<grid, 160, kSmemTC>>>(tin, twt, bias, out, out_f32, H, W, TW, TH, dil, relu, ntiles);
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) {  // not launched: the caller's kernel runs instead
         tc_note(cudaGetErrorString(err));
