@@ -671,7 +671,8 @@ def main():
                           f"ned={w['ned']}, maxlan={w['maxlan']}, tol={w['tol']}, "
                           f"{args.format.upper()}, basis fp{args.basis_bits}, one thick-restart cycle/step",
               "global_batch": world, "parallelism": f"replicas x{world}",
-              "l2": "inputs larger than L2 (basis >= 4 GB, CSR >= 1 GB)"}
+              "l2": ("inputs larger than L2 (basis >= 2 GB)" if w["kind"] == "anderson" else
+                     "working set L2-resident (n = 16384: latency-bound, not an HBM measurement)")}
 
     if args.impl == "reference":
         if rank != 0:
