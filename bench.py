@@ -138,20 +138,79 @@ def run_reference_sample(A, w, x0, sample_steps):
     return r["info"].matvec, r["seconds"]
 
 
+BATCHED_SAMPLE = ("reference trlan on {n} problems of the batch spread over the size range, "
+                  "solved one after another (OpenBLAS + OpenMP CSR callback)")
+
+
+def batched_problems(w, rank):
+    """Sizes (L uniform in [48, 256]) and uniform[0, 2] diagonals of the
+    batched configuration's problems."""
+    from nutrlan_b200 import operators as ops
+    Ls = ops.batched_sizes(w["count"], seed=777 + rank)
+    diags = [2.0 * ops.uniform01(1000 + 7919 * rank + k, np.arange(int(L) * int(L), dtype=np.uint64))
+             for k, L in enumerate(Ls)]
+    return Ls, diags
+
+
+def batched_reference_sample(w, Ls, diags, rank, nprob=6):
+    """The reference library on `nprob` problems of the batch spread over
+    the size range, same operators, start vectors and parameters as the
+    batched solver; returns (problems, seconds)."""
+    from nutrlan_b200 import operators as ops
+    from nutrlan_b200.batched import seeded_start
+    from oracle import ref
+    ref.build()
+    t_cpu, n_cpu = 0.0, 0
+    for k in np.linspace(0, len(Ls) - 1, nprob).astype(int):
+        A = ops.laplacian_2d(int(Ls[k]), diag=diags[k])
+        x0 = seeded_start(4242 + rank, int(k), A.n)
+        o = ref.trlan_csr(A, ned=w["ned"], maxlan=w["maxlan"], tol=w["tol"], restart=1,
+                          maxmv=100000, start=x0)
+        t_cpu += o["seconds"]
+        n_cpu += 1
+    return n_cpu, t_cpu
+
+
+def run_batched_reference(args, w, world, rank):
+    """Reference arm of the batched configuration: problems/s of the
+    reference library on a bounded sample of the batch (rank 0 only)."""
+    if rank != 0:
+        return
+    count = w["count"]
+    Ls, diags = batched_problems(w, rank)
+    times, probs = [], []
+    for s in range(args.warmup + args.steps):
+        n_cpu, t_cpu = batched_reference_sample(w, Ls, diags, rank)
+        if s >= args.warmup:
+            times.append(t_cpu)
+            probs.append(n_cpu)
+    val = sum(probs) / sum(times)
+    sample = BATCHED_SAMPLE.format(n=probs[0])
+    print(json.dumps({"impl": "reference",
+                      "metric": f"batched thick-restart Lanczos, {count} problems (smallest {w['ned']} each)",
+                      "value": val, "unit": "problems/s", "n_gpus": world, "steps": args.steps,
+                      "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic (seeded)",
+                      "config": {"workload": f"batched{count}: L~U[48,256], 5-pt Laplacian + U[0,2] diag, "
+                                             f"ned={w['ned']}, maxlan={w['maxlan']}, tol={w['tol']}"},
+                      "cpu_baseline": {"value": val, "unit": "problems/s", "cores": os.cpu_count(),
+                                       "kind": "reference", "sample": sample},
+                      "e2e": {"value": val, "unit": "problems/s", "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}), flush=True)
+
+
 def run_batched(args, w, world, rank, local, pg):
     """Batched configuration: `count` problems, L x L Dirichlet Laplacian +
     uniform[0, 2] diagonal, L uniform in [48, 256]; 8 smallest each,
     maxlan 32, tol 1e-8; one persistent launch per step.  Metric:
     problems solved per second."""
     import torch
-    from nutrlan_b200 import operators as ops
     from nutrlan_b200.batched import Batch
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     count = w["count"]
-    Ls = ops.batched_sizes(count, seed=777 + rank)
-    diags = [2.0 * ops.uniform01(1000 + 7919 * rank + k, np.arange(int(L) * int(L), dtype=np.uint64))
-             for k, L in enumerate(Ls)]
+    Ls, diags = batched_problems(w, rank)
     b = Batch.stencil5(Ls, diags)
     kw = dict(ned=w["ned"], maxlan=w["maxlan"], tol=w["tol"], restart=1, maxmv=100000, seed=4242 + rank)
     t_tune = time.perf_counter()
@@ -183,21 +242,9 @@ def run_batched(args, w, world, rank, local, pg):
     value = count * world * args.steps / dt
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle import ref
-        ref.build()
-        idx = np.linspace(0, count - 1, 6).astype(int)
-        t_cpu, n_cpu = 0.0, 0
-        for k in idx:
-            A = ops.laplacian_2d(int(Ls[k]), diag=diags[k])
-            from nutrlan_b200.batched import seeded_start
-            x0 = seeded_start(4242 + rank, int(k), A.n)
-            o = ref.trlan_csr(A, ned=w["ned"], maxlan=w["maxlan"], tol=w["tol"], restart=1,
-                              maxmv=100000, start=x0)
-            t_cpu += o["seconds"]
-            n_cpu += 1
+        n_cpu, t_cpu = batched_reference_sample(w, Ls, diags, rank)
         cpu = {"value": n_cpu / t_cpu, "unit": "problems/s", "cores": os.cpu_count(), "kind": "reference",
-               "sample": f"reference trlan on {n_cpu} problems of the batch spread over the size range, "
-                         "solved one after another (OpenBLAS + OpenMP CSR callback)"}
+               "sample": BATCHED_SAMPLE.format(n=n_cpu)}
     if rank == 0:
         line = {"metric": f"batched thick-restart Lanczos, {count} problems (smallest {w['ned']} each)",
                 "value": value, "unit": "problems/s", "n_gpus": world, "steps": args.steps,
@@ -659,7 +706,9 @@ def main():
         return
     if w["kind"] == "batched":
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "unavailable": "batched workload: use the default workload"}))
+            run_batched_reference(args, w, world, rank)
+            if pg is not None:
+                pg.destroy_process_group()
             return
         run_batched(args, w, world, rank, local, pg)
         if pg is not None:

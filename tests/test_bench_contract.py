@@ -37,6 +37,9 @@ def test_reference_arm_prints_one_contract_line():
     assert "workload" in line["config"]
 
 
-def test_reference_arm_of_batched_workload_is_unavailable():
+@pytest.mark.skipif(not ref.available(), reason="reference library not built")
+def test_reference_arm_of_batched_workload():
     line = _run("--impl", "reference", "--workload", "batched512", "--steps", "1", "--warmup", "1")
-    assert line["impl"] == "reference" and "unavailable" in line
+    assert line["impl"] == "reference" and line["unit"] == "problems/s" and line["value"] > 0
+    assert line["cpu_baseline"]["value"] == line["value"]
+    assert "6 problems" in line["cpu_baseline"]["sample"]
