@@ -18,6 +18,10 @@
 //     pixels 32w .. 32w+31, 32 channels each), add the bias, apply the ReLU
 //     and store BF16 NHWC (or the first 16 channels as FP32 for the last
 //     layer).
+// That is k_conv_tc, used for images narrower than 128 pixels.  Wider
+// images (W a multiple of 128) use k_conv_rows: the three input rows of a
+// tile loaded once, a producer warp for the loads, and the BF16 output
+// staged in shared memory and written with TMA stores.
 // Every mbarrier wait is bounded; a wait that runs out sets a device flag
 // (read by the seed-network entry points) and the kernel still runs to its
 // end, so the TMEM allocation is always released.
@@ -142,17 +146,8 @@ __device__ __forceinline__ unsigned pack2(float lo, float hi) {
 // Barriers: full[s] (tile loaded into stage s), done[a] (MMAs into
 // accumulator a finished: the epilogue may read it and stage s may be
 // refilled), empty[a] (the 4 epilogue warps finished reading accumulator
-// a), weights.
-// kRows (128-pixel row tiles only): instead of 9 tap tiles, the three input
-// rows y - d, y, y + d are loaded once with a halo of d pixels on each side
-// (box of 128 + 2d pixels), and each tap's A operand is a view starting kx*d
-// rows into its row buffer (the swizzle follows the absolute shared-memory
-// address, as the TMA wrote it; results are bitwise those of the 9-tap
-// form): 3 loads of at most 9 KB per tile instead of 9 of 8 KB, 4 stages in
-// flight, each stage refilled one tile after its MMAs were issued.
-constexpr int kRowBuf = 10 * 1024;  // one staged input row, (128 + 2*8) x 64 B, 1 KB aligned
-
-template <bool kRows>
+// a), weights.  Serves tiles narrower than 128 pixels (W < 128), as 9
+// shifted tap tiles of TW x TH pixels.
 __global__ void __launch_bounds__(160, 1)
     k_conv_tc(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap twt,
               const float *__restrict__ bias, __nv_bfloat16 *out, float *out_f32, int H, int W, int TW, int TH,
@@ -161,9 +156,7 @@ __global__ void __launch_bounds__(160, 1)
     unsigned char *sm = reinterpret_cast<unsigned char *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char *ws = sm;
     unsigned char *as = sm + kOffA;
-    // Stages: 2 of 72 KB (9 tap tiles) or 4 of 30 KB (3 staged rows).
-    constexpr int NS = kRows ? 4 : 2;
-    constexpr int SB = kRows ? 3 * kRowBuf : kStageA;
+    constexpr int NS = 2;  // stages of 72 KB (9 tap tiles)
     uint64_t *bars = reinterpret_cast<uint64_t *>(sm + kOffBar);
     uint64_t *full = bars, *done = bars + 4, *empty = bars + 6, *wbar = bars + 8;
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 9);
@@ -196,17 +189,10 @@ __global__ void __launch_bounds__(160, 1)
                 const int tx = tile % tiles_x, rest = tile / tiles_x;
                 const int ty = rest % tiles_y, b = rest / tiles_y;
                 const int x0 = tx * TW, y0 = ty * TH, st = it % NS;
-                if constexpr (kRows) {
-                    bar_expect(full + st, 3u * (unsigned)(TW + 2 * dil) * kRow);
-                    for (int ky = 0; ky < 3; ++ky)
-                        tma_load_4d(as + st * SB + ky * kRowBuf, &tin, full + st, 0, x0 - dil, y0 + (ky - 1) * dil,
-                                    b);
-                } else {
-                    bar_expect(full + st, kStageA);
-                    for (int tap = 0; tap < kTapsTC; ++tap) {
-                        const int dy = (tap / 3 - 1) * dil, dx = (tap % 3 - 1) * dil;
-                        tma_load_4d(as + st * SB + tap * kTapA, &tin, full + st, 0, x0 + dx, y0 + dy, b);
-                    }
+                bar_expect(full + st, kStageA);
+                for (int tap = 0; tap < kTapsTC; ++tap) {
+                    const int dy = (tap / 3 - 1) * dil, dx = (tap % 3 - 1) * dil;
+                    tma_load_4d(as + st * kStageA + tap * kTapA, &tin, full + st, 0, x0 + dx, y0 + dy, b);
                 }
             };
             // Every load issued here is waited for below (no copy is in
@@ -223,27 +209,16 @@ __global__ void __launch_bounds__(160, 1)
                 bar_wait(full + st, (unsigned)((it / NS) & 1));
                 if (it >= 2) bar_wait(empty + acc, (unsigned)(((it >> 1) - 1) & 1));
                 tc_fence_after();
-                const unsigned a0 = saddr(as + st * SB);
+                const unsigned a0 = saddr(as + st * kStageA);
                 const uint32_t d = tmem + (uint32_t)(acc * kCh);
 #pragma unroll 1
                 for (int tap = 0; tap < kTapsTC; ++tap)
 #pragma unroll
                     for (int k = 0; k < 2; ++k)
-                        mma_f16(d,
-                                smem_desc(kRows ? a0 + (tap / 3) * kRowBuf + (tap % 3) * dil * kRow + k * 32
-                                                : a0 + tap * kTapA + k * 32),
-                                smem_desc(w0 + tap * kTapW + k * 32), (tap | k) != 0);
+                        mma_f16(d, smem_desc(a0 + tap * kTapA + k * 32), smem_desc(w0 + tap * kTapW + k * 32),
+                                (tap | k) != 0);
                 mma_commit(done + acc);
-                if constexpr (NS > 2) {
-                    // Refill the previous tile's stage (its MMAs have most
-                    // likely completed), so this tile's MMAs are not waited
-                    // for here.
-                    const int pv = it - 1;
-                    if (pv >= 0 && pv + NS < my_tiles) {
-                        bar_wait(done + (pv & 1), (unsigned)((pv >> 1) & 1));
-                        issue(pv + NS);
-                    }
-                } else if (it + NS < my_tiles) {
+                if (it + NS < my_tiles) {
                     // The MMAs have read stage st once they complete.
                     bar_wait(done + acc, (unsigned)((it >> 1) & 1));
                     issue(it + NS);
@@ -286,6 +261,176 @@ __global__ void __launch_bounds__(160, 1)
                                       pack2(v[8 * q + 4], v[8 * q + 5]), pack2(v[8 * q + 6], v[8 * q + 7]));
             }
         }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
+}
+
+// Row tiles (W a multiple of 128, dilation <= 8): one tile = 128 pixels of
+// one image row.  Instead of 9 tap tiles, the three input rows y - d, y,
+// y + d are loaded once with a halo of d pixels on each side (box of
+// 128 + 2d pixels), and each tap's A operand is a view starting kx*d rows
+// into its row buffer (the swizzle follows the absolute shared-memory
+// address, as the TMA wrote it; results are bitwise those of the 9-tap
+// form).  Six warps:
+//   * warp 5 (one lane) is the producer: weights once, then the three rows
+//     of each tile into 4 stages, refilling stage s once the MMAs that read
+//     it have completed (free[s], committed by the MMA lane);
+//   * warp 4 (one lane) issues the 18 MMAs of a tile from descriptors
+//     precomputed per tile (the taps are compile-time offsets) and commits
+//     to free[s] and done[a];
+//   * warps 0-3 read accumulator a, add the bias, apply the ReLU, and for
+//     BF16 output write their 32 pixels x 64 B into a shared-memory buffer
+//     in the tensor map's 64-byte swizzle (conflict-free 16-byte stores),
+//     which one lane sends out with a TMA tensor store (two buffers per warp;
+//     a buffer is rewritten once the store from two tiles back has read it).
+//     FP32 output (the last layer) is stored directly.
+// Measured (256 x 256, 32 -> 32 channels, batch 8): 35 us per launch
+// against 48 us for the single-lane form, the 18 MMA issues per tile
+// (M = 128, N = 32) being what is left on the critical path.
+constexpr int kRowBuf = 10 * 1024;                   // one staged input row, (128 + 2*8) x 64 B, 1 KB aligned
+constexpr int kRowStages = 4;
+constexpr int kOffRowA = kWBytes;                     // 4 stages x 3 rows
+constexpr int kOffRowO = kOffRowA + kRowStages * 3 * kRowBuf;  // 4 warps x 2 output buffers of 2 KB
+constexpr int kOffRowBar = kOffRowO + 8 * 2048;
+constexpr size_t kSmemRows = kOffRowBar + 128 + 1024;  // 13 mbarriers + TMEM slot + alignment slack
+
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, const void *src, int c0, int c1, int c2, int c3) {
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%2, %3, %4, %5}], [%1];" ::"l"(map),
+                 "r"(saddr(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(192, 1)
+    k_conv_rows(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap twt,
+                const __grid_constant__ CUtensorMap tout, const float *__restrict__ bias, float *out_f32, int H,
+                int W, int dil, int relu, int ntiles) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *sm = reinterpret_cast<unsigned char *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char *ws = sm;
+    unsigned char *as = sm + kOffRowA;
+    unsigned char *os = sm + kOffRowO;
+    constexpr int NS = kRowStages;
+    constexpr int SB = 3 * kRowBuf;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + kOffRowBar);
+    uint64_t *full = bars, *freeb = bars + 4, *done = bars + 8, *empty = bars + 10, *wbar = bars + 12;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 13);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tiles_x = W / kTM;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tslot)),
+                     "r"(64)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int k = 0; k < 10; ++k) bar_init(bars + k, 1);  // full[4], free[4], done[2]
+        bar_init(empty, 4);
+        bar_init(empty + 1, 4);
+        bar_init(wbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const int my_tiles = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    if (warp == 5) {
+        // Every load issued here is waited for by the MMA lane (full[s]), so
+        // no copy is in flight when the CTA exits.
+        if (lane == 0 && my_tiles > 0) {
+            bar_expect(wbar, kWBytes);
+            tma_load_3d(ws, &twt, wbar, 0, 0, 0);
+            int tile = blockIdx.x;
+            for (int it = 0; it < my_tiles; ++it, tile += gridDim.x) {
+                const int st = it % NS;
+                const int tx = tile % tiles_x, rest = tile / tiles_x;
+                const int y = rest % H, b = rest / H;
+                if (it >= NS) bar_wait(freeb + st, (unsigned)(((it / NS) - 1) & 1));
+                bar_expect(full + st, 3u * (unsigned)(kTM + 2 * dil) * kRow);
+                for (int ky = 0; ky < 3; ++ky)
+                    tma_load_4d(as + st * SB + ky * kRowBuf, &tin, full + st, 0, tx * kTM - dil, y + (ky - 1) * dil,
+                                b);
+            }
+        }
+    } else if (warp == 4) {
+        if (lane == 0 && my_tiles > 0) {
+            bar_wait(wbar, 0);
+            const uint64_t dB = smem_desc(saddr(ws));
+            const uint32_t d4 = (uint32_t)dil * (kRow >> 4);  // one pixel shift in 16-byte units
+            for (int it = 0; it < my_tiles; ++it) {
+                const int st = it % NS, acc = it & 1;
+                bar_wait(full + st, (unsigned)((it / NS) & 1));
+                if (it >= 2) bar_wait(empty + acc, (unsigned)(((it >> 1) - 1) & 1));
+                tc_fence_after();
+                // Descriptor start addresses stay below 2^14 x 16 B (shared
+                // memory), so adding offsets never carries out of the field.
+                const uint64_t dA = smem_desc(saddr(as + st * SB));
+                const uint32_t d = tmem + (uint32_t)(acc * kCh);
+#pragma unroll
+                for (int tap = 0; tap < kTapsTC; ++tap)
+#pragma unroll
+                    for (int k = 0; k < 2; ++k)
+                        mma_f16(d, dA + (uint64_t)((tap / 3) * (kRowBuf >> 4) + (tap % 3) * d4 + k * 2),
+                                dB + (uint64_t)((tap * kTapW + k * 32) >> 4), (tap | k) != 0);
+                mma_commit(freeb + st);
+                mma_commit(done + acc);
+            }
+        }
+    } else {
+        float bv[kCh];
+#pragma unroll
+        for (int c = 0; c < kCh; ++c) bv[c] = bias ? bias[c] : 0.f;
+        int tile = blockIdx.x;
+        for (int it = 0; it < my_tiles; ++it, tile += gridDim.x) {
+            const int acc = it & 1;
+            bar_wait(done + acc, (unsigned)((it >> 1) & 1));
+            tc_fence_after();
+            uint32_t r[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(acc * kCh), r);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(empty + acc)) : "memory");
+            const int tx = tile % tiles_x, rest = tile / tiles_x;
+            const int y = rest % H, b = rest / H;
+            float v[kCh];
+#pragma unroll
+            for (int c = 0; c < kCh; ++c) {
+                v[c] = __uint_as_float(r[c]) + bv[c];
+                if (relu) v[c] = fmaxf(v[c], 0.f);
+            }
+            if (out_f32) {
+                const long p = ((long)b * H + y) * W + tx * kTM + warp * 32 + lane;
+                float4 *o = reinterpret_cast<float4 *>(out_f32 + p * 16);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            } else {
+                unsigned char *ob = os + (warp * 2 + acc) * 2048;
+                if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                __syncwarp();
+                // 16-byte chunk q of pixel l at l*64 + 16*(q ^ ((l >> 1) & 3)):
+                // the 64-byte swizzle of the output tensor map.
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    *reinterpret_cast<uint4 *>(ob + lane * 64 + ((q ^ ((lane >> 1) & 3)) << 4)) =
+                        make_uint4(pack2(v[8 * q], v[8 * q + 1]), pack2(v[8 * q + 2], v[8 * q + 3]),
+                                   pack2(v[8 * q + 4], v[8 * q + 5]), pack2(v[8 * q + 6], v[8 * q + 7]));
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) {
+                    tma_store_4d(&tout, ob, 0, tx * kTM + warp * 32, y, b);
+                    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                }
+            }
+        }
+        // The stores have finished before the CTA exits.
+        if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+        __syncwarp();
     }
     tc_fence_before();
     __syncthreads();
@@ -491,9 +636,9 @@ bool tc_enabled() {
     if (dev < 0 || dev >= kMaxDev) return false;
     if (g_dev_state[dev] == 0) {
         cudaError_t err =
-            cudaFuncSetAttribute(k_conv_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTC);
+            cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTC);
         if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(k_conv_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTC);
+            err = cudaFuncSetAttribute(k_conv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemRows);
         if (err != cudaSuccess) {
             tc_note(cudaGetErrorString(err));
             cudaGetLastError();
@@ -548,20 +693,27 @@ bool conv_tc(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
     }
     const int ntiles = B * (H / TH) * (W / TW);
     const int grid = ntiles < sms ? ntiles : sms;
-    if (rows_mode() && TW == kTM && dil <= 8) {
-        CUtensorMap trow;
+    if (rows_mode() && TW == kTM && dil >= 1 && dil <= 8 && (out_f32 || !((uintptr_t)out & 15))) {
+        CUtensorMap trow, tout;
         const cuuint32_t brow[4] = {(cuuint32_t)kCh, (cuuint32_t)(TW + 2 * dil), 1, 1};
+        const cuuint32_t bout[4] = {(cuuint32_t)kCh, 32, 1, 1};  // one warp's 32 pixels
+        // The output map is only used for BF16 output (same NHWC shape as the
+        // input); for FP32 output it is encoded over the input and not used.
+        void *obase = out_f32 ? const_cast<__nv_bfloat16 *>(in) : static_cast<void *>(out);
         if (encoder()(&trow, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(in), din, sin, brow, ones,
                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+            encoder()(&tout, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, obase, din, sin, bout, ones,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS) {
-            k_conv_tc<true><<<grid, 160, kSmemTC>>>(trow, twt, bias, out, out_f32, H, W, TW, TH, dil, relu, ntiles);
+            k_conv_rows<<<grid, 192, kSmemRows>>>(trow, twt, tout, bias, out_f32, H, W, dil, relu, ntiles);
             const cudaError_t e = cudaGetLastError();
             if (e == cudaSuccess) return true;
             tc_note(cudaGetErrorString(e));
             return false;
         }
     }
-    k_conv_tc<false><<<grid, 160, kSmemTC>>>(tin, twt, bias, out, out_f32, H, W, TW, TH, dil, relu, ntiles);
+    k_conv_tc<<<grid, 160, kSmemTC>>>(tin, twt, bias, out, out_f32, H, W, TW, TH, dil, relu, ntiles);
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) {  // not launched: the caller's kernel runs instead
         tc_note(cudaGetErrorString(err));
