@@ -275,28 +275,42 @@ __global__ void __launch_bounds__(160, 1)
 // 128 + 2d pixels), and each tap's A operand is a view starting kx*d rows
 // into its row buffer (the swizzle follows the absolute shared-memory
 // address, as the TMA wrote it; results are bitwise those of the 9-tap
-// form).  Six warps:
-//   * warp 5 (one lane) is the producer: weights once, then the three rows
-//     of each tile into 4 stages, refilling stage s once the MMAs that read
-//     it have completed (free[s], committed by the MMA lane);
-//   * warp 4 (one lane) issues the 18 MMAs of a tile from descriptors
-//     precomputed per tile (the taps are compile-time offsets) and commits
-//     to free[s] and done[a];
-//   * warps 0-3 read accumulator a, add the bias, apply the ReLU, and for
-//     BF16 output write their 32 pixels x 64 B into a shared-memory buffer
-//     in the tensor map's 64-byte swizzle (conflict-free 16-byte stores),
-//     which one lane sends out with a TMA tensor store (two buffers per warp;
-//     a buffer is rewritten once the store from two tiles back has read it).
-//     FP32 output (the last layer) is stored directly.
-// Measured (256 x 256, 32 -> 32 channels, batch 8): 35 us per launch
-// against 48 us for the single-lane form, the 18 MMA issues per tile
-// (M = 128, N = 32) being what is left on the critical path.
-constexpr int kRowBuf = 10 * 1024;                   // one staged input row, (128 + 2*8) x 64 B, 1 KB aligned
-constexpr int kRowStages = 4;
-constexpr int kOffRowA = kWBytes;                     // 4 stages x 3 rows
-constexpr int kOffRowO = kOffRowA + kRowStages * 3 * kRowBuf;  // 4 warps x 2 output buffers of 2 KB
-constexpr int kOffRowBar = kOffRowO + 8 * 2048;
-constexpr size_t kSmemRows = kOffRowBar + 128 + 1024;  // 13 mbarriers + TMEM slot + alignment slack
+// form).  Warp roles (kEpi epilogue warpgroups, kLanes MMA lanes):
+//   * warps 0 .. 4*kEpi-1 run the epilogue, warpgroup g taking the tiles
+//     it = g (mod kEpi): read accumulator it % kAcc, add the bias, apply
+//     the ReLU, and for BF16 output write their 32 pixels x 64 B into a
+//     shared-memory buffer in the output tensor map's 64-byte swizzle
+//     (conflict-free 16-byte stores), which one lane sends out with a TMA
+//     tensor store (two buffers per warp; a buffer is rewritten once the
+//     store from two tiles back has read it).  FP32 output (the last
+//     layer) is stored directly;
+//   * warp 4*kEpi (one lane) is the producer: weights once, then the three
+//     rows of each tile into kStages stages, refilling stage s once the
+//     MMAs that read it have completed (free[s]);
+//   * the next kLanes warps (one lane each) issue the MMAs, lane m taking
+//     the tiles it = m (mod kLanes): 18 tcgen05.mma from descriptors
+//     precomputed per tile (the taps are compile-time offsets), committed
+//     to free[s] and done[a].
+// Measured (256 x 256, 32 -> 32 channels, batch 8, clock stamps per tile):
+// one lane spends about 71 cycles per M = 128, N = 32, K = 16 MMA issue, 18
+// per tile, while the tensor pipe is mostly idle; two lanes issuing for
+// alternate tiles take the layer from 35 to 23 us, bitwise equal.
+constexpr int kRowBuf = 9 * 1024;  // one staged input row, (128 + 2*8) x 64 B, 1 KB aligned
+
+template <int kLanes, int kEpi, int kStages>
+struct RowCfg {
+    static constexpr int kAcc = 2 * kLanes;  // TMEM accumulators of 32 columns
+    static_assert(kAcc % kEpi == 0, "an accumulator belongs to one epilogue warpgroup");
+    static constexpr int kThreads = 32 * (4 * kEpi + 1 + kLanes);
+    static constexpr int kCols = kAcc * kCh;
+    static_assert(kCols >= 32 && kCols <= 512 && (kCols & (kCols - 1)) == 0, "TMEM allocations are powers of two");
+    static constexpr int kOffA = kWBytes;
+    static constexpr int kOffO = kOffA + kStages * 3 * kRowBuf;  // 4*kEpi warps x 2 buffers of 2 KB
+    static constexpr int kOffBar = kOffO + 4 * kEpi * 2 * 2048;
+    static constexpr int kBars = 2 * kStages + 2 * kAcc + 1;
+    static_assert(kBars * 8 + 4 <= 256, "mbarriers and the TMEM slot fit in 256 bytes");
+    static constexpr size_t kSmem = kOffBar + 256 + 1024;  // + alignment slack
+};
 
 __device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, const void *src, int c0, int c1, int c2, int c3) {
     asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%2, %3, %4, %5}], [%1];" ::"l"(map),
@@ -304,33 +318,35 @@ __device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, const void 
                  : "memory");
 }
 
-__global__ void __launch_bounds__(192, 1)
+template <int kLanes, int kEpi, int kStages>
+__global__ void __launch_bounds__(RowCfg<kLanes, kEpi, kStages>::kThreads, 1)
     k_conv_rows(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap twt,
                 const __grid_constant__ CUtensorMap tout, const float *__restrict__ bias, float *out_f32, int H,
                 int W, int dil, int relu, int ntiles) {
+    using Cfg = RowCfg<kLanes, kEpi, kStages>;
+    constexpr int NS = kStages, NA = Cfg::kAcc;
+    constexpr int SB = 3 * kRowBuf;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *sm = reinterpret_cast<unsigned char *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char *ws = sm;
-    unsigned char *as = sm + kOffRowA;
-    unsigned char *os = sm + kOffRowO;
-    constexpr int NS = kRowStages;
-    constexpr int SB = 3 * kRowBuf;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + kOffRowBar);
-    uint64_t *full = bars, *freeb = bars + 4, *done = bars + 8, *empty = bars + 10, *wbar = bars + 12;
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 13);
+    unsigned char *as = sm + Cfg::kOffA;
+    unsigned char *os = sm + Cfg::kOffO;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + Cfg::kOffBar);
+    uint64_t *full = bars, *freeb = bars + NS, *done = bars + 2 * NS, *empty = bars + 2 * NS + NA;
+    uint64_t *wbar = bars + 2 * NS + 2 * NA;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + Cfg::kBars);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tiles_x = W / kTM;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tslot)),
-                     "r"(64)
+                     "r"(Cfg::kCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int k = 0; k < 10; ++k) bar_init(bars + k, 1);  // full[4], free[4], done[2]
-        bar_init(empty, 4);
-        bar_init(empty + 1, 4);
+        for (int k = 0; k < 2 * NS + NA; ++k) bar_init(bars + k, 1);  // full, free, done
+        for (int k = 0; k < NA; ++k) bar_init(empty + k, 4);          // the 4 warps of a warpgroup
         bar_init(wbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -340,8 +356,8 @@ __global__ void __launch_bounds__(192, 1)
     const uint32_t tmem = *tslot;
     const int my_tiles = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
 
-    if (warp == 5) {
-        // Every load issued here is waited for by the MMA lane (full[s]), so
+    if (warp == 4 * kEpi) {
+        // Every load issued here is waited for by an MMA lane (full[s]), so
         // no copy is in flight when the CTA exits.
         if (lane == 0 && my_tiles > 0) {
             bar_expect(wbar, kWBytes);
@@ -358,15 +374,16 @@ __global__ void __launch_bounds__(192, 1)
                                 b);
             }
         }
-    } else if (warp == 4) {
-        if (lane == 0 && my_tiles > 0) {
+    } else if (warp > 4 * kEpi) {
+        const int m = warp - 4 * kEpi - 1;  // MMA lane
+        if (lane == 0 && m < my_tiles) {
             bar_wait(wbar, 0);
             const uint64_t dB = smem_desc(saddr(ws));
             const uint32_t d4 = (uint32_t)dil * (kRow >> 4);  // one pixel shift in 16-byte units
-            for (int it = 0; it < my_tiles; ++it) {
-                const int st = it % NS, acc = it & 1;
+            for (int it = m; it < my_tiles; it += kLanes) {
+                const int st = it % NS, acc = it % NA;
                 bar_wait(full + st, (unsigned)((it / NS) & 1));
-                if (it >= 2) bar_wait(empty + acc, (unsigned)(((it >> 1) - 1) & 1));
+                if (it >= NA) bar_wait(empty + acc, (unsigned)(((it / NA) - 1) & 1));
                 tc_fence_after();
                 // Descriptor start addresses stay below 2^14 x 16 B (shared
                 // memory), so adding offsets never carries out of the field.
@@ -383,16 +400,18 @@ __global__ void __launch_bounds__(192, 1)
             }
         }
     } else {
+        const int g = warp >> 2, quarter = warp & 3;  // epilogue warpgroup, TMEM lane quarter
         float bv[kCh];
 #pragma unroll
         for (int c = 0; c < kCh; ++c) bv[c] = bias ? bias[c] : 0.f;
-        int tile = blockIdx.x;
-        for (int it = 0; it < my_tiles; ++it, tile += gridDim.x) {
-            const int acc = it & 1;
-            bar_wait(done + acc, (unsigned)((it >> 1) & 1));
+        int nb = 0;  // this warp's tiles so far (output buffer parity)
+        for (int it = g; it < my_tiles; it += kEpi, ++nb) {
+            const int acc = it % NA;
+            const int tile = blockIdx.x + it * gridDim.x;
+            bar_wait(done + acc, (unsigned)((it / NA) & 1));
             tc_fence_after();
             uint32_t r[32];
-            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(acc * kCh), r);
+            tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kCh), r);
             tc_fence_before();
             __syncwarp();
             if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(empty + acc)) : "memory");
@@ -405,12 +424,12 @@ __global__ void __launch_bounds__(192, 1)
                 if (relu) v[c] = fmaxf(v[c], 0.f);
             }
             if (out_f32) {
-                const long p = ((long)b * H + y) * W + tx * kTM + warp * 32 + lane;
+                const long p = ((long)b * H + y) * W + tx * kTM + quarter * 32 + lane;
                 float4 *o = reinterpret_cast<float4 *>(out_f32 + p * 16);
 #pragma unroll
                 for (int q = 0; q < 4; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
             } else {
-                unsigned char *ob = os + (warp * 2 + acc) * 2048;
+                unsigned char *ob = os + (warp * 2 + (nb & 1)) * 2048;
                 if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
                 __syncwarp();
                 // 16-byte chunk q of pixel l at l*64 + 16*(q ^ ((l >> 1) & 3)):
@@ -423,7 +442,7 @@ __global__ void __launch_bounds__(192, 1)
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncwarp();
                 if (lane == 0) {
-                    tma_store_4d(&tout, ob, 0, tx * kTM + warp * 32, y, b);
+                    tma_store_4d(&tout, ob, 0, tx * kTM + quarter * 32, y, b);
                     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                 }
             }
@@ -436,8 +455,13 @@ __global__ void __launch_bounds__(192, 1)
     __syncthreads();
     tc_fence_after();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::kCols) : "memory");
 }
+
+// The configuration the library launches: two MMA lanes, one epilogue
+// warpgroup, four stages.
+using RowsCfg = RowCfg<2, 1, 4>;
+constexpr auto *kRowsKernel = &k_conv_rows<2, 1, 4>;
 
 // ---------------------------------------------------------------------------
 // Weight gradient on tcgen05: dW[tap][ci][co] = sum_p in[p + off(tap)][ci] *
@@ -638,7 +662,8 @@ bool tc_enabled() {
         cudaError_t err =
             cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTC);
         if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(k_conv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemRows);
+            err = cudaFuncSetAttribute(kRowsKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)RowsCfg::kSmem);
         if (err != cudaSuccess) {
             tc_note(cudaGetErrorString(err));
             cudaGetLastError();
@@ -706,7 +731,8 @@ bool conv_tc(const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
             encoder()(&tout, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, obase, din, sin, bout, ones,
                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS) {
-            k_conv_rows<<<grid, 192, kSmemRows>>>(trow, twt, tout, bias, out_f32, H, W, dil, relu, ntiles);
+            kRowsKernel<<<grid, RowsCfg::kThreads, RowsCfg::kSmem>>>(trow, twt, tout, bias, out_f32, H, W, dil,
+                                                                          relu, ntiles);
             const cudaError_t e = cudaGetLastError();
             if (e == cudaSuccess) return true;
             tc_note(cudaGetErrorString(e));
