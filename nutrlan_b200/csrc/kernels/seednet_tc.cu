@@ -293,8 +293,8 @@ __global__ void __launch_bounds__(160, 1)
 //     to free[s] and done[a].
 // Measured (256 x 256, 32 -> 32 channels, batch 8, clock stamps per tile):
 // one lane spends about 71 cycles per M = 128, N = 32, K = 16 MMA issue, 18
-// per tile, while the tensor pipe is mostly idle; two lanes issuing for
-// alternate tiles take the layer from 35 to 23 us, bitwise equal.
+// per tile, while the tensor pipe is mostly idle, so several lanes issue
+// for different tiles.
 constexpr int kRowBuf = 9 * 1024;  // one staged input row, (128 + 2*8) x 64 B, 1 KB aligned
 
 template <int kLanes, int kEpi, int kStages>
@@ -458,10 +458,13 @@ __global__ void __launch_bounds__(RowCfg<kLanes, kEpi, kStages>::kThreads, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::kCols) : "memory");
 }
 
-// The configuration the library launches: two MMA lanes, one epilogue
-// warpgroup, four stages.
-using RowsCfg = RowCfg<2, 1, 4>;
-constexpr auto *kRowsKernel = &k_conv_rows<2, 1, 4>;
+// The configuration the library launches: four MMA lanes, two epilogue
+// warpgroups, six stages (213 KB of shared memory, 416 threads).  Measured
+// per 32 -> 32 layer at 256 x 256, batch 16: 1 lane 66 us, 2 lanes 41 us,
+// 4 lanes with one epilogue warpgroup 41 us (the epilogue bound), 4 lanes
+// with two 37 us; every configuration bitwise equal to the 9-tap kernel.
+using RowsCfg = RowCfg<4, 2, 6>;
+constexpr auto *kRowsKernel = &k_conv_rows<4, 2, 6>;
 
 // ---------------------------------------------------------------------------
 // Weight gradient on tcgen05: dW[tap][ci][co] = sum_p in[p + off(tap)][ci] *
