@@ -607,6 +607,148 @@ __global__ void __launch_bounds__(160, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128) : "memory");
 }
 
+// Weight gradient with the input rows staged once per segment: a stage holds
+// the three input rows y - d, y, y + d of a 64-pixel segment with a halo of
+// d pixels (64 + 2d pixels each, zero fill outside the image), a row of
+// ones and the g tile.  Accumulator group kx (M = 128 = 4 atoms of 32 ci)
+// is one descriptor whose M atoms are the three rows at pixel shift kx*d
+// (taps (0, kx), (1, kx), (2, kx)) and the ones row (the leading byte
+// offset is the row-buffer stride), so the K shift runs along the pixels of
+// an MN-major operand, read at the absolute swizzled addresses the TMA
+// wrote.  Group 0's ones atom gives db; the ones atoms of groups 1 and 2
+// compute the same sums and are not written.  Loads per segment: 3 rows of
+// at most 5 KB and a 4 KB g tile, against 9 + 1 tiles of 4 KB.
+// Warps 0-3 read the accumulators, warp 4 (one lane) is the producer, and
+// kLanes warps (one lane each) issue the MMAs for alternate segments into
+// private accumulators (3 x 32 columns each), which the epilogue adds in
+// lane order.
+constexpr int kWRowBuf = 5 * 1024;                       // (64 + 2*8) px x 64 B, 1 KB aligned
+constexpr int kWRowStage = 4 * kWRowBuf + kWSlot;        // 3 rows, ones, g: 24 KB
+constexpr int kWRowStages = 6;
+constexpr int kWRowLanes = 2;
+constexpr int kWRowOffBar = kWRowStages * kWRowStage;
+constexpr int kWRowThreads = 32 * (5 + kWRowLanes);
+constexpr size_t kSmemWR = kWRowOffBar + 128 + 1024;
+
+__device__ __forceinline__ uint64_t smem_desc_mn_rows(unsigned addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);               // start address
+    d |= (uint64_t)((kWRowBuf >> 4) & 0x3FFF) << 16;     // leading byte offset: next row buffer (M atom)
+    d |= (uint64_t)((512 >> 4) & 0x3FFF) << 32;          // stride byte offset: next 8 pixels of K
+    d |= (uint64_t)1 << 46;                              // version
+    d |= (uint64_t)4 << 61;                              // SWIZZLE_64B
+    return d;
+}
+
+__global__ void __launch_bounds__(kWRowThreads, 1)
+    k_wgrad_rows(const __grid_constant__ CUtensorMap trow, const __grid_constant__ CUtensorMap tg, float *part,
+                 int H, int W, int dil, int nseg) {
+    constexpr int NS = kWRowStages;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *sm = reinterpret_cast<unsigned char *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + kWRowOffBar);
+    uint64_t *full = bars, *freeb = bars + NS, *fin = bars + 2 * NS;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2 * NS + kWRowLanes);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int segs_x = W / kWSeg;
+    const int my = (int)blockIdx.x < nseg ? (nseg - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    // The ones row of every stage (bf16 1.0 pairs).
+    for (int st = 0; st < NS; ++st) {
+        uint4 *o = reinterpret_cast<uint4 *>(sm + st * kWRowStage + 3 * kWRowBuf);
+        for (int i = tid; i < kWRowBuf / 16; i += blockDim.x)
+            o[i] = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tslot)),
+                     "r"(256)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int k = 0; k < 2 * NS + kWRowLanes; ++k) bar_init(bars + k, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (warp == 4) {
+        // Every load issued here is waited for by an MMA lane (full[s]).
+        if (lane == 0) {
+            int seg = blockIdx.x;
+            for (int it = 0; it < my; ++it, seg += gridDim.x) {
+                const int st = it % NS;
+                const int sx = seg % segs_x, rest = seg / segs_x;
+                const int y = rest % H, b = rest / H, x0 = sx * kWSeg;
+                unsigned char *base = sm + st * kWRowStage;
+                if (it >= NS) bar_wait(freeb + st, (unsigned)(((it / NS) - 1) & 1));
+                bar_expect(full + st, 3u * (unsigned)(kWSeg + 2 * dil) * kRow + kWSlot);
+                for (int ky = 0; ky < 3; ++ky)
+                    tma_load_4d(base + ky * kWRowBuf, &trow, full + st, 0, x0 - dil, y + (ky - 1) * dil, b);
+                tma_load_4d(base + 4 * kWRowBuf, &tg, full + st, 0, x0, y, b);
+            }
+        }
+    } else if (warp >= 5) {
+        const int m = warp - 5;  // MMA lane
+        if (lane == 0 && m < my) {
+            const uint32_t d0 = tmem + (uint32_t)(m * 128);
+            const unsigned shift = (unsigned)dil * kRow;  // bytes per pixel shift
+            for (int it = m; it < my; it += kWRowLanes) {
+                const int st = it % NS;
+                bar_wait(full + st, (unsigned)((it / NS) & 1));
+                tc_fence_after();
+                const unsigned a0 = saddr(sm + st * kWRowStage), b0 = a0 + 4 * kWRowBuf;
+#pragma unroll
+                for (int kx = 0; kx < 3; ++kx)
+#pragma unroll
+                    for (int k = 0; k < kWSeg / 16; ++k)
+                        mma_f16_mn(d0 + (uint32_t)(kx * kCh), smem_desc_mn_rows(a0 + kx * shift + k * 1024),
+                                   smem_desc_mn(b0 + k * 1024), (it != m || k != 0) ? 1u : 0u);
+                mma_commit(freeb + st);
+            }
+            mma_commit(fin + m);
+        }
+    } else if (my > 0) {
+        const int lanes = my < kWRowLanes ? my : kWRowLanes;  // lanes that accumulated
+        for (int m = 0; m < lanes; ++m) bar_wait(fin + m, 0);
+        tc_fence_after();
+        float *pb = part + (size_t)blockIdx.x * (kTapsTC + 1) * kCh * kCh;
+#pragma unroll 1
+        for (int kx = 0; kx < 3; ++kx) {
+            if (warp == 3 && kx > 0) continue;  // ones atoms of groups 1, 2: not used
+            float v[32];
+            {
+                uint32_t r[32];
+                tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(kx * kCh), r);
+#pragma unroll
+                for (int c = 0; c < 32; ++c) v[c] = __uint_as_float(r[c]);
+            }
+            for (int m = 1; m < lanes; ++m) {
+                uint32_t r[32];
+                tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(m * 128 + kx * kCh), r);
+#pragma unroll
+                for (int c = 0; c < 32; ++c) v[c] += __uint_as_float(r[c]);
+            }
+            float *row = nullptr;
+            if (warp < 3) row = pb + ((size_t)(warp * 3 + kx) * kCh + lane) * kCh;  // tap (ky = warp, kx), ci = lane
+            else if (lane == 0) row = pb + (size_t)kTapsTC * kCh * kCh;             // db
+            if (row) {
+                float4 *o = reinterpret_cast<float4 *>(row);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+}
+
 using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -762,8 +904,9 @@ int wgrad_tc(const __nv_bfloat16 *in, const __nv_bfloat16 *g, float *part, int m
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= kMaxDev) return 0;
     if (wg_ok[dev] == 0) {
-        const cudaError_t e =
-            cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemWG);
+        cudaError_t e = cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemWG);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_wgrad_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemWR);
         if (e != cudaSuccess) {
             tc_note(cudaGetErrorString(e));
             cudaGetLastError();
@@ -793,6 +936,20 @@ int wgrad_tc(const __nv_bfloat16 *in, const __nv_bfloat16 *g, float *part, int m
     int grid = nseg < sms ? nseg : sms;
     if (grid > max_blocks) grid = max_blocks;
     if (grid < 1) return 0;
+    if (rows_mode() && dil >= 1 && dil <= 8) {
+        // Three staged rows per segment (box of 64 + 2d pixels).
+        CUtensorMap trow;
+        const cuuint32_t brow[4] = {(cuuint32_t)kCh, (cuuint32_t)(kWSeg + 2 * dil), 1, 1};
+        if (encoder()(&trow, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(in), dims, strides,
+                      brow, ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS) {
+            k_wgrad_rows<<<grid, kWRowThreads, kSmemWR>>>(trow, tgm, part, H, W, dil, nseg);
+            const cudaError_t e = cudaGetLastError();
+            if (e == cudaSuccess) return grid;
+            tc_note(cudaGetErrorString(e));
+            return 0;
+        }
+    }
     k_wgrad_tc<<<grid, 160, kSmemWG>>>(tin, tgm, part, H, W, dil, nseg);
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) {
