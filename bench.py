@@ -476,22 +476,66 @@ def learned_seed_ab(problems, seed0=10 ** 6, log=None):
     return out
 
 
+def wells_reference_sample(seed0, count=2):
+    """The reference library's plain solves of `count` held-out well
+    operators (same operators, start vector and parameters as the plain arm
+    of the A/B test); returns (solves, seconds, matvecs)."""
+    from oracle import ref
+    from nutrlan_b200 import operators as ops
+    ref.build()
+    t_cpu, n_cpu, mv = 0.0, 0, 0
+    for s_ in range(seed0, seed0 + count):
+        A, _ = ops.wells_2d(256, seed=s_)
+        o = ref.trlan_csr(A, ned=16, maxlan=48, tol=1e-8, restart=1, maxmv=100000,
+                          start=ops.start_vector(A.n))
+        t_cpu += o["seconds"]
+        n_cpu += 1
+        mv += o["info"].matvec
+    return n_cpu, t_cpu, mv
+
+
+WELLS_METRIC = "learned-seed solves/s to residual <= 1e-8 (Gaussian wells 256x256, smallest 16)"
+WELLS_WORKLOAD = ("wells256: n=65536, 8 Gaussian wells, ned=16, maxlan=48, tol=1e-8, "
+                  "CSR, seed = sum of network outputs (guess=1)")
+
+
 def run_wells(args, w, world, rank, local, pg):
     """Learned-seed configuration: time to residual <= 1e-8 on held-out
     Gaussian-well operators, seeded by the packaged network (start vector =
     sum of its normalised outputs) against the plain solve.  Metric: seeded
-    solves per second (whole job); the plain rate and matvec counts beside it."""
+    solves per second (whole job); the plain rate and matvec counts beside it.
+    The reference arm times the reference's plain solves of the same held-out
+    operators (the learned seed has no counterpart there), rank 0 only."""
+    seed0 = 10 ** 6 + 1000 * rank
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        times, solves, mvs = [], [], []
+        for s in range(args.warmup + args.steps):
+            n_cpu, t_cpu, mv = wells_reference_sample(seed0)
+            if s >= args.warmup:
+                times.append(t_cpu)
+                solves.append(n_cpu)
+                mvs.append(mv)
+        val = sum(solves) / sum(times)
+        sample = (f"reference trlan, plain solves of {solves[0]} of the held-out operators per step "
+                  f"({sum(mvs) / sum(solves):.0f} matvecs each), OpenBLAS + OpenMP CSR callback")
+        print(json.dumps({"impl": "reference", "metric": WELLS_METRIC, "value": val, "unit": "solves/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic (seeded well potentials, held-out seeds)",
+                          "config": {"workload": WELLS_WORKLOAD, "parallelism": f"replicas x{world}",
+                                     "reference": "plain solve (no learned seed), start vector uniform[-1,1]"},
+                          "cpu_baseline": {"value": val, "unit": "solves/s", "cores": os.cpu_count(),
+                                           "kind": "reference", "sample": sample},
+                          "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
     import torch
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if args.impl == "reference":
-        if rank == 0:
-            print(json.dumps({"impl": "reference",
-                              "unavailable": "the learned seed has no counterpart in the reference; "
-                                             "its CPU baseline is the plain reference solve in cpu_baseline"}))
-        return
     n_prob = w["problems"]
-    seed0 = 10 ** 6 + 1000 * rank
     learned_seed_ab(2, seed0=seed0 + 500)  # warm-up (workspace, library, network)
     for _ in range(max(args.warmup - 1, 0)):
         learned_seed_ab(1, seed0=seed0 + 600)
@@ -505,29 +549,18 @@ def run_wells(args, w, world, rank, local, pg):
     seeded_s = reduce_max(pg, ab["sum_s"], dev)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle import ref
-        from nutrlan_b200 import operators as ops
-        ref.build()
-        t_cpu, n_cpu, mv = 0.0, 0, 0
-        for s_ in range(seed0, seed0 + 2):
-            A, _ = ops.wells_2d(256, seed=s_)
-            o = ref.trlan_csr(A, ned=16, maxlan=48, tol=1e-8, restart=1, maxmv=100000,
-                              start=ops.start_vector(A.n))
-            t_cpu += o["seconds"]
-            n_cpu += 1
-            mv += o["info"].matvec
+        n_cpu, t_cpu, mv = wells_reference_sample(seed0)
         cpu = {"value": n_cpu / t_cpu, "unit": "solves/s", "cores": os.cpu_count(), "kind": "reference",
                "sample": f"reference trlan, plain solves of {n_cpu} of the held-out operators "
                          f"({mv / n_cpu:.0f} matvecs each), OpenBLAS + OpenMP CSR callback"}
     if rank == 0:
         print(json.dumps({
-            "metric": "learned-seed solves/s to residual <= 1e-8 (Gaussian wells 256x256, smallest 16)",
+            "metric": WELLS_METRIC,
             "value": world / seeded_s, "unit": "solves/s", "n_gpus": world, "steps": n_prob,
             "warmup": args.warmup, "ms_per_step": 1e3 * seeded_s, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64 solver, bf16 network",
             "data": "synthetic (seeded well potentials, held-out seeds)",
-            "config": {"workload": "wells256: n=65536, 8 Gaussian wells, ned=16, maxlan=48, tol=1e-8, "
-                                   "CSR, seed = sum of network outputs (guess=1)",
+            "config": {"workload": WELLS_WORKLOAD,
                        "problems_per_rank": n_prob, "parallelism": f"replicas x{world}",
                        "l2": "operator and basis fit in L2 (latency-bound regime)"},
             "plain_solves_per_s": world / reduce_max(pg, ab["plain_s"], dev),

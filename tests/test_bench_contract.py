@@ -43,3 +43,10 @@ def test_reference_arm_of_batched_workload():
     assert line["impl"] == "reference" and line["unit"] == "problems/s" and line["value"] > 0
     assert line["cpu_baseline"]["value"] == line["value"]
     assert "6 problems" in line["cpu_baseline"]["sample"]
+
+
+@pytest.mark.skipif(not ref.available(), reason="reference library not built")
+def test_reference_arm_of_learned_seed_workload_needs_no_gpu():
+    line = _run("--impl", "reference", "--workload", "wells256", "--steps", "1", "--warmup", "1")
+    assert line["impl"] == "reference" and line["unit"] == "solves/s" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "reference"
