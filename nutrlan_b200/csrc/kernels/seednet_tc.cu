@@ -18,8 +18,9 @@
 //     pixels 32w .. 32w+31, 32 channels each), add the bias, apply the ReLU
 //     and store BF16 NHWC (or the first 16 channels as FP32 for the last
 //     layer).
-// That is k_conv_tc, used for images narrower than 128 pixels.  Wider
-// images (W a multiple of 128) use k_conv_rows: the three input rows of a
+// That is k_conv_tc, used for images narrower than 128 pixels (and under
+// TRLX_SEEDNET_CONV=tap).  Wider images (W a multiple of 128) use
+// k_conv_rows: the three input rows of a
 // tile loaded once, a producer warp for the loads, and the BF16 output
 // staged in shared memory and written with TMA stores.
 // Every mbarrier wait is bounded; a wait that runs out sets a device flag
@@ -146,8 +147,9 @@ __device__ __forceinline__ unsigned pack2(float lo, float hi) {
 // Barriers: full[s] (tile loaded into stage s), done[a] (MMAs into
 // accumulator a finished: the epilogue may read it and stage s may be
 // refilled), empty[a] (the 4 epilogue warps finished reading accumulator
-// a), weights.  Serves tiles narrower than 128 pixels (W < 128), as 9
-// shifted tap tiles of TW x TH pixels.
+// a), weights.  Serves images narrower than 128 pixels (tiles of TW x TH
+// pixels), dilations above 8 and TRLX_SEEDNET_CONV=tap, as 9 shifted tap
+// tiles.
 __global__ void __launch_bounds__(160, 1)
     k_conv_tc(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap twt,
               const float *__restrict__ bias, __nv_bfloat16 *out, float *out_f32, int H, int W, int TW, int TH,
