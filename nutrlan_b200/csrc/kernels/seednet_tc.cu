@@ -20,9 +20,10 @@
 //     layer).
 // That is k_conv_tc, used for images narrower than 128 pixels (and under
 // TRLX_SEEDNET_CONV=tap).  Wider images (W a multiple of 128) use
-// k_conv_rows: the three input rows of a
-// tile loaded once, a producer warp for the loads, and the BF16 output
-// staged in shared memory and written with TMA stores.
+// k_conv_rows: the three input rows of a tile loaded once, a producer warp
+// for the loads, several MMA-issuing lanes, and the BF16 output staged in
+// shared memory and written with TMA stores.  The weight gradients are
+// k_wgrad_rows (staged rows) and k_wgrad_tc (nine tap tiles).
 // Every mbarrier wait is bounded; a wait that runs out sets a device flag
 // (read by the seed-network entry points) and the kernel still runs to its
 // end, so the TMEM allocation is always released.
