@@ -70,7 +70,8 @@ void trlx_zmatvec(const int nrow, const int ncol, const trl_dcomplex *x,
    the legacy default stream) and wrk is valid once that stream reaches it.
    Deterministic (fixed summation order).  Returns 0, -201 if ld1 or ld2 is
    smaller than nrow (the reference aborts there), -1 on invalid arguments,
-   -5 if the reduction scratch cannot be allocated. */
+   -5 if the reduction scratch cannot be allocated.  nrow = 0 (a rank with
+   no local rows) writes zeros. */
 int trlx_g_dot(int nrow, const double *v1, int ld1, int m1, const double *v2,
                int ld2, int m2, const double *rr, double *wrk, void *stream);
 /* Complex twin: wrk = [v1 v2]^H rr (ztrl_g_dot_, SRC/ztrl_comm_none.c:16). */
@@ -87,8 +88,11 @@ int trlx_zg_dot(int nrow, const trl_dcomplex *v1, int ld1, int m1,
    592 KiB array inside the library, held by every GPU that loads the library
    until the process exits; at most TRLX_G_DOT_NOALLOC_MAX_COLS columns
    (m1 + m2), larger requests return -7.  The first call on a device looks
-   up that array's device address (cudaGetSymbolAddress) and caches it, so
-   make the first call on each device before any stream capture.  All calls
+   up that array's device address (cudaGetSymbolAddress) and caches it; under
+   CUDA's lazy module loading that lookup also loads the array onto the
+   device, so the first call may allocate and synchronize.  Make it once per
+   device as a warm-up, outside any memory budget, hot loop or stream
+   capture; later calls allocate nothing.  All calls
    share the array: calls whose work overlaps on the GPU (different streams
    or threads on one device) race and must be serialised. */
 #define TRLX_G_DOT_NOALLOC_MAX_COLS 512

@@ -399,6 +399,9 @@ void ztrl_check_ritz(ztrl_matvec op, trl_info *info, int nrow, int ncol, trl_dco
         }
     }
     error_estimates(ncol, alpha, res.data(), err.data());
+    // The complex check floors the error estimate at machine epsilon times the
+    // last Ritz value (SRC/ztrlan.c:393-397); the real check does not.
+    for (int i = 0; i < ncol; ++i) err[i] = std::max(err[i], DBL_EPSILON * alpha[ncol - 1]);
     print_check_table(info, ncol, alpha, beta, eval, rq.data(), res.data(), err.data(), nrow, check);
 }
 
@@ -472,6 +475,10 @@ void trl_ritz_projection(trl_matvec op, trl_info *info, int mev, double *evec, i
         if (info->lohi != 0) nev++;
     }
     nev = std::min(nev, mev);
+    if (info->verbose >= 0) {
+        FILE *fp = info->log_fp ? info->log_fp : stdout;
+        std::fprintf(fp, "TRLAN performing a Rayleigh-Ritz project for %d vectors.", nev);
+    }
     if (nev <= 0 || nev > 128) {
         info->stat = -231;
         return;

@@ -140,6 +140,9 @@ int gdot_entry(int nrow, const C *v1, int ld1, int m1, const C *v2, int ld2, int
         return -201;
     }
     if (!rr || !wrk || (m1 > 0 && !v1) || (m2 > 0 && !v2)) return -1;
+    // No local rows (a rank that owns none): the partial products are zero.
+    if (nrow == 0)
+        return cudaMemsetAsync(wrk, 0, sizeof(C) * m, static_cast<cudaStream_t>(stream)) == cudaSuccess ? 0 : -1001;
     static thread_local GdotScratch sc;
     int dev = 0;
     cudaGetDevice(&dev);

@@ -23,7 +23,11 @@
 // Host code cannot use the array's name as a device address (in host code it
 // names a host-side stand-in).  The first call on each device, with that
 // device current, looks the address up with cudaGetSymbolAddress and caches
-// it; that first call should therefore come before any stream capture.
+// it.  With CUDA's lazy module loading (the default) that lookup is also
+// what loads the library's module, and with it the array, onto the device:
+// the first call may itself allocate device memory and synchronize.  Make it
+// once per device as a warm-up, outside any memory budget, hot loop or
+// stream capture; later calls allocate nothing.
 #include <cstdio>
 #include <mutex>
 
@@ -83,10 +87,12 @@ extern "C" int trlx_g_dot_noalloc(int nrow, const double *v1, int ld1, int m1, c
         return -7;
     }
     if (!rr || !wrk || (m1 > 0 && !v1) || (m2 > 0 && !v2)) return -1;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // No local rows (a rank that owns none): the partial products are zero.
+    if (nrow == 0) return cudaMemsetAsync(wrk, 0, sizeof(double) * m, st) == cudaSuccess ? 0 : -1001;
     int err = 0;
     double *base = scratch_address(&err);
     if (!base) return err;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     unsigned *ticket = reinterpret_cast<unsigned *>(base);
     double *part = base + kHeaderDoubles;
     if (cudaMemsetAsync(ticket, 0, sizeof(unsigned), st) != cudaSuccess) return -1001;

@@ -51,3 +51,34 @@ def csr_matvec(row_ptr, col, val, x):
         # otherwise pick up the element at its start index.
         out[nz] = np.add.reduceat(val * x[col], row_ptr[:-1][nz])
     return out
+
+
+def ritz_projection(V, matvec, lohi=-1):
+    """Rayleigh-Ritz over the rows of V (nev near-orthonormal vectors), the
+    five steps trl_ritz_projection documents (SRC/trlan.c:1443-1452):
+    G = V V^T = R^T R (Cholesky), H = R^-T (V A V^T) R^-1 = Y D Y^T, Ritz
+    vectors (R^-1 Y)^T V, residuals ||A x - d x||.  Returns (d, X, res) in
+    ascending order of d, shifted like the reference's output (lohi < 0:
+    drop the last pair; lohi > 0: drop the first).
+
+    The reference's own code does not compute this: it fills the lower
+    triangle of V^T A V and the transposed copy from column i-1 instead of
+    column i (SRC/trlan.c:1589-1593, 1602-1606), which leaves a zero row in
+    the projected matrix, so its eigenvalues are wrong; this restatement
+    follows the documented steps."""
+    V = np.asarray(V, dtype=np.float64)
+    G = V @ V.T
+    R = np.linalg.cholesky(G).T                    # G = R^T R, R upper
+    AV = np.array([matvec(v) for v in V])
+    H1 = V @ AV.T
+    H1 = 0.5 * (H1 + H1.T)
+    Rinv = np.linalg.inv(R)
+    H = Rinv.T @ H1 @ Rinv
+    d, Y = np.linalg.eigh(H)
+    X = (Rinv @ Y).T @ V
+    res = np.array([np.linalg.norm(matvec(x) - di * x) for di, x in zip(d, X)])
+    if lohi < 0:
+        return d[:-1], X[:-1], res[:-1]
+    if lohi > 0:
+        return d[1:], X[1:], res[1:]
+    return d, X, res

@@ -17,6 +17,8 @@ from nutrlan_b200._abi import TrlInfo, MATVEC, declare_common
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libnutrlan_ref.so")
+# Where the reference checkout lives: $TRLAN_REFERENCE, else the default path.
+REF_ROOT = os.environ.get("TRLAN_REFERENCE", "/root/reference")
 _LIB = None
 
 
@@ -24,8 +26,9 @@ def available():
     return os.path.exists(REF_SO)
 
 
-def build(ref_root="/root/reference"):
+def build(ref_root=None):
     """Compile the reference from its sources (only where they exist)."""
+    ref_root = ref_root or REF_ROOT
     if os.path.isdir(ref_root):
         subprocess.run(["make", "-C", HERE, f"REF={ref_root}", "-j8"], check=True,
                        stdout=subprocess.DEVNULL)
@@ -186,4 +189,5 @@ def trlan_csr(A, ned, maxlan, lohi=-1, tol=1.4901e-8, restart=1, maxmv=0, start=
         lib.trlan(fn, None, C.byref(info), n, mev, eval_.ctypes.data, evec.ctypes.data, n,
                   lwrk, wrk.ctypes.data)
     dt = time.perf_counter() - t0
-    return dict(eval=eval_, evec=evec, info=info, seconds=dt)
+    res = None if cplx else wrk[:mev].copy()  # ztrlan keeps its residual norms internal
+    return dict(eval=eval_, evec=evec, res=res, info=info, seconds=dt)

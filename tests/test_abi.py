@@ -70,3 +70,29 @@ def test_init_info_defaults(lib):
 
 def test_version_string(lib):
     assert b"sm_100a" in lib.trlx_version()
+
+
+REF_ROOT = os.environ.get("TRLAN_REFERENCE", "/root/reference")
+
+
+@pytest.mark.skipif(not os.path.isfile(os.path.join(REF_ROOT, "INC", "trlan.h")),
+                    reason="reference headers not present (set TRLAN_REFERENCE)")
+def test_every_trl_info_offset_matches_the_reference_header(tmp_path):
+    """sizeof(trl_info) and offsetof of every field, compiled with gcc
+    against include/trlan.h and against the reference's INC/trlan.h
+    (:77-245), are identical."""
+    fields = [f[0] for f in TrlInfo._fields_]
+    body = "".join(f'printf("{f} %zu\\n", offsetof(trl_info, {f}));' for f in fields)
+    src = tmp_path / "offsets.c"
+    src.write_text("#include <stddef.h>\n#include <stdio.h>\n#include \"trlan.h\"\n"
+                   "int main(){printf(\"sizeof %zu\\n\", sizeof(trl_info));" + body + "return 0;}\n")
+    outs = []
+    for inc in (os.path.join(ROOT, "include"), os.path.join(REF_ROOT, "INC")):
+        exe = tmp_path / ("off_" + str(len(outs)))
+        subprocess.run(["gcc", "-I", inc, str(src), "-o", str(exe)], check=True)
+        outs.append(subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout)
+    assert outs[0] == outs[1]
+    got = dict(line.split() for line in outs[0].splitlines())
+    assert got["sizeof"] == "800" and len(got) == len(fields) + 1
+    for f in fields:                      # and the Python mirror agrees with both
+        assert int(got[f]) == getattr(TrlInfo, f).offset, f

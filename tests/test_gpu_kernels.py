@@ -77,6 +77,14 @@ def test_g_dot_argument_errors():
                           w.data_ptr(), None) == -201
     assert lib.trlx_g_dot(100, x.data_ptr(), 100, 0, x.data_ptr(), 100, 0, x.data_ptr(),
                           w.data_ptr(), None) == 0
+    # A rank with no local rows: the partial products are zeros, not an error
+    # (the reference's ddot of length 0 is 0).
+    for f in (lib.trlx_g_dot, lib.trlx_zg_dot):
+        w.fill_(7.0)
+        assert f(0, x.data_ptr(), 0, 1, x.data_ptr(), 0, 1, x.data_ptr(), w.data_ptr(), None) == 0
+        torch.cuda.synchronize()
+        got = w.cpu().numpy()
+        assert np.all(got[:4 if f is lib.trlx_zg_dot else 2] == 0.0)
 
 
 @pytest.mark.parametrize("fmt", ["csr", "sell"])

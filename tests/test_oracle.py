@@ -153,3 +153,49 @@ def test_operator_families():
     assert V.shape == (32, 32) and V.max() <= 0 and W.n == 1024
     sizes = ops.batched_sizes(4096)
     assert sizes.min() >= 48 and sizes.max() <= 256
+
+
+def test_ritz_projection_restatement_against_dense():
+    """The numpy restatement of trl_ritz_projection's documented steps gives
+    the eigenpairs of a subspace that is an invariant subspace up to 1e-8,
+    whatever the (non-orthonormal, condition ~80) basis of it: eigenvalues
+    to 1e-10, residuals at the perturbation times the basis condition."""
+    A = ops.laplacian_2d(16, diag=ops.uniform01(4, np.arange(256, dtype=np.uint64)))
+    w, U = np.linalg.eigh(A.to_scipy().toarray())
+    rng = np.random.default_rng(1)
+    V = (U[:, :7] @ rng.standard_normal((7, 7))).T + 1e-8 * rng.standard_normal((7, 256))
+    d, X, res = K.ritz_projection(V, A.matvec, lohi=-1)
+    np.testing.assert_allclose(d, w[:6], rtol=1e-10)
+    assert np.all(res < 1e-5)
+    np.testing.assert_allclose(np.abs(np.sum(X * U[:, :6].T, axis=1)) / np.linalg.norm(X, axis=1), 1.0,
+                               atol=1e-9)
+
+
+def test_reference_ritz_projection_defect(reflib):
+    """The reference's trl_ritz_projection copies the lower triangle of V^T A V
+    from the wrong column (SRC/trlan.c:1589-1593, 1602-1606): on an exactly
+    orthonormal invariant subspace its smallest reported value is 0, not the
+    smallest eigenvalue.  This pins why the library's routine is checked
+    against the restatement of the documented steps instead."""
+    import ctypes as C
+    from nutrlan_b200._abi import TrlInfo, MATVEC
+    A = ops.laplacian_2d(16, diag=1.0 + ops.uniform01(4, np.arange(256, dtype=np.uint64)))
+    w, U = np.linalg.eigh(A.to_scipy().toarray())
+    n, mev = A.n, 8
+    V = np.ascontiguousarray(U[:, :mev].T)
+
+    def op(nrow, ncol, x, ldx, y, ldy, mvparam):
+        xv = np.ctypeslib.as_array(C.cast(x, C.POINTER(C.c_double)), (nrow,))
+        yv = np.ctypeslib.as_array(C.cast(y, C.POINTER(C.c_double)), (nrow,))
+        yv[:] = A.matvec(xv)
+    cb = MATVEC(op)
+    info = TrlInfo()
+    reflib.trl_init_info(C.byref(info), n, 32, -1, 6, 1e-8, 1, 1000, None)
+    info.verbose = -1
+    eres, base, wrk = np.zeros(2 * mev), np.zeros(n), np.zeros(256)
+    reflib.trl_ritz_projection(cb, C.byref(info), mev, V.ctypes.data, n, eres.ctypes.data, wrk.ctypes.data,
+                               wrk.size, base.ctypes.data)
+    assert info.stat == 0
+    assert eres[0] == 0.0 and w[0] > 1.0
+    d, _, _ = K.ritz_projection(U[:, :7].T, A.matvec, lohi=-1)
+    np.testing.assert_allclose(d, w[:6], rtol=1e-12)

@@ -51,3 +51,30 @@ def test_noalloc_rejects_more_columns_than_its_scratch():
     assert lib.trlx_g_dot_noalloc(n, v.data_ptr(), n, MAX_COLS, v.data_ptr(), n, 0,
                                   r.data_ptr(), w.data_ptr(), None) == 0
     torch.cuda.synchronize()
+
+
+def test_noalloc_zero_rows_and_no_device_allocation():
+    """A rank with no local rows gets zeros; after the per-device warm-up
+    (the first call loads the library's fixed array), many calls leave the
+    device's free memory unchanged.  The check is coarse: free memory moves
+    in the driver's allocation granules, so it catches allocations that are
+    kept (a leak, a growing pool), not one that is freed within the call."""
+    lib = load()
+    n, m = 1 << 20, 400
+    v = torch.randn(m * n, dtype=torch.float64, device="cuda")
+    r = torch.randn(n, dtype=torch.float64, device="cuda")
+    w = torch.full((m,), 7.0, dtype=torch.float64, device="cuda")
+    assert lib.trlx_g_dot_noalloc(0, v.data_ptr(), 0, 3, v.data_ptr(), 0, 2, r.data_ptr(), w.data_ptr(),
+                                  None) == 0
+    torch.cuda.synchronize()
+    assert torch.all(w[:5] == 0.0)
+    assert lib.trlx_g_dot_noalloc(n, v.data_ptr(), n, m, v.data_ptr(), n, 0, r.data_ptr(), w.data_ptr(),
+                                  None) == 0          # warm-up on this device
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(50):
+        assert lib.trlx_g_dot_noalloc(n, v.data_ptr(), n, m, v.data_ptr(), n, 0, r.data_ptr(),
+                                      w.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
