@@ -23,8 +23,18 @@ The metric is Lanczos steps (matvec + full reorthogonalisation) per second.
          (oracle/_ref, built from the reference sources with OpenBLAS) on the
          same operator with a compiled OpenMP CSR callback, on a bounded
          sample: the first 32 Lanczos steps (maxlan = maxmv = 32) of the same
-         solve.  The sample's basis is 4x smaller on average than a full
-         cycle's, so per-step CPU throughput is overstated, not understated.
+         solve; the reference arm's config.workload says so.  The sample's
+         basis is 4x smaller on average than a full cycle's, so per-step CPU
+         throughput is overstated, not understated.
+* format: by default the operator is created as CSR and
+         trlx_operator_autotune keeps the faster of CSR / SELL-C-32 and of
+         the projection widths (config.autotune has its measurements; the
+         other format is timed as a variant).
+* solve: time to solution, the metric's own measure: one solve to
+         residual <= 1e-8 with an FP64 basis and one with an FP32 basis plus
+         FP64 refinement: seconds, matvecs, true residuals (--no-solve skips).
+* batched: the 4096-problem batched configuration, one persistent launch
+         per solve, timed with CUDA events (--no-batched skips).
 
 Inputs (basis >= 4 GB, CSR 1.4 GB) exceed the 126 MB L2 between steps.
 Multi-GPU (N > 1): every rank solves its own replica (different potential
@@ -198,6 +208,43 @@ def run_batched_reference(args, w, world, rank):
                                        "kind": "reference", "sample": sample},
                       "e2e": {"value": val, "unit": "problems/s", "h2d_bytes_per_step": 0,
                               "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def batched_record(w, rank, solves=2):
+    """The batched configuration measured inside the default line: one
+    autotuned persistent launch per solve of all `count` problems, timed with
+    CUDA events over `solves` solves after one warm-up solve."""
+    import torch
+    from nutrlan_b200.batched import Batch
+    Ls, diags = batched_problems(w, rank)
+    b = Batch.stencil5(Ls, diags)
+    try:
+        kw = dict(ned=w["ned"], maxlan=w["maxlan"], tol=w["tol"], restart=1, maxmv=100000, seed=4242 + rank)
+        t_tune = time.perf_counter()
+        cfg = b.autotune(**kw)
+        t_tune = time.perf_counter() - t_tune
+        b.solve(**kw)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(solves):
+            r = b.solve(**kw)
+        e1.record()
+        torch.cuda.synchronize()
+        dt = e0.elapsed_time(e1) * 1e-3 / solves
+        sizes = Ls.astype(np.int64) ** 2
+        alg = float(np.sum(r.info[:, 2] * sizes * 8 * (3 + 2 * 0.75 * w["maxlan"] + 4)))
+        peak, kind = read_peaks()
+        return {"workload": f"batched{w['count']}: L~U[48,256], 5-pt Laplacian + U[0,2] diag, ned={w['ned']}, "
+                            f"maxlan={w['maxlan']}, tol={w['tol']}, one persistent launch per solve",
+                "problems_per_s": w["count"] / dt, "ms_per_solve": 1e3 * dt, "solves_timed": solves,
+                "solved": int(np.sum((r.info[:, 0] == 0) & (r.info[:, 1] >= w["ned"]))),
+                "matvecs_total": int(np.sum(r.info[:, 2])), "alg_GBps": alg / dt / 1e9,
+                "hbm_frac": alg / dt / 1e9 / peak, "peak_source": kind,
+                "autotune": {"bucket_threads": list(cfg.bucket_threads), "bucket_format": list(cfg.bucket_format),
+                             "seconds": t_tune}}
+    finally:
+        b.close()
 
 
 def run_batched(args, w, world, rank, local, pg):
@@ -412,7 +459,7 @@ def run_complex(args, w, world, rank, local, pg):
                "d2h_bytes_per_step": int(16 * n * mev + 8 * mev)}
 
     solve_rec = None
-    if args.full_solve and rank == 0:
+    if not args.no_solve and rank == 0:
         from nutrlan_b200 import residual_norms
         solve_rec = {}
         for bits in (64, 32):
@@ -585,7 +632,8 @@ def run_dist(args, w, world, rank, local, pg):
     rp, ci, va = local_rows(A, row0, nloc)
     x0 = ops.start_vector(n)[row0:row0 + nloc]
     comm = Comm.from_process_group() if pg is not None else Comm.nccl(1, 0, Comm.nccl_unique_id())
-    op = DistOperator(comm, rp, ci, va, fmt=args.format)
+    dist_fmt = "sell" if args.format == "auto" else args.format   # block rows: no autotuner
+    op = DistOperator(comm, rp, ci, va, fmt=dist_fmt)
     evec = torch.zeros((mev, nloc), dtype=torch.float64, device=dev)
 
     def one_call(profile=True):
@@ -632,7 +680,7 @@ def run_dist(args, w, world, rank, local, pg):
         hev = np.zeros((mev, nloc))
 
         def e2e_call():
-            with DistOperator(comm, rp, ci, va, fmt=args.format) as hop:
+            with DistOperator(comm, rp, ci, va, fmt=dist_fmt) as hop:
                 r = dsolve(comm, hop, ned, maxlan, tol=tol, maxmv=maxlan, start=x0, basis_bits=args.basis_bits,
                            evec=hev)
                 return r.info.matvec
@@ -660,7 +708,7 @@ def run_dist(args, w, world, rank, local, pg):
             "vs_baseline": None, "dtype": "f64" if args.basis_bits == 64 else "f32 basis / f64",
             "data": "synthetic (seeded)",
             "config": {"workload": f"{args.workload}: n={n}, ned={ned}, maxlan={maxlan}, tol={tol}, "
-                                   f"{args.format.upper()} block rows, basis fp{args.basis_bits}, "
+                                   f"{dist_fmt.upper()} block rows, basis fp{args.basis_bits}, "
                                    "one thick-restart cycle/step",
                        "parallelism": f"block rows x{world} (NCCL sums + halo exchange)",
                        "l2": "inputs larger than L2"},
@@ -704,15 +752,19 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="anderson256")
     ap.add_argument("--basis-bits", type=int, choices=[64, 32], default=64)
-    ap.add_argument("--format", choices=["csr", "sell"], default="sell")
+    ap.add_argument("--format", choices=["auto", "csr", "sell"], default="auto",
+                    help="operator format; auto: trlx_operator_autotune picks CSR or SELL-C-32 "
+                         "and the projection width by measurement")
     ap.add_argument("--cpu-sample", type=int, default=32,
                     help="Lanczos steps in the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-variants", action="store_true",
                     help="skip the secondary timings (other format, 32-bit basis)")
-    ap.add_argument("--full-solve", action="store_true",
-                    help="also run one solve to convergence (time to solution)")
+    ap.add_argument("--no-solve", action="store_true",
+                    help="skip the solves to convergence (time to solution, FP64 and FP32 basis)")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-solver record of the default line")
     ap.add_argument("--solve-maxmv", type=int, default=20000)
     ap.add_argument("--no-learned-seed", action="store_true",
                     help="skip the learned-seed A/B record of the default line")
@@ -749,14 +801,25 @@ def main():
         return
     seed = 2024 + rank
     metric = f"Lanczos steps/s (SpMV + full CGS reorth), {args.workload}, smallest {w['ned']}"
-    config = {"workload": f"{args.workload}: n={w['L'] ** (3 if w['kind'] == 'anderson' else 2)}, "
-                          f"ned={w['ned']}, maxlan={w['maxlan']}, tol={w['tol']}, "
-                          f"{args.format.upper()}, basis fp{args.basis_bits}, one thick-restart cycle/step",
+    nrows = w['L'] ** (3 if w['kind'] == 'anderson' else 2)
+
+    def workload(fmt, what):
+        return (f"{args.workload}: n={nrows}, ned={w['ned']}, maxlan={w['maxlan']}, tol={w['tol']}, "
+                f"{fmt}, {what}")
+
+    config = {"workload": workload("{fmt}", f"basis fp{args.basis_bits}, one thick-restart cycle/step"),
               "global_batch": world, "parallelism": f"replicas x{world}",
               "l2": ("inputs larger than L2 (basis >= 2 GB)" if w["kind"] == "anderson" else
                      "working set L2-resident (n = 16384: latency-bound, not an HBM measurement)")}
 
     if args.impl == "reference":
+        # The reference's per-step sample is what this line says it is: the
+        # first cpu_sample Lanczos steps of the same solve (a 128-step cycle
+        # takes about 40 s on the host cores, too long for --steps K).
+        config["workload"] = workload(
+            "CSR callback (OpenMP) + OpenBLAS",
+            f"basis fp64; sample per step: the first {args.cpu_sample} Lanczos steps of the same solve "
+            f"(maxlan=maxmv={args.cpu_sample}, reference trlan)")
         if rank != 0:
             return
         A = build_operator(w, seed)
@@ -805,7 +868,12 @@ def main():
     stats = TrlxStats()
 
     # ---- device-resident arm -------------------------------------------------
-    op = DeviceOperator(A, fmt=args.format)
+    op = DeviceOperator(A, fmt=args.format, maxlan=maxlan)
+    fmt_used = op.fmt
+    config["workload"] = config["workload"].replace("{fmt}", fmt_used.upper())
+    if op.tune is not None:
+        config["format_choice"] = "autotuned (trlx_operator_autotune)"
+        config["autotune"] = op.tune
     evec = torch.zeros((mev, n), dtype=torch.float64, device=dev)
     x0_dev = torch.as_tensor(x0, device=dev)
     eval_ = np.zeros(mev)
@@ -894,7 +962,7 @@ def main():
 
         def e2e_call():
             handle.value = None
-            if args.format == "sell":
+            if fmt_used == "sell":
                 rc = lib.trlx_sell_create(n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, 1, 0,
                                           C.byref(handle))
             else:
@@ -928,7 +996,7 @@ def main():
     variants = {}
     if not args.no_variants:
         def time_variant(fmt, bits):
-            vop = op if fmt == args.format else DeviceOperator(A, fmt=fmt)
+            vop = op if fmt == fmt_used else DeviceOperator(A, fmt=fmt)
             vopts = TrlxOptions()
             lib.trlx_default_options(C.byref(vopts))
             vopts.basis_bits = bits
@@ -956,13 +1024,13 @@ def main():
                 vop.close()
             return reduce_max(pg, mv, dev) * world / dt
 
-        other = "csr" if args.format == "sell" else "sell"
+        other = "csr" if fmt_used == "sell" else "sell"
         variants[f"{other}_fp{args.basis_bits}"] = time_variant(other, args.basis_bits)
         alt_bits = 32 if args.basis_bits == 64 else 64
-        variants[f"{args.format}_fp{alt_bits}"] = time_variant(args.format, alt_bits)
+        variants[f"{fmt_used}_fp{alt_bits}"] = time_variant(fmt_used, alt_bits)
 
     solve_rec = None
-    if args.full_solve and rank == 0:
+    if not args.no_solve and rank == 0:
         from nutrlan_b200 import residual_norms
         solve_rec = {}
         for bits in (64, 32):
@@ -990,6 +1058,7 @@ def main():
                 "max_true_residual": float(res.max()), "anrm": anrm,
                 "max_true_residual_rel": float(res.max() / anrm),
                 "eval_min": float(eval_[0]), "eval_max_converged": float(eval_[k - 1]),
+                "all_residuals_within_tol_anrm": bool(inf.nec >= ned and res.max() <= tol * anrm),
                 "evals": [float(v) for v in eval_[:k]]}
         if "fp64" in solve_rec and "fp32" in solve_rec:
             a, b = np.array(solve_rec["fp64"]["evals"]), np.array(solve_rec["fp32"]["evals"])
@@ -1013,6 +1082,12 @@ def main():
             cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {e}"}
 
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        try:
+            batched = batched_record(WORKLOADS["batched4096"], rank)
+        except Exception as e:  # noqa: BLE001
+            batched = {"failed": str(e)}
     seed_ab = None
     if rank == 0 and world == 1 and not args.no_learned_seed:
         try:
@@ -1026,7 +1101,7 @@ def main():
                 "data": "synthetic (seeded Anderson potential and start vector)", "config": config,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks, "host_wall_s": wall, "variants": variants, "solve": solve_rec,
-                "learned_seed": seed_ab,
+                "batched": batched, "learned_seed": seed_ab,
                 "matvecs_per_call": int(matvecs // max(args.steps, 1))}
         print(json.dumps(line), flush=True)
     if pg is not None:

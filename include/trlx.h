@@ -52,6 +52,29 @@ void trlx_operator_destroy(trlx_operator *op);
 long long trlx_operator_nnz(const trlx_operator *op);
 int trlx_operator_nrow(const trlx_operator *op);
 
+/* Single-solve autotuner (no counterpart in the reference, whose operator
+   is an opaque callback).  For a real operator created with
+   trlx_csr_create (not distributed) it times, on the current GPU, one fused
+   product y = A x + alpha in the CSR form and in the SELL-C-32 form built
+   from the same device arrays, and one Gram-Schmidt projection over
+   maxlan / 2 columns of the operator's row count with 8, 12 and 16 columns
+   per warp (median of 5 launches each).  It keeps the faster form in the
+   operator (storage switched in place, the handle stays valid) and the
+   faster projection for every later solve with this operator.  Temporary
+   device memory: two vectors and the projection's columns (at most a
+   quarter of the free memory).  Returns 0, -1 for an operator it does not
+   tune (complex, SELL-created or distributed), -2 if the temporary memory
+   cannot be allocated, -3 on a CUDA error. */
+typedef struct {
+    int format;            /* kept form: 0 CSR, 1 SELL-C-32                 */
+    int project_cpw;       /* kept projection columns per warp (8, 12, 16)  */
+    double spmv_ms[2];     /* one product: CSR, SELL-C-32 (-1: not built)  */
+    double project_ms[3];  /* one projection with 8, 12, 16 columns/warp    */
+    int columns;           /* projection width timed                        */
+    double seconds;        /* wall time of the tuning                       */
+} trlx_tune_result;
+int trlx_operator_autotune(trlx_operator *op, int maxlan, trlx_tune_result *out);
+
 /* trl_matvec / ztrl_matvec compatible appliers (device x, y). */
 void trlx_matvec(const int nrow, const int ncol, const double *x,
                  const int ldx, double *y, const int ldy, void *mvparam);

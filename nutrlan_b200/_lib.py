@@ -43,6 +43,18 @@ class TrlxOptions(C.Structure):
                 ("stream", c_void_p), ("refine", c_int), ("profile", c_int)]
 
 
+class TrlxTuneResult(C.Structure):
+    """trlx_tune_result: what trlx_operator_autotune measured and kept."""
+    _fields_ = [("format", c_int), ("project_cpw", c_int), ("spmv_ms", c_double * 2),
+                ("project_ms", c_double * 3), ("columns", c_int), ("seconds", c_double)]
+
+    def as_dict(self):
+        return {"format": ("csr", "sell")[self.format], "project_cpw": self.project_cpw,
+                "spmv_ms": {"csr": self.spmv_ms[0], "sell": self.spmv_ms[1]},
+                "project_ms": {str(c): self.project_ms[i] for i, c in enumerate((8, 12, 16))},
+                "columns": self.columns, "seconds": self.seconds}
+
+
 def _declare(lib):
     declare_common(lib)
     P = C.POINTER
@@ -75,6 +87,8 @@ def _declare(lib):
     lib.trlx_operator_nnz.restype = C.c_longlong
     lib.trlx_operator_nrow.argtypes = [c_void_p]
     lib.trlx_operator_nrow.restype = c_int
+    lib.trlx_operator_autotune.argtypes = [c_void_p, c_int, P(TrlxTuneResult)]
+    lib.trlx_operator_autotune.restype = c_int
     # Block-row communicators and distributed operators.
     lib.trlx_comm_create_host.argtypes = [c_int, c_int, ALLREDUCE_FN, c_void_p, P(c_void_p)]
     lib.trlx_comm_create_host.restype = c_int
@@ -138,5 +152,5 @@ def load():
     return _LIB
 
 
-__all__ = ["load", "LIB_PATH", "TrlInfo", "TrlxStats", "TrlxOptions", "MATVEC",
+__all__ = ["load", "LIB_PATH", "TrlInfo", "TrlxStats", "TrlxOptions", "TrlxTuneResult", "MATVEC",
            "USER_ORTHO"]

@@ -1,0 +1,190 @@
+// trlx_operator_autotune: the single-solve autotuner (no counterpart in the
+// reference, whose user operator is opaque).  For a built-in real operator
+// created in CSR form it measures, on this GPU and this matrix:
+//
+//  * one fused product y = A x, alpha = x^T y (the kernel every Lanczos step
+//    starts with) in the CSR form and in the SELL-C-32 form built from the
+//    same device arrays;
+//  * one Gram-Schmidt projection h = V^T r over `maxlan / 2` basis columns
+//    of this operator's row count (the average width of a thick-restart
+//    cycle) with 8, 12 and 16 columns per warp;
+//
+// and keeps the faster of each: the operator's storage is switched in place
+// to the faster form (the handle stays valid; the other form is freed) and
+// the projection width is stored in the operator, where solves with it read
+// it.  Every candidate is timed with CUDA events over `kReps` launches after
+// a warm-up launch, and the median is kept.  Products are checked against
+// each other (the same alpha up to summation order) before a form is adopted.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "../../../include/trlx.h"
+#include "lanczos_kernels.h"
+#include "spmv.h"
+
+namespace {
+
+constexpr int kReps = 5;
+
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf() { cudaFree(p); }
+    bool alloc(size_t bytes) {
+        if (cudaMalloc(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            return false;
+        }
+        return true;
+    }
+};
+
+__global__ void k_fill_pattern(double *v, long n, long n_pad, unsigned salt) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += stride) {
+        // Deterministic values in [-1, 1); padding rows stay zero as the
+        // kernels require.
+        unsigned x = (unsigned)(i * 2654435761u) ^ (salt * 0x9E3779B9u);
+        x ^= x >> 15;
+        x *= 0x2c1b3c6du;
+        x ^= x >> 12;
+        v[i] = i < n ? (double)(x & 0xFFFFFF) / 8388608.0 - 1.0 : 0.0;
+    }
+}
+
+template <class F>
+double median_ms(F launch, cudaStream_t st) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    launch();  // warm-up
+    std::vector<float> t(kReps);
+    for (int r = 0; r < kReps; ++r) {
+        cudaEventRecord(a, st);
+        launch();
+        cudaEventRecord(b, st);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&t[r], a, b);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    std::sort(t.begin(), t.end());
+    return t[kReps / 2];
+}
+
+void move_storage(trlx_operator *dst, trlx_operator *src) {
+    std::swap(dst->kind, src->kind);
+    std::swap(dst->nnz, src->nnz);
+    std::swap(dst->row_ptr, src->row_ptr);
+    std::swap(dst->col, src->col);
+    std::swap(dst->val, src->val);
+    std::swap(dst->nslice, src->nslice);
+    std::swap(dst->sigma, src->sigma);
+    std::swap(dst->slice_ptr, src->slice_ptr);
+    std::swap(dst->perm, src->perm);
+}
+
+}  // namespace
+
+extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_result *out) {
+    if (!A || !out) return -1;
+    *out = trlx_tune_result{};
+    if (A->kind != 0 || A->halo) return -1;  // tunes real CSR-created, undistributed operators
+    const auto t0 = std::chrono::steady_clock::now();
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (A->device >= 0 && A->device != prev) cudaSetDevice(A->device);
+    int rc = 0;
+    const long n = A->nrow;
+    const long n_pad = (n + 255) / 256 * 256;
+    const int m = std::max(8, std::min(128, maxlan / 2));
+    cudaStream_t st = nullptr;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    // Vectors, reduction scratch and the projection's basis columns.
+    trlb::Scratch s;
+    s.max_blocks = 148 * 8;
+    s.max_cols = m;
+    DevBuf x, y, part, tick, dsc, basis, table;
+    const size_t vec = sizeof(double) * (size_t)n_pad;
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    // The projection is timed over m columns when they fit in a quarter of
+    // the free memory, else over as many as fit (at least 8).
+    int mp = (int)std::min<size_t>((size_t)m, free_b / 4 / std::max<size_t>(vec, 1));
+    if (mp < 8 || !x.alloc(vec) || !y.alloc(vec) || !part.alloc((size_t)s.max_blocks * (m + 2) * 16) ||
+        !tick.alloc(sizeof(unsigned) * trlb::kNumTickets) || !dsc.alloc(sizeof(double) * (m + 4)) ||
+        !basis.alloc(vec * mp) || !table.alloc(sizeof(double *) * mp)) {
+        rc = -2;
+    }
+    trlx_operator *other = nullptr;
+    if (!rc) {
+        s.partials = part.p;
+        s.tickets = static_cast<unsigned *>(tick.p);
+        cudaMemsetAsync(tick.p, 0, sizeof(unsigned) * trlb::kNumTickets, st);
+        k_fill_pattern<<<592, 256, 0, st>>>(static_cast<double *>(x.p), n, n_pad, 1u);
+        for (int c = 0; c < mp; ++c)
+            k_fill_pattern<<<592, 256, 0, st>>>(static_cast<double *>(basis.p) + (size_t)c * n_pad, n, n_pad,
+                                                 7u + c);
+        std::vector<double *> cols(mp);
+        for (int c = 0; c < mp; ++c) cols[c] = static_cast<double *>(basis.p) + (size_t)c * n_pad;
+        cudaMemcpyAsync(table.p, cols.data(), sizeof(double *) * mp, cudaMemcpyHostToDevice, st);
+        cudaStreamSynchronize(st);
+        // ---- operator form ----------------------------------------------
+        double *alpha = static_cast<double *>(dsc.p);
+        out->spmv_ms[0] = median_ms(
+            [&] {
+                trlb::spmv_fused_real(A, static_cast<double *>(x.p), static_cast<double *>(y.p), n_pad, alpha, &s,
+                                      st);
+            },
+            st);
+        double a_csr = 0.0, a_sell = 0.0;
+        cudaMemcpy(&a_csr, alpha, sizeof(double), cudaMemcpyDeviceToHost);
+        rc = trlx_sell_create((int)n, A->row_ptr, A->col, static_cast<const double *>(A->val), 1,
+                              TRLX_DEVICE_ARRAYS, &other);
+        if (rc == 0) {
+            out->spmv_ms[1] = median_ms(
+                [&] {
+                    trlb::spmv_fused_real(other, static_cast<double *>(x.p), static_cast<double *>(y.p), n_pad,
+                                          alpha, &s, st);
+                },
+                st);
+            cudaMemcpy(&a_sell, alpha, sizeof(double), cudaMemcpyDeviceToHost);
+            // Same product up to the summation order of n terms of order one.
+            const bool same = std::fabs(a_sell - a_csr) <= 1e-13 * (double)n + 1e-12 * std::fabs(a_csr);
+            out->format = (same && out->spmv_ms[1] < out->spmv_ms[0]) ? 1 : 0;
+            if (out->format == 1) move_storage(A, other);  // A takes the SELL arrays, `other` the CSR ones
+        } else {
+            rc = 0;  // keep CSR when SELL cannot be built (memory)
+            out->format = 0;
+            out->spmv_ms[1] = -1.0;
+        }
+        // ---- projection columns per warp --------------------------------
+        trlb::Recur<double> none;
+        const int cpws[3] = {8, 12, 16};
+        int best = 2;
+        for (int k = 0; k < 3; ++k) {
+            out->project_ms[k] = median_ms(
+                [&] {
+                    trlb::launch_project<double>(static_cast<double *const *>(table.p), mp, n_pad,
+                                                 static_cast<const double *>(x.p), none,
+                                                 static_cast<double *>(dsc.p), static_cast<double *>(dsc.p) + m + 1,
+                                                 s, st, cpws[k]);
+                },
+                st);
+            if (out->project_ms[k] < out->project_ms[best]) best = k;
+        }
+        A->project_cpw = cpws[best];
+        out->project_cpw = cpws[best];
+        out->columns = mp;
+        if (cudaStreamSynchronize(st) != cudaSuccess) rc = -3;
+    }
+    if (other) trlx_operator_destroy(other);
+    cudaStreamDestroy(st);
+    cudaGetLastError();
+    if (A->device >= 0 && A->device != prev) cudaSetDevice(prev);
+    out->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}

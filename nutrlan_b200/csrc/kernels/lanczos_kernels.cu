@@ -638,7 +638,7 @@ void launch_dot(const C *x, const C *y, long n_pad, double *out, Scratch &s, cud
 template <class T>
 void launch_project(T *const *cols, int m, long n_pad, const typename Store<T>::C *r,
                     Recur<typename Store<T>::C> rec, typename Store<T>::C *h, double *out2,
-                    Scratch &s, cudaStream_t st) {
+                    Scratch &s, cudaStream_t st, int cpw_req) {
     using C = typename Store<T>::C;
     constexpr int R = Store<T>::R;
     int nb = std::min(stream_blocks(n_pad, R), s.max_blocks);
@@ -654,12 +654,14 @@ void launch_project(T *const *cols, int m, long n_pad, const typename Store<T>::
     if constexpr (std::is_same<C, double>::value) {
         // Columns per warp: 16 keeps one accumulator per column for 128
         // columns per sweep (2 blocks/SM); 12 and 8 trade a second sweep for
-        // 3-4 resident blocks.  TRLX_PROJECT_CPW selects (tuning only).
-        static const int cpw = [] {
+        // 3-4 resident blocks.  The caller's choice (the operator's
+        // autotuned value), else TRLX_PROJECT_CPW, else 16.
+        static const int cpw_env = [] {
             const char *e = std::getenv("TRLX_PROJECT_CPW");
             int v = e ? std::atoi(e) : 16;
             return (v == 8 || v == 12) ? v : 16;
         }();
+        const int cpw = (cpw_req == 8 || cpw_req == 12 || cpw_req == 16) ? cpw_req : cpw_env;
         if (cpw == 8)
             args(k_project<T, 8>);
         else if (cpw == 12)
@@ -797,7 +799,7 @@ void launch_cheb(const zd *ay, const zd *y, const zd *yp, long n_pad, double a, 
 
 #define TRLB_INST(T)                                                                              \
     template void launch_project<T>(T *const *, int, long, const Store<T>::C *, Recur<Store<T>::C>, \
-                                    Store<T>::C *, double *, Scratch &, cudaStream_t);            \
+                                    Store<T>::C *, double *, Scratch &, cudaStream_t, int);       \
     template void launch_update<T>(T *const *, int, long, const Store<T>::C *, Recur<Store<T>::C>,  \
                                    const Store<T>::C *, Store<T>::C *, double *, Scratch &,        \
                                    cudaStream_t);                                                 \

@@ -31,6 +31,9 @@ struct trlx_operator {
     // this rank's rows, [nrow, nrow + halo entries) values received from
     // other ranks before every product.
     trlb::Halo *halo = nullptr;
+    // Columns per warp of the FP64 Gram-Schmidt projection for solves with
+    // this operator, set by trlx_operator_autotune (0: the default).
+    int project_cpw = 0;
 };
 
 namespace trlb {

@@ -19,14 +19,23 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from ._abi import TrlInfo, MATVEC
-from ._lib import load, TrlxStats, TrlxOptions
+from ._lib import load, TrlxStats, TrlxOptions, TrlxTuneResult
 
 
 class DeviceOperator:
-    """A trlx_operator (CSR, SELL-C-32 or complex CSR) resident on the GPU."""
+    """A trlx_operator (CSR, SELL-C-32 or complex CSR) resident on the GPU.
 
-    def __init__(self, csr, fmt="csr", sigma=1):
+    ``fmt="auto"`` creates the CSR form and runs trlx_operator_autotune
+    (``maxlan`` sets the projection width it times): the operator keeps the
+    faster of CSR and SELL-C-32 and the faster projection kernel for its
+    solves; ``self.tune`` holds what was measured."""
+
+    def __init__(self, csr, fmt="csr", sigma=1, maxlan=128):
         lib = load()
+        self.tune = None
+        auto = fmt == "auto"
+        if auto:
+            fmt = "csr"
         self.lib = lib
         self.n = csr.n
         self.complex = np.iscomplexobj(csr.val)
@@ -48,6 +57,14 @@ class DeviceOperator:
         if rc != 0:
             raise RuntimeError(f"trlx operator creation failed ({rc})")
         self.fmt = "zcsr" if self.complex else fmt
+        if auto and not self.complex:
+            res = TrlxTuneResult()
+            rc = lib.trlx_operator_autotune(self.handle, int(maxlan), C.byref(res))
+            if rc != 0:
+                self.close()
+                raise RuntimeError(f"trlx_operator_autotune failed ({rc})")
+            self.tune = res.as_dict()
+            self.fmt = self.tune["format"]
         self.nnz = lib.trlx_operator_nnz(self.handle)
         # The exported applier, used as `op` so the engine takes its fused path.
         name = "trlx_zmatvec" if self.complex else "trlx_matvec"

@@ -1,0 +1,73 @@
+"""Single-solve autotuner (trlx_operator_autotune): it keeps the faster of
+the measured CSR / SELL-C-32 forms and of the measured projection widths,
+the tuned operator computes the same product, and a solve with it returns
+the reference's eigenvalues (the golden Anderson 64^3 run of
+tests/golden/config_runs.json) like the untuned CSR operator does."""
+import ctypes as C
+import json
+import os
+
+import numpy as np
+import pytest
+
+from nutrlan_b200 import operators as ops, DeviceOperator, solve, load
+from nutrlan_b200._lib import TrlxTuneResult
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def product(op, x):
+    lib = load()
+    f = lib.trlx_matvec
+    f.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+    f.restype = None
+    xd = torch.as_tensor(x).cuda()
+    yd = torch.empty_like(xd)
+    f(op.n, 1, xd.data_ptr(), op.n, yd.data_ptr(), op.n, op.handle)
+    torch.cuda.synchronize()
+    return yd.cpu().numpy()
+
+
+@pytest.mark.parametrize("L", [24, 96])
+def test_autotune_keeps_the_faster_measured_forms(L):
+    A = ops.anderson_3d(L, W=4.0, seed=5)
+    x = ops.start_vector(A.n, seed=3)
+    with DeviceOperator(A, fmt="auto", maxlan=64) as op:
+        t = op.tune
+        print(f"L={L}: {t}")
+        assert t["format"] in ("csr", "sell") and op.fmt == t["format"]
+        sp = t["spmv_ms"]
+        assert min(sp.values()) > 0
+        assert sp[t["format"]] == min(sp.values())
+        pm = t["project_ms"]
+        assert t["project_cpw"] in (8, 12, 16) and pm[str(t["project_cpw"])] == min(pm.values())
+        assert t["columns"] == 32
+        y = product(op, x)
+    np.testing.assert_allclose(y, A.matvec(x), rtol=1e-13, atol=1e-13)
+
+
+def test_autotuned_solve_matches_reference():
+    g = json.load(open(os.path.join(HERE, "golden", "config_runs.json")))["anderson64_full"]
+    A = ops.anderson_3d(g["L"], W=g["W"], seed=g["pot_seed"])
+    with DeviceOperator(A, fmt="auto", maxlan=g["maxlan"]) as op:
+        r = solve(op, ned=g["ned"], maxlan=g["maxlan"], maxmv=100000, tol=g["tol"], restart=g["restart"],
+                  start=ops.start_vector(A.n, seed=g["start_seed"]), mev=g["mev"], device=True)
+    assert r.stat == 0 and r.nec >= g["ned"]
+    got, want = np.sort(r.eval[:g["ned"]]), np.sort(np.array(g["eval"])[:g["ned"]])
+    assert np.max(np.abs(got - want) / np.abs(want)) <= 1e-10
+    assert abs(r.info.matvec - g["matvec"]) <= 0.05 * g["matvec"]
+
+
+def test_autotune_rejects_operators_it_does_not_tune():
+    lib = load()
+    res = TrlxTuneResult()
+    P = ops.peierls_2d(16, phi=1.0 / 16.0)
+    with DeviceOperator(P) as op:
+        assert lib.trlx_operator_autotune(op.handle, 32, C.byref(res)) == -1
+    A = ops.laplacian_2d(32)
+    with DeviceOperator(A, fmt="sell") as op:
+        assert lib.trlx_operator_autotune(op.handle, 32, C.byref(res)) == -1
+    assert lib.trlx_operator_autotune(None, 32, C.byref(res)) == -1
