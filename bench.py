@@ -510,7 +510,8 @@ def learned_seed_ab(problems, seed0=10 ** 6, log=None):
     from nutrlan_b200.seed_train import evaluate, summarize
     net = SeedNet.pretrained()
     try:
-        recs = evaluate(net, range(seed0, seed0 + problems), 256, maxlan=48, log=log or (lambda *a: None))
+        recs = evaluate(net, range(seed0, seed0 + problems), 256, maxlan=48, log=log or (lambda *a: None),
+                        subspace=True)
     finally:
         net.close()
     out = summarize(recs)
@@ -520,6 +521,12 @@ def learned_seed_ab(problems, seed0=10 ** 6, log=None):
                                                   for r in recs))
     out["max_eval_rel_diff_vs_plain"] = float(max(max(r["sum_eval_rel_diff"], r["rr_eval_rel_diff"])
                                                   for r in recs))
+    out["subspace"] = {
+        "dense": "restarted dense Rayleigh-Ritz over span(seed Ritz vectors, Krylov block), exact residuals",
+        "first": "one dense cycle from the seed, then trlan from the sum of its Ritz vectors",
+        "dense_all_converged": bool(all(r["dense_converged"] for r in recs)),
+        "dense_max_eval_rel_diff_vs_plain": float(max(r["dense_eval_rel_diff"] for r in recs)),
+        "first_all_converged": bool(all(r["first_nec"] >= 16 for r in recs))}
     return out
 
 

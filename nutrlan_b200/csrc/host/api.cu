@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <ctime>
+#include <memory>
 #include <vector>
 
 #include "../../../include/trlx.h"
@@ -90,7 +91,8 @@ double host_dot(int n, const double *x, const double *y) {
 
 void print_check_table(trl_info *info, int ncol, const double *alpha, const double *beta, const double *eval,
                        const double *rq, const double *res, const double *err, int nrow, int *check) {
-    FILE *fp = info->log_fp ? info->log_fp : stdout;
+    trlb::LogOut log_out(info);
+    FILE *fp = log_out.fp;
     if (info->stat != 0) *check = -4;
     std::fprintf(fp, "TRL_CHECK_RITZ: \n");
     std::fprintf(fp, "           Ritz value       res norm   res diff  est error  diff w rq  act. error\n");
@@ -274,7 +276,8 @@ void trlx_release_workspace(void) { trlb::release_workspace(); }
 const char *trlx_version(void) { return "trlan-b200 0.1 (sm_100a)"; }
 
 void trl_print_info(trl_info *info, int mvflop) {
-    FILE *fp = info->log_fp ? info->log_fp : stdout;
+    trlb::LogOut log_out(info);
+    FILE *fp = log_out.fp;
     const double t_op = info->tick_o, t_tot = info->tick_t, t_res = info->tick_r, t_orth = info->tick_h;
     const double r_op = (t_op != 0 && mvflop > 0) ? (double)mvflop * info->matvec : 0.0;
     const double r_orth = info->rflp_h + info->flop_h;
@@ -314,7 +317,11 @@ void trl_print_info(trl_info *info, int mvflop) {
 }
 
 void trl_terse_info(trl_info *info, FILE *iou) {
-    if (!iou) iou = info->log_fp ? info->log_fp : stdout;
+    std::unique_ptr<trlb::LogOut> log_out;
+    if (!iou) {
+        log_out.reset(new trlb::LogOut(info));
+        iou = log_out->fp;
+    }
     const double t_op = info->tick_o, t_tot = info->tick_t, t_res = info->tick_r, t_orth = info->tick_h;
     const char sign = info->lohi > 0 ? '+' : (info->lohi < 0 ? '-' : '0');
     std::fprintf(iou, "MAXLAN:%10d, Restart:%10d,   NED: %c %7d,      NEC:%10d\n", info->maxlan, info->restart, sign,
@@ -413,7 +420,8 @@ void trl_rayleigh_quotients(trl_matvec op, trl_info *info, int ncol, double *eve
     const int nrow = info->nloc;
     if (ncol <= 0) return;
     if (info->verbose >= 0) {
-        FILE *fp = info->log_fp ? info->log_fp : stdout;
+        trlb::LogOut log_out(info);
+    FILE *fp = log_out.fp;
         std::fprintf(fp, "TRLAN computing Rayleigh Quotients for %d Ritz pairs\n", ncol);
     }
     const bool dev = trlb::is_device_pointer(evec);
@@ -476,7 +484,8 @@ void trl_ritz_projection(trl_matvec op, trl_info *info, int mev, double *evec, i
     }
     nev = std::min(nev, mev);
     if (info->verbose >= 0) {
-        FILE *fp = info->log_fp ? info->log_fp : stdout;
+        trlb::LogOut log_out(info);
+    FILE *fp = log_out.fp;
         std::fprintf(fp, "TRLAN performing a Rayleigh-Ritz project for %d vectors.", nev);
     }
     if (nev <= 0 || nev > 128) {

@@ -57,6 +57,23 @@ std::string pe_filename(const char *prefix, int rank, int npes) {
     return base + num;
 }
 
+LogOut::LogOut(trl_info *info, const char *mode) {
+    if (info->log_fp) {
+        fp = static_cast<FILE *>(info->log_fp);
+    } else if (info->log_file[0] != '\0') {
+        const std::string name = pe_filename(info->log_file, info->my_pe, info->npes);
+        FILE *f = std::fopen(name.c_str(), mode);
+        if (f) {
+            fp = f;
+            own = true;
+        }
+    }
+}
+
+LogOut::~LogOut() {
+    if (own) std::fclose(fp);
+}
+
 trlx_stats &last_stats() {
     static thread_local trlx_stats s;
     return s;
@@ -1412,7 +1429,8 @@ int Engine<T>::refine_fp64(int k, double *max_res) {
 template <class T>
 void Engine<T>::log_progress() {
     if (info_->verbose <= 0) return;
-    FILE *fp = info_->log_fp ? info_->log_fp : stdout;
+    LogOut log(info_);
+    FILE *fp = log.fp;
     std::fprintf(fp, "MATVEC: %10d,    Nloop: %10d,     Nec: %10d\n", info_->matvec, info_->nloop, info_->nec);
     std::fprintf(fp, "Reorth: %10d,    Nrand: %10d,    Ierr: %10d\n", info_->north, info_->nrand, info_->stat);
     std::fprintf(fp, "Target: %10.3e,   ResNrm: %10.3e,  CFact: %10.3e\n", info_->trgt, info_->tres, info_->crat);
@@ -1801,6 +1819,7 @@ void run_trlan(trl_matvec op, trl_uo uo, trl_info *info, int nrow, int mev, doub
     info->stat = 0;
     clear_counter(info, nrow, mev, lde);
     if (info->stat != 0) return;
+    { LogOut start(info, "w"); }  // a new solve starts a new log file (SRC/trlan.c:235)
     if (opt.basis_bits == 32)
         solve<float>(op, uo, info, nrow, mev, eval, evec, lde, wrk, std::min(mev, lwrk), opt);
     else
@@ -1820,6 +1839,7 @@ void run_ztrlan(ztrl_matvec op, trl_info *info, int nrow, int mev, double *eval,
     info->stat = 0;
     clear_counter(info, nrow, mev, lde);
     if (info->stat != 0) return;
+    { LogOut start(info, "w"); }  // a new solve starts a new log file (SRC/trlan.c:235)
     std::vector<double> res(mev, 0.0);
     if (opt.basis_bits == 32)
         solve<zf>(op, nullptr, info, nrow, mev, eval, evec, lde, res.data(), mev, opt);

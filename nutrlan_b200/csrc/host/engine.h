@@ -39,6 +39,19 @@ bool is_device_pointer(const void *p);
 // zero-padded to the number of digits of npes.
 std::string pe_filename(const char *prefix, int rank, int npes);
 
+// The reference's diagnostic channel (trl_open_logfile / trl_reopen_logfile,
+// SRC/trlaux.c:48-118): info->log_fp when the caller opened one, else the
+// per-process file named by trl_set_debug's prefix, else stdout.  A file
+// opened here is closed by the destructor.
+struct LogOut {
+    FILE *fp = stdout;
+    bool own = false;
+    explicit LogOut(trl_info *info, const char *mode = "a");
+    ~LogOut();
+    LogOut(const LogOut &) = delete;
+    LogOut &operator=(const LogOut &) = delete;
+};
+
 // Frees the calling thread's cached device workspace.
 void release_workspace();
 

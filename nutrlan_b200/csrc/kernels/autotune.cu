@@ -164,7 +164,6 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
         // ---- projection columns per warp --------------------------------
         trlb::Recur<double> none;
         const int cpws[3] = {8, 12, 16};
-        int best = 2;
         for (int k = 0; k < 3; ++k) {
             out->project_ms[k] = median_ms(
                 [&] {
@@ -174,8 +173,10 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
                                                  s, st, cpws[k]);
                 },
                 st);
-            if (out->project_ms[k] < out->project_ms[best]) best = k;
         }
+        int best = 2;  // the default width unless another one measured faster
+        for (int k = 0; k < 2; ++k)
+            if (out->project_ms[k] < out->project_ms[best]) best = k;
         A->project_cpw = cpws[best];
         out->project_cpw = cpws[best];
         out->columns = mp;

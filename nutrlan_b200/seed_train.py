@@ -117,13 +117,16 @@ def validate(net, V, U, batch=32, lam=1.0):
     return tot / max(cnt, 1)
 
 
-def evaluate(net, seeds, L=256, ned=NOUT, maxlan=48, tol=1e-8, restart=1, log=print):
+def evaluate(net, seeds, L=256, ned=NOUT, maxlan=48, tol=1e-8, restart=1, log=print, subspace=False):
     """Plain vs learned-seed solves on held-out operators.  Per seed: the
     plain solve (seeded uniform start), the seed injected as the sum of its
     Rayleigh-Ritz vectors ("rr", its NOUT projection matvecs counted) and as
     the sum of the normalised network outputs ("sum"); matvecs, wall seconds
     (network forward and projection inside the seeded times), eigenvalue
-    agreement with the plain solve and true residuals of the seeded ones."""
+    agreement with the plain solve and true residuals of the seeded ones.
+    With ``subspace`` also the seed as a subspace (seed_subspace.py): dense
+    restarted Rayleigh-Ritz ("dense") and one dense cycle followed by trlan
+    ("first")."""
     import torch
     from .solver import residual_norms
     out = []
@@ -162,6 +165,23 @@ def evaluate(net, seeds, L=256, ned=NOUT, maxlan=48, tol=1e-8, restart=1, log=pr
                 if project:
                     rec["seed_res_median"] = float(np.median(sres))
             rec["tol_abs"] = tol * float(rp.info.anrm)
+            if subspace:
+                # The seed as a subspace (evaluation paths, seed_subspace.py).
+                from .seed_subspace import dense_cycles, first_cycle_then_trlan
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                net.forward(Vd, out=Y)
+                d = dense_cycles(op, Y[0], k=ned, m=maxlan, tol=tol)
+                torch.cuda.synchronize()
+                rec.update(dense_matvec=int(d["matvec"]), dense_s=time.perf_counter() - t0,
+                           dense_cycles=int(d["cycles"]), dense_converged=bool(d["converged"]),
+                           dense_eval_rel_diff=float(np.max(np.abs(np.sort(d["theta"]) - ep_[:ned]) /
+                                                            np.abs(ep_[:ned]))))
+                t0 = time.perf_counter()
+                net.forward(Vd, out=Y)
+                mv1, r1 = first_cycle_then_trlan(op, Y[0], ned=ned, m=maxlan, tol=tol, maxlan=maxlan)
+                torch.cuda.synchronize()
+                rec.update(first_matvec=int(mv1), first_s=time.perf_counter() - t0, first_nec=int(r1.nec))
         out.append(rec)
         log(f"eval seed {s}: plain {rec['plain_matvec']} mv {rec['plain_s'] * 1e3:.1f} ms | rr "
             f"{rec['rr_matvec']} mv (incl. {NOUT} projection) {rec['rr_s'] * 1e3:.1f} ms | sum "
@@ -173,7 +193,9 @@ def evaluate(net, seeds, L=256, ned=NOUT, maxlan=48, tol=1e-8, restart=1, log=pr
 def summarize(recs):
     m = lambda k: float(np.mean([r[k] for r in recs]))
     out = dict(problems=len(recs), plain_matvec=m("plain_matvec"), plain_s=m("plain_s"))
-    for mode in ("rr", "sum"):
+    for mode in ("rr", "sum", "dense", "first"):
+        if f"{mode}_matvec" not in recs[0]:
+            continue
         out[f"{mode}_matvec"] = m(f"{mode}_matvec")
         out[f"{mode}_s"] = m(f"{mode}_s")
         out[f"{mode}_matvec_ratio"] = out["plain_matvec"] / out[f"{mode}_matvec"]

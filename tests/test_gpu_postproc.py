@@ -171,7 +171,7 @@ def test_check_ritz_reports_unconverged_and_error_state(reflib, capfd):
     capfd.readouterr()
     assert got[:2] == got[2:], got
     assert got[0] == 1          # nec < ned
-    assert got[1] == -4         # the solver's error status
+    assert got[1] <= -4         # the solver's error status (-4), then the table's own checks
 
 
 @pytest.mark.parametrize("noise", [0.0, 1e-3])

@@ -143,9 +143,10 @@ def test_learned_seed_on_held_out_wells():
     predicted subspaces are far closer to the true lowest eigenvectors and
     its seeds have far smaller Rayleigh-Ritz residuals; seeded solves return
     the plain solve's eigenvalues (1e-10 relative) with true residuals <=
-    tol * ||A|| and use fewer matvecs than seeds from the untrained network.
-    Matvecs and times of plain vs seeded solves are reported, not asserted:
-    the gain over the plain solve is small on this family."""
+    tol * ||A|| and use fewer matvecs than seeds from the untrained network;
+    the output-sum seed uses no more matvecs than the plain solve on average
+    (gain >= 1.0x asserted, printed: the gain is small on this family, see
+    the subspace variants of the benchmark's learned_seed record)."""
     from nutrlan_b200.seed_train import evaluate, summarize, potentials
     import torch
     seeds = range(2 * 10 ** 6, 2 * 10 ** 6 + 6)
@@ -178,6 +179,9 @@ def test_learned_seed_on_held_out_wells():
     print("untrained", su)
     assert np.median([r["seed_res_median"] for r in rt]) < 0.3 * np.median([r["seed_res_median"] for r in ru])
     assert st["rr_matvec"] < su["rr_matvec"] and st["sum_matvec"] < su["sum_matvec"], (st, su)
+    print(f"gain over plain: output-sum seed {st['sum_matvec_ratio']:.3f}x matvecs, "
+          f"{st['sum_time_ratio']:.3f}x time; Rayleigh-Ritz seed {st['rr_matvec_ratio']:.3f}x matvecs")
+    assert st["sum_matvec_ratio"] >= 1.0, st
 
 
 _CONV_CHILD = r"""
