@@ -242,7 +242,7 @@ def batched_record(w, rank, solves=2):
                 "matvecs_total": int(np.sum(r.info[:, 2])), "alg_GBps": alg / dt / 1e9,
                 "hbm_frac": alg / dt / 1e9 / peak, "peak_source": kind,
                 "autotune": {"bucket_threads": list(cfg.bucket_threads), "bucket_format": list(cfg.bucket_format),
-                             "seconds": t_tune}}
+                             "cta_threads": cfg.cta_threads, "seconds": t_tune}}
     finally:
         b.close()
 
@@ -303,7 +303,7 @@ def run_batched(args, w, world, rank, local, pg):
                 "solved": solved, "matvecs_total": matvecs,
                 "alg_GBps": alg_bytes / (dt / args.steps) / 1e9,
                 "autotune": {"bucket_threads": list(cfg.bucket_threads), "bucket_format": list(cfg.bucket_format),
-                             "seconds": t_tune},
+                             "cta_threads": cfg.cta_threads, "seconds": t_tune},
                 "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(line), flush=True)
     b.close()

@@ -57,23 +57,30 @@ int trlx_operator_nrow(const trlx_operator *op);
    trlx_csr_create (not distributed) it times, on the current GPU, one fused
    product y = A x + alpha in the CSR form and in the SELL-C-32 form built
    from the same device arrays, and one Gram-Schmidt projection over
-   maxlan / 2 columns of the operator's row count with 8, 12 and 16 columns
-   per warp (median of 5 launches each).  It keeps the faster form in the
-   operator (storage switched in place, the handle stays valid) and the
-   faster projection for every later solve with this operator.  Temporary
+   maxlan / 2 columns of the operator's row count in each of the projection
+   kernel's forms (median of 5 launches each).  It keeps the faster operator
+   form (storage switched in place, the handle stays valid) and the faster
+   projection form for every later solve with this operator.  Temporary
    device memory: two vectors and the projection's columns (at most a
    quarter of the free memory).  Returns 0, -1 for an operator it does not
    tune (complex, SELL-created or distributed), -2 if the temporary memory
    cannot be allocated, -3 on a CUDA error. */
 typedef struct {
-    int format;            /* kept form: 0 CSR, 1 SELL-C-32                 */
-    int project_cpw;       /* kept projection columns per warp (8, 12, 16)  */
+    int format;            /* kept operator form: 0 CSR, 1 SELL-C-32        */
+    int project_form;      /* kept projection form: 1, 2, 3: 8, 12, 16
+                              columns per warp; 4: 16 columns with the
+                              column-pointer table in shared memory        */
     double spmv_ms[2];     /* one product: CSR, SELL-C-32 (-1: not built)  */
-    double project_ms[3];  /* one projection with 8, 12, 16 columns/warp    */
+    double project_ms[4];  /* one projection in forms 1 .. 4               */
     int columns;           /* projection width timed                        */
     double seconds;        /* wall time of the tuning                       */
 } trlx_tune_result;
 int trlx_operator_autotune(trlx_operator *op, int maxlan, trlx_tune_result *out);
+/* Sets the projection form of later solves with this operator (a
+   trlx_tune_result.project_form value, 0 for the default), for example to
+   reuse a tuning result on an operator created again from the same matrix.
+   Returns 0, or -1 for a null operator or an unknown form. */
+int trlx_operator_set_project_form(trlx_operator *op, int project_form);
 
 /* trl_matvec / ztrl_matvec compatible appliers (device x, y). */
 void trlx_matvec(const int nrow, const int ncol, const double *x,
@@ -216,12 +223,13 @@ long long trlx_operator_halo(const trlx_operator *op);
 /* ---------------------------------------------------------------------------
  * Batched solver: many independent real symmetric problems of uneven size,
  * smallest (lohi < 0) eigenpairs of each, solved by ONE persistent kernel
- * launch.  Each problem is solved by a group of 256, 512 or 1024 threads of
- * a CTA running the same thick-restart algorithm as trlan() (FP64 basis);
- * problems are taken largest first from a device work queue.  The group
- * size and the operator format (stencil or CSR) per size bucket
- * (n > 32768, 8192 < n <= 32768, n <= 8192) are chosen by an autotuner
- * that times a sample of each bucket.  No counterpart in the reference.
+ * launch.  Each problem is solved by a group of threads of a CTA (the
+ * CTA's 1024 or 512 threads, or a half or quarter of them) running the same
+ * thick-restart algorithm as trlan() (FP64 basis); problems are taken
+ * largest first from a device work queue.  The CTA size, the group size
+ * and the operator format (stencil or CSR) per size bucket (n > 32768,
+ * 8192 < n <= 32768, n <= 8192) are chosen by an autotuner that times a
+ * sample of each bucket.  No counterpart in the reference.
  * ------------------------------------------------------------------------- */
 typedef struct trlx_batch trlx_batch;
 
@@ -238,16 +246,21 @@ typedef struct {
     int ned, maxlan, lohi, restart, maxmv; /* as in trl_info; maxlan <= 64 */
     double tol;
     unsigned long long seed; /* start vectors / random restarts          */
-    int threads;             /* 0: autotuned per bucket; else 256/512/1024
-                                (-1 if that split's shared memory does not
-                                fit for this maxlan)                        */
+    int threads;             /* 0: autotuned per bucket; else the group
+                                size: cta_threads, 1/2 or 1/4 of it (-1 if
+                                that split's shared memory does not fit for
+                                this maxlan)                                */
     int format;              /* -1: autotuned; 0 stencil, 1 CSR           */
+    int cta_threads;         /* 0: autotuned; 1024 (64 registers/thread,
+                                8-column projection passes) or 512 (up to
+                                128 registers, 16-column passes)           */
 } trlx_batch_options;
 
 typedef struct {
     int bucket_threads[3];
     int bucket_format[3];
     double tune_seconds;
+    int cta_threads;         /* threads per CTA of the launch              */
 } trlx_batch_config;
 
 void trlx_batch_default_options(trlx_batch_options *o);

@@ -45,13 +45,15 @@ class TrlxOptions(C.Structure):
 
 class TrlxTuneResult(C.Structure):
     """trlx_tune_result: what trlx_operator_autotune measured and kept."""
-    _fields_ = [("format", c_int), ("project_cpw", c_int), ("spmv_ms", c_double * 2),
-                ("project_ms", c_double * 3), ("columns", c_int), ("seconds", c_double)]
+    _fields_ = [("format", c_int), ("project_form", c_int), ("spmv_ms", c_double * 2),
+                ("project_ms", c_double * 4), ("columns", c_int), ("seconds", c_double)]
+
+    FORMS = ("cpw8", "cpw12", "cpw16", "cpw16_shared_ptrs")
 
     def as_dict(self):
-        return {"format": ("csr", "sell")[self.format], "project_cpw": self.project_cpw,
+        return {"format": ("csr", "sell")[self.format], "project_form": self.FORMS[self.project_form - 1],
                 "spmv_ms": {"csr": self.spmv_ms[0], "sell": self.spmv_ms[1]},
-                "project_ms": {str(c): self.project_ms[i] for i, c in enumerate((8, 12, 16))},
+                "project_ms": {f: self.project_ms[i] for i, f in enumerate(self.FORMS)},
                 "columns": self.columns, "seconds": self.seconds}
 
 
@@ -89,6 +91,8 @@ def _declare(lib):
     lib.trlx_operator_nrow.restype = c_int
     lib.trlx_operator_autotune.argtypes = [c_void_p, c_int, P(TrlxTuneResult)]
     lib.trlx_operator_autotune.restype = c_int
+    lib.trlx_operator_set_project_form.argtypes = [c_void_p, c_int]
+    lib.trlx_operator_set_project_form.restype = c_int
     # Block-row communicators and distributed operators.
     lib.trlx_comm_create_host.argtypes = [c_int, c_int, ALLREDUCE_FN, c_void_p, P(c_void_p)]
     lib.trlx_comm_create_host.restype = c_int

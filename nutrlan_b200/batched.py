@@ -16,12 +16,12 @@ from ._lib import load
 class BatchOptions(C.Structure):
     _fields_ = [("ned", C.c_int), ("maxlan", C.c_int), ("lohi", C.c_int), ("restart", C.c_int),
                 ("maxmv", C.c_int), ("tol", C.c_double), ("seed", C.c_ulonglong),
-                ("threads", C.c_int), ("format", C.c_int)]
+                ("threads", C.c_int), ("format", C.c_int), ("cta_threads", C.c_int)]
 
 
 class BatchConfig(C.Structure):
     _fields_ = [("bucket_threads", C.c_int * 3), ("bucket_format", C.c_int * 3),
-                ("tune_seconds", C.c_double)]
+                ("tune_seconds", C.c_double), ("cta_threads", C.c_int)]
 
 
 def _declare(lib):
@@ -81,13 +81,13 @@ class Batch:
             raise RuntimeError(f"trlx_batch_set_start failed ({rc})")
 
     def options(self, ned=8, maxlan=32, tol=1e-8, restart=1, maxmv=100000, seed=None, threads=0,
-                fmt=-1, lohi=-1):
+                fmt=-1, lohi=-1, cta=0):
         o = BatchOptions()
         self.lib.trlx_batch_default_options(C.byref(o))
         o.ned, o.maxlan, o.tol, o.restart, o.maxmv, o.lohi = ned, maxlan, tol, restart, maxmv, lohi
         if seed is not None:
             o.seed = seed
-        o.threads, o.format = threads, fmt
+        o.threads, o.format, o.cta_threads = threads, fmt, cta
         return o
 
     def autotune(self, **kw):
@@ -160,14 +160,16 @@ def main(argv=None):
     from . import operators as ops
     ap = argparse.ArgumentParser(description=main.__doc__)
     ap.add_argument("--problems", type=int, default=512)
-    ap.add_argument("--threads", type=int, default=0, help="0: autotuned; 256/512/1024")
+    ap.add_argument("--threads", type=int, default=0, help="0: autotuned; else the group size (128..1024)")
     ap.add_argument("--format", type=int, default=-1, help="-1: autotuned; 0 stencil, 1 CSR")
+    ap.add_argument("--cta", type=int, default=0, help="0: autotuned; 1024 or 512 threads per CTA")
     ap.add_argument("--repeat", type=int, default=2)
     a = ap.parse_args(argv)
     Ls = ops.batched_sizes(a.problems, seed=777)
     diags = [2.0 * ops.uniform01(1000 + k, np.arange(int(L) * int(L), dtype=np.uint64)) for k, L in enumerate(Ls)]
     b = Batch.stencil5(Ls, diags)
-    kw = dict(ned=8, maxlan=32, tol=1e-8, restart=1, maxmv=100000, seed=4242, threads=a.threads, fmt=a.format)
+    kw = dict(ned=8, maxlan=32, tol=1e-8, restart=1, maxmv=100000, seed=4242, threads=a.threads, fmt=a.format,
+              cta=a.cta)
     for _ in range(a.repeat):
         t0 = time.perf_counter()
         r = b.solve(**kw)
@@ -175,7 +177,7 @@ def main(argv=None):
     print(json.dumps({"problems": a.problems, "seconds": dt, "problems_per_s": a.problems / dt,
                       "matvecs": int(r.info[:, 2].sum()), "solved": int((r.info[:, 1] >= 8).sum()),
                       "bucket_threads": list(r.config.bucket_threads),
-                      "bucket_format": list(r.config.bucket_format)}))
+                      "bucket_format": list(r.config.bucket_format), "cta_threads": r.config.cta_threads}))
     b.close()
 
 

@@ -298,8 +298,8 @@ class Engine {
     // modes
     bool user_dev_ = false;
     const trlx_operator *builtin_ = nullptr;
-    // Projection columns per warp tuned for the built-in operator (0: default).
-    int proj_cpw() const { return builtin_ ? builtin_->project_cpw : 0; }
+    // Projection kernel form tuned for the built-in operator (0: default).
+    int proj_form() const { return builtin_ ? builtin_->project_form : 0; }
     bool host_op_ = false;
     // Block-row solve: sums over the ranks of the communicator stored in
     // info->mpicomp by trlx_init_info_comm (nullptr: one GPU).
@@ -670,7 +670,7 @@ int Engine<T>::cgs(int m, bool pass_done, double *rnrm, bool *irnd_used) {
             if (!(first && pass_done)) {
                 Recur<C> none;
                 int p1 = pbeg();
-                launch_project<T>(d_cols_, m, n_pad_, r64_, none, d_coef_, d_scal_ + kR2Pre, scratch_, st_, proj_cpw());
+                launch_project<T>(d_cols_, m, n_pad_, r64_, none, d_coef_, d_scal_ + kR2Pre, scratch_, st_, proj_form());
                 pend(p1, TRLX_K_PROJECT, (double)m * nrow_ * sv() + nrow_ * cs());
                 if (int e = project_sums(m)) return e;
                 int p2 = pbeg();
@@ -746,7 +746,7 @@ int Engine<T>::orth(int m, bool recur, double beta_prev, int kept) {
     }
     const double recb = recur ? 2.0 * nrow_ * cs() : 0.0;
     int p1 = pbeg();
-    launch_project<T>(d_cols_, m, n_pad_, r64_, rec, d_coef_, d_scal_ + kR2Pre, scratch_, st_, proj_cpw());
+    launch_project<T>(d_cols_, m, n_pad_, r64_, rec, d_coef_, d_scal_ + kR2Pre, scratch_, st_, proj_form());
     pend(p1, TRLX_K_PROJECT, (double)m * nrow_ * sv() + nrow_ * cs() + recb);
     if (int e = project_sums(m)) return e;
     int p2 = pbeg();
@@ -1180,7 +1180,7 @@ int Engine<T>::spec_segment(int *jnd_io, int S, int kept) {
                 rec.beta_r2 = lg - 4 + 3;
             const double recb = 2.0 * nrow_ * cs();
             int p1 = pbeg();
-            launch_project<T>(d_cols_, j, n_pad_, r, rec, d_coef_, lg + 1, scratch_, st_, proj_cpw());
+            launch_project<T>(d_cols_, j, n_pad_, r, rec, d_coef_, lg + 1, scratch_, st_, proj_form());
             pend(p1, TRLX_K_PROJECT, (double)j * nrow_ * sv() + nrow_ * cs() + recb);
             int p2 = pbeg();
             launch_update<T>(d_cols_, j, n_pad_, r, rec, d_coef_, r, lg + 3, scratch_, st_);

@@ -7,11 +7,12 @@
 //    same device arrays;
 //  * one Gram-Schmidt projection h = V^T r over `maxlan / 2` basis columns
 //    of this operator's row count (the average width of a thick-restart
-//    cycle) with 8, 12 and 16 columns per warp;
+//    cycle) in each form of the projection kernel (8, 12, 16 columns per
+//    warp; 16 with the pointer table in shared memory);
 //
 // and keeps the faster of each: the operator's storage is switched in place
 // to the faster form (the handle stays valid; the other form is freed) and
-// the projection width is stored in the operator, where solves with it read
+// the projection form is stored in the operator, where solves with it read
 // it.  Every candidate is timed with CUDA events over `kReps` launches after
 // a warm-up launch, and the median is kept.  Products are checked against
 // each other (the same alpha up to summation order) before a form is adopted.
@@ -161,24 +162,23 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
             out->format = 0;
             out->spmv_ms[1] = -1.0;
         }
-        // ---- projection columns per warp --------------------------------
+        // ---- projection kernel form -------------------------------------
         trlb::Recur<double> none;
-        const int cpws[3] = {8, 12, 16};
-        for (int k = 0; k < 3; ++k) {
+        for (int k = 0; k < 4; ++k) {
             out->project_ms[k] = median_ms(
                 [&] {
                     trlb::launch_project<double>(static_cast<double *const *>(table.p), mp, n_pad,
                                                  static_cast<const double *>(x.p), none,
                                                  static_cast<double *>(dsc.p), static_cast<double *>(dsc.p) + m + 1,
-                                                 s, st, cpws[k]);
+                                                 s, st, trlb::kProject8 + k);
                 },
                 st);
         }
-        int best = 2;  // the default width unless another one measured faster
-        for (int k = 0; k < 2; ++k)
+        int best = trlb::kProject16 - trlb::kProject8;  // the default unless another form measured faster
+        for (int k = 0; k < 4; ++k)
             if (out->project_ms[k] < out->project_ms[best]) best = k;
-        A->project_cpw = cpws[best];
-        out->project_cpw = cpws[best];
+        A->project_form = trlb::kProject8 + best;
+        out->project_form = trlb::kProject8 + best;
         out->columns = mp;
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = -3;
     }
@@ -188,4 +188,10 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
     if (A->device >= 0 && A->device != prev) cudaSetDevice(prev);
     out->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return rc;
+}
+
+extern "C" int trlx_operator_set_project_form(trlx_operator *A, int form) {
+    if (!A || form < trlb::kProjectDefault || form > trlb::kProject16Shared) return -1;
+    A->project_form = form;
+    return 0;
 }

@@ -37,7 +37,7 @@ struct Shared {
     trl_info info;
     double alpha[kMaxL + 2], beta[kMaxL + 2], alfrot[kMaxL + 2], betrot[kMaxL + 2];
     double lambda[kMaxL + 2], res[kMaxL + 2], h[kMaxL + 2], g[kMaxL + 2], wrk2[2 * (kMaxL + 2)];
-    double red[32][8];
+    double red[32][16];
     double scal[8];
     int ctl[8];
 };
@@ -132,15 +132,18 @@ __device__ inline double apply_op(const Params &P, const Problem &pr, const doub
 // handled by thread 0.  Padding rows (n .. ld) are never read.
 __device__ inline double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
 
+template <int CW>
 __device__ inline void project(const double *V, int ld, int n, int m, double *y, bool rec, const double *x,
                                const double *xp, double alpha, double beta, const Grp &G) {
     Shared &S = *G.S;
     double r2 = 0.0;
     const int np = n >> 1;
     const bool tail = (n & 1) && G.tid == 0;
-    for (int c0 = 0; c0 < m; c0 += 8) {
-        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        const int mm = min(8, m - c0);
+    for (int c0 = 0; c0 < m; c0 += CW) {
+        double acc[CW];
+#pragma unroll
+        for (int k = 0; k < CW; ++k) acc[k] = 0.0;
+        const int mm = min(CW, m - c0);
         const double *Vc = V + (size_t)c0 * ld;
         for (int p = G.tid; p < np; p += G.nt) {
             const int i = 2 * p;
@@ -157,7 +160,7 @@ __device__ inline void project(const double *V, int ld, int n, int m, double *y,
                 r2 += r1 * r1;
             }
 #pragma unroll
-            for (int k = 0; k < 8; ++k)
+            for (int k = 0; k < CW; ++k)
                 if (k < mm) {
                     const double2 v = ld2(Vc + (size_t)k * ld + i);
                     acc[k] = fma(v.x, r0, acc[k]);
@@ -173,10 +176,10 @@ __device__ inline void project(const double *V, int ld, int n, int m, double *y,
             }
             if (c0 == 0) r2 += ri * ri;
 #pragma unroll
-            for (int k = 0; k < 8; ++k)
+            for (int k = 0; k < CW; ++k)
                 if (k < mm) acc[k] = fma(Vc[(size_t)k * ld + i], ri, acc[k]);
         }
-        block_reduce<8>(acc, &S.h[c0], G);
+        block_reduce<CW>(acc, &S.h[c0], G);
     }
     if (m == 0) {
         for (int i = G.tid; i < n; i += G.nt) {
@@ -271,6 +274,7 @@ __device__ inline void random_vector(double *y, int n, uint64_t seed, const Grp 
 // Classical Gram-Schmidt of column m against columns 0..m-1, continuing
 // after a first pass whose scalars are in S.scal (trl_cgs,
 // SRC/trlcore.c:2913-3117).  Returns the status; *rnrm the final norm.
+template <int CW>
 __device__ inline int cgs(const Params &P, int pid, double *V, int ld, int n, int m, bool pass_done, double *rnrm,
                           const Grp &G) {
     Shared &S = *G.S;
@@ -282,7 +286,7 @@ __device__ inline int cgs(const Params &P, int pid, double *V, int ld, int n, in
         bool first = true;
         while (cnt <= maxorth) {
             if (!(first && pass_done)) {
-                project(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, G);
+                project<CW>(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, G);
                 update(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, S.h, G);
             }
             first = false;
@@ -315,6 +319,7 @@ __device__ inline int cgs(const Params &P, int pid, double *V, int ld, int n, in
 
 // trl_orth (SRC/trlcore.c:1766-1975) for the new column m: alpha(m-1) is in
 // S.alpha, the recurrence uses beta_prev; sets S.beta[m-1].
+template <int CW>
 __device__ inline int orth(const Params &P, int pid, double *V, int ld, int n, int m, bool recur, double beta_prev,
                            int kept, const Grp &G) {
     Shared &S = *G.S;
@@ -323,7 +328,7 @@ __device__ inline int orth(const Params &P, int pid, double *V, int ld, int n, i
     const double *x = V + (size_t)(m - 1) * ld;
     const double *xp = m >= 2 ? V + (size_t)(m - 2) * ld : nullptr;
     const double a = S.alpha[jnd - 1];
-    project(V, ld, n, m, r, recur, x, xp, a, beta_prev, G);
+    project<CW>(V, ld, n, m, r, recur, x, xp, a, beta_prev, G);
     const double normrr2 = S.scal[kR2Pre];
     if (!(normrr2 >= 0.0) || !(normrr2 <= DBL_MAX)) return -102;
     double tmp = a * a;
@@ -349,7 +354,7 @@ __device__ inline int orth(const Params &P, int pid, double *V, int ld, int n, i
     if (usecgs) {
         update(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, S.h, G);
         double rnrm = sqrt(normrr2);
-        const int st = cgs(P, pid, V, ld, n, m, true, &rnrm, G);
+        const int st = cgs<CW>(P, pid, V, ld, n, m, true, &rnrm, G);
         if (st) return st;
         beta_new = rnrm;
     } else {
@@ -451,6 +456,7 @@ __device__ inline void init_info(trl_info *info, int n, int maxlan, int lohi, in
 }
 
 // One complete solve of problem pid by the calling CTA.
+template <int CW>
 __device__ void solve(const Params &P, int pid, const Grp &G, double *dyn, long tile_cap) {
     Shared &S = *G.S;
     const Problem pr = P.probs[pid];
@@ -493,7 +499,7 @@ __device__ void solve(const Params &P, int pid, const Grp &G, double *dyn, long 
         }
         G.sync();
         update(V, ld, n, jnd, V + (size_t)jnd * ld, false, nullptr, nullptr, 0.0, 0.0, S.beta, G);
-        stat = orth(P, pid, V, ld, n, jnd, false, 0.0, kept, G);
+        stat = orth<CW>(P, pid, V, ld, n, jnd, false, 0.0, kept, G);
         if (stat) break;
         if (G.tid < 32) {
             const int lane = G.tid;
@@ -515,7 +521,7 @@ __device__ void solve(const Params &P, int pid, const Grp &G, double *dyn, long 
                 S.alpha[jnd - 1] = a;
             }
             G.sync();
-            stat = orth(P, pid, V, ld, n, jnd, true, S.beta[jnd - 2], kept, G);
+            stat = orth<CW>(P, pid, V, ld, n, jnd, true, S.beta[jnd - 2], kept, G);
             if (G.tid == 0) {
                 S.alfrot[jnd - 1] = S.alpha[jnd - 1];
                 S.betrot[jnd - 1] = S.beta[jnd - 1];
@@ -690,7 +696,12 @@ __device__ void solve(const Params &P, int pid, const Grp &G, double *dyn, long 
 // Phases run largest problems first; in phase f the CTA is split into
 // groups of P.phase_threads[f] threads, each group taking problems from the
 // phase's queue until it is empty, then the whole CTA moves on.
-__global__ void __launch_bounds__(1024, 1) k_batched(Params P) {
+// CTA: threads per CTA.  The 1024-thread form has 64 registers per thread
+// and projects 8 basis columns per pass over r; the 512-thread form has up
+// to 128 and projects 16, reading r half as often.
+template <int CTA>
+__global__ void __launch_bounds__(CTA, 1) k_batched(Params P) {
+    constexpr int CW = CTA >= 1024 ? 8 : 16;
     extern __shared__ __align__(16) unsigned char smem[];
     for (int f = 0; f < P.nphases; ++f) {
         const int nt = P.phase_threads[f];
@@ -713,7 +724,7 @@ __global__ void __launch_bounds__(1024, 1) k_batched(Params P) {
                 const int q = G.S->ctl[cGo];
                 G.sync();
                 if (q >= P.phase_end[f]) break;
-                solve(P, P.order[q], G, dyn, tile_cap);
+                solve<CW>(P, P.order[q], G, dyn, tile_cap);
             }
         }
         __syncthreads();
@@ -724,40 +735,50 @@ size_t group_bytes(int maxlan) {
     return ((sizeof(Shared) + 15) / 16 * 16 + dyn_doubles(maxlan) * sizeof(double) + 127) / 128 * 128;
 }
 // Shared memory for the largest split used by the launch.
-size_t smem_bytes(int maxlan, int min_threads) { return group_bytes(maxlan) * (1024 / min_threads); }
+size_t smem_bytes(int maxlan, int min_threads, int cta) { return group_bytes(maxlan) * (cta / min_threads); }
 
 // What a launch asks for: the split's need, raised to kLaunchSmem so the
 // restart tiles of 1024- and 512-thread groups hold a few hundred rows; the
 // rest of the SM's 256 KB stays L1 cache, which the Gram-Schmidt passes'
 // re-reads of r and the previous vectors rely on.
 constexpr size_t kLaunchSmem = 96 * 1024;
-static size_t launch_smem(int maxlan, int min_threads) {
+static size_t launch_smem(int maxlan, int min_threads, int cta) {
     static const size_t want = [] {
         const char *e = std::getenv("TRLX_BATCH_SMEM_KB");  // tuning only
         const long kb = e ? std::atol(e) : 0;
         return kb > 0 ? (size_t)kb * 1024 : kLaunchSmem;
     }();
-    return std::max(smem_bytes(maxlan, min_threads), want);
+    return std::max(smem_bytes(maxlan, min_threads, cta), want);
 }
 
-int launch(const Params &P, int blocks, cudaStream_t st) {
-    int min_threads = 1024;
+template <int CTA>
+static int launch_cta(const Params &P, int blocks, cudaStream_t st) {
+    int min_threads = CTA;
     for (int f = 0; f < P.nphases; ++f) min_threads = std::min(min_threads, P.phase_threads[f]);
-    const size_t sm = launch_smem(P.maxlan, min_threads);
-    if (cudaFuncSetAttribute(k_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+    const size_t sm = launch_smem(P.maxlan, min_threads, CTA);
+    if (cudaFuncSetAttribute(k_batched<CTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
         return -1001;
     Params Q = P;
     Q.smem_total = sm;
-    k_batched<<<blocks, 1024, sm, st>>>(Q);
+    k_batched<CTA><<<blocks, CTA, sm, st>>>(Q);
     return cudaGetLastError() == cudaSuccess ? 0 : -1001;
 }
 
-int max_blocks_per_sm(int min_threads, int maxlan) {
+int launch(const Params &P, int blocks, cudaStream_t st) {
+    return P.cta == 512 ? launch_cta<512>(P, blocks, st) : launch_cta<1024>(P, blocks, st);
+}
+
+template <int CTA>
+static int blocks_per_sm(int min_threads, int maxlan) {
     int nb = 0;
-    const size_t sm = launch_smem(maxlan, min_threads);
-    cudaFuncSetAttribute(k_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batched, 1024, sm) != cudaSuccess) return 1;
+    const size_t sm = launch_smem(maxlan, min_threads, CTA);
+    cudaFuncSetAttribute(k_batched<CTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batched<CTA>, CTA, sm) != cudaSuccess) return 1;
     return std::max(nb, 1);
+}
+
+int max_blocks_per_sm(int min_threads, int maxlan, int cta) {
+    return cta == 512 ? blocks_per_sm<512>(min_threads, maxlan) : blocks_per_sm<1024>(min_threads, maxlan);
 }
 
 }  // namespace batched

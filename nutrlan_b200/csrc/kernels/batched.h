@@ -40,8 +40,11 @@ struct Params {
     double *res;   // nprob * ned
     int *info_out; // nprob * 4: stat, nec, matvec, nloop
     unsigned *queue; // one counter per phase (zero before the launch)
+    // Threads per CTA of the launch: 1024 (groups of 1024, 512 or 256) or
+    // 512 (groups of 512, 256 or 128; twice the registers per thread).
+    int cta;
     // Phases over order[]: problems order[phase_begin[f] .. phase_end[f])
-    // are solved by groups of phase_threads[f] (256, 512 or 1024) threads.
+    // are solved by groups of phase_threads[f] threads.
     int nphases;
     int phase_threads[4];
     int phase_begin[4];
@@ -50,9 +53,9 @@ struct Params {
 };
 
 size_t group_bytes(int maxlan);
-size_t smem_bytes(int maxlan, int min_threads);
+size_t smem_bytes(int maxlan, int min_threads, int cta);
 int launch(const Params &P, int blocks, cudaStream_t st);
-int max_blocks_per_sm(int min_threads, int maxlan);
+int max_blocks_per_sm(int min_threads, int maxlan, int cta);
 
 }  // namespace batched
 }  // namespace trlb

@@ -40,6 +40,7 @@ struct trlx_batch {
     int tuned_maxlan = 0;
     int bucket_threads[3] = {1024, 512, 256};
     int bucket_format[3] = {0, 0, 0};
+    int cta = 1024;
     double tune_seconds = 0.0;
 };
 
@@ -167,8 +168,12 @@ int build_csr(trlx_batch *b, const std::vector<double> &hdiag) {
     return rc;
 }
 
-int run(trlx_batch *b, Params P, int blocks) {
+// One persistent launch: SMs x resident CTAs of P.cta threads.
+int run(trlx_batch *b, Params P, int nsm) {
     if (cudaMemset(b->d_queue, 0, sizeof(unsigned) * 4) != cudaSuccess) return -1001;
+    int min_threads = P.cta;
+    for (int f = 0; f < P.nphases; ++f) min_threads = std::min(min_threads, P.phase_threads[f]);
+    const int blocks = nsm * trlb::batched::max_blocks_per_sm(min_threads, P.maxlan, P.cta);
     int rc = trlb::batched::launch(P, blocks, 0);
     if (rc) return rc;
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1001;
@@ -250,15 +255,18 @@ void trlx_batch_default_options(trlx_batch_options *o) {
     o->seed = 0x3243F6A8885A308Dull;
     o->threads = 0;
     o->format = -1;
+    o->cta_threads = 0;
 }
 
-// Whether groups of th threads fit: 1024 / th groups per CTA, each with its
-// shared state and dense workspace for maxlan.
-static bool split_fits(int maxlan, int th) {
+// Whether groups of th threads fit a CTA of cta threads: a valid split
+// (cta, cta / 2 or cta / 4) whose cta / th groups each get their shared
+// state and dense workspace for maxlan.
+static bool split_fits(int maxlan, int th, int cta) {
+    if (th != cta && th != cta / 2 && th != cta / 4) return false;
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
-    return trlb::batched::smem_bytes(maxlan, th) <= (size_t)optin;
+    return trlb::batched::smem_bytes(maxlan, th, cta) <= (size_t)optin;
 }
 
 int trlx_batch_autotune(trlx_batch *b, const trlx_batch_options *o, trlx_batch_config *best) {
@@ -275,6 +283,12 @@ int trlx_batch_autotune(trlx_batch *b, const trlx_batch_options *o, trlx_batch_c
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return b->probs[a].n > b->probs[c].n; });
     double total = 0.0;
+    // Per CTA size and bucket: the fastest split and format on the sample,
+    // and that time scaled to the whole bucket.
+    const int ctas[2] = {1024, 512};
+    double best_t[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    int best_th[2][3] = {{1024, 512, 256}, {512, 256, 128}}, best_fmt[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    bool cta_ok[2] = {o->cta_threads == 0 || o->cta_threads == 1024, o->cta_threads == 0 || o->cta_threads == 512};
     for (int bk = 0; bk < 3; ++bk) {
         std::vector<int> members;
         for (int q : order)
@@ -286,36 +300,52 @@ int trlx_batch_autotune(trlx_batch *b, const trlx_batch_options *o, trlx_batch_c
         for (int k = 0; k < want; ++k) sample.push_back(members[(size_t)k * members.size() / want]);
         int *d_sample = nullptr;
         if (upload(sample, &d_sample)) return -5;
-        double best_t = 1e30;
-        for (int fmt = 0; fmt < 2; ++fmt) {
-            for (int th : {1024, 512, 256}) {
-                if (!split_fits(o->maxlan, th)) continue;
-                Params P = base_params(b, o);
-                P.order = d_sample;
-                P.format = fmt;
-                P.nphases = 1;
-                P.phase_threads[0] = th;
-                P.phase_begin[0] = 0;
-                P.phase_end[0] = (int)sample.size();
-                P.maxmv = std::min(o->maxmv, 4 * o->maxlan);  // a bounded slice of the solve
-                cudaEventRecord(e0);
-                if (run(b, P, nsm)) {
-                    cudaFree(d_sample);
-                    return -1001;
-                }
-                cudaEventRecord(e1);
-                cudaEventSynchronize(e1);
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                total += ms * 1e-3;
-                if (ms < best_t) {
-                    best_t = ms;
-                    b->bucket_threads[bk] = th;
-                    b->bucket_format[bk] = fmt;
+        for (int ci = 0; ci < 2; ++ci) {
+            if (!cta_ok[ci]) continue;
+            const int cta = ctas[ci];
+            double bt = 1e30;
+            for (int fmt = 0; fmt < 2; ++fmt) {
+                for (int th : {cta, cta / 2, cta / 4}) {
+                    if (!split_fits(o->maxlan, th, cta)) continue;
+                    Params P = base_params(b, o);
+                    P.order = d_sample;
+                    P.format = fmt;
+                    P.cta = cta;
+                    P.nphases = 1;
+                    P.phase_threads[0] = th;
+                    P.phase_begin[0] = 0;
+                    P.phase_end[0] = (int)sample.size();
+                    P.maxmv = std::min(o->maxmv, 4 * o->maxlan);  // a bounded slice of the solve
+                    cudaEventRecord(e0);
+                    if (run(b, P, nsm)) {
+                        cudaFree(d_sample);
+                        return -1001;
+                    }
+                    cudaEventRecord(e1);
+                    cudaEventSynchronize(e1);
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    total += ms * 1e-3;
+                    if (ms < bt) {
+                        bt = ms;
+                        best_th[ci][bk] = th;
+                        best_fmt[ci][bk] = fmt;
+                    }
                 }
             }
+            if (bt >= 1e30) cta_ok[ci] = false;  // no split of this CTA fits
+            best_t[ci][bk] = bt * (double)members.size() / (double)sample.size();
         }
         cudaFree(d_sample);
+    }
+    int ci = 0;
+    if (cta_ok[1] && (!cta_ok[0] || best_t[1][0] + best_t[1][1] + best_t[1][2] <
+                                        best_t[0][0] + best_t[0][1] + best_t[0][2]))
+        ci = 1;
+    b->cta = ctas[ci];
+    for (int k = 0; k < 3; ++k) {
+        b->bucket_threads[k] = best_th[ci][k];
+        b->bucket_format[k] = best_fmt[ci][k];
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -328,6 +358,7 @@ int trlx_batch_autotune(trlx_batch *b, const trlx_batch_options *o, trlx_batch_c
             best->bucket_format[k] = b->bucket_format[k];
         }
         best->tune_seconds = total;
+        best->cta_threads = b->cta;
     }
     return 0;
 }
@@ -342,19 +373,25 @@ int trlx_batch_solve(trlx_batch *b, const trlx_batch_options *o, double *eval, d
         rc = trlx_batch_autotune(b, o, nullptr);
         if (rc) return rc;
     }
+    // CTA size: the caller's, else the one a forced group size implies
+    // (128-thread groups exist only in 512-thread CTAs), else the tuned one.
+    int cta = o->cta_threads;
+    if (!cta) cta = o->threads ? (o->threads == 128 ? 512 : 1024) : b->cta;
+    if (cta != 1024 && cta != 512) return -1;
     // Phases follow the buckets (largest problems first).  One format per
     // launch: the one most problems' buckets prefer.
     int cnt[3] = {0, 0, 0};
     for (auto &p : b->probs) cnt[bucket_of(p.n)]++;
     Params P = base_params(b, o);
     int fmt_votes[2] = {0, 0};
+    int th_of[3] = {cta, cta, cta};
     int pos = 0;
     P.nphases = 0;
     for (int bk = 0; bk < 3; ++bk) {
         if (!cnt[bk]) continue;
-        int th = o->threads ? o->threads : b->bucket_threads[bk];
-        if (th != 256 && th != 512 && th != 1024) th = 1024;
-        if (!split_fits(o->maxlan, th)) return -1;
+        int th = o->threads ? o->threads : (cta == b->cta ? b->bucket_threads[bk] : cta);
+        if (!split_fits(o->maxlan, th, cta)) return -1;
+        th_of[bk] = th;
         fmt_votes[o->format >= 0 ? o->format : b->bucket_format[bk]] += cnt[bk];
         P.phase_threads[P.nphases] = th;
         P.phase_begin[P.nphases] = pos;
@@ -362,6 +399,7 @@ int trlx_batch_solve(trlx_batch *b, const trlx_batch_options *o, double *eval, d
         pos += cnt[bk];
         P.nphases++;
     }
+    P.cta = cta;
     P.format = o->format >= 0 ? o->format : (fmt_votes[1] > fmt_votes[0] ? 1 : 0);
     if (P.format == 0 && !b->stencil) P.format = 1;
     rc = run(b, P, sms());
@@ -371,10 +409,11 @@ int trlx_batch_solve(trlx_batch *b, const trlx_batch_options *o, double *eval, d
     if (info) cudaMemcpy(info, b->d_info, sizeof(int) * 4 * (size_t)b->nprob, cudaMemcpyDeviceToHost);
     if (used) {
         for (int k = 0; k < 3; ++k) {
-            used->bucket_threads[k] = o->threads ? o->threads : b->bucket_threads[k];
+            used->bucket_threads[k] = th_of[k];
             used->bucket_format[k] = P.format;
         }
         used->tune_seconds = b->tune_seconds;
+        used->cta_threads = cta;
     }
     return 0;
 }

@@ -85,8 +85,11 @@ constexpr int proj_min_blocks() {
                : (Store<T>::R == 4 ? (CPW >= 12 ? 2 : 3) : (CPW >= 16 ? 2 : (CPW >= 12 ? 3 : 4)));
 }
 
-template <class T, int CPW>
-__global__ void __launch_bounds__(kThreads, (proj_min_blocks<T, CPW>()))
+// PS: the warp's column pointers live in shared memory and are re-read at
+// every use instead of being held in 2 * CPW registers, which lets three
+// blocks of the 16-column form reside per SM.
+template <class T, int CPW, bool PS = false>
+__global__ void __launch_bounds__(kThreads, (PS ? 3 : proj_min_blocks<T, CPW>()))
     k_project(T *const *__restrict__ cols, int m, long n_pad, long chunk,
               const typename Store<T>::C *__restrict__ r, Recur<typename Store<T>::C> rec,
               typename Store<T>::C *part, double *part_r2, unsigned *ticket,
@@ -97,26 +100,39 @@ __global__ void __launch_bounds__(kThreads, (proj_min_blocks<T, CPW>()))
     constexpr int W = kThreads / 32;
     __shared__ C red_c[W][CPW];
     __shared__ double red_r2[W];
+    __shared__ const T *sp[PS ? W : 1][PS ? CPW : 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long row0 = (long)blockIdx.x * chunk;
     const long row1 = min(n_pad, row0 + chunk);
     const double alpha = rec.on ? *rec.alpha : 0.0;
     const double beta = rec.on ? (rec.beta_r2 ? sqrt(*rec.beta_r2) : rec.beta) : 0.0;
-    const int ngroups = (m + CPW - 1) / CPW;
     double r2acc = 0.0;
-    for (int g0 = 0; g0 < ngroups; g0 += W) {
-        const int G = min(W, ngroups - g0);
+    // A sweep covers up to W * CPW columns.  Its mc columns are cut into G
+    // groups (G the smallest power of two with G * CPW >= mc) of `per`
+    // columns each, and each group's W / G warps split the rows, so every
+    // warp streams whatever the basis size.
+    for (int c0 = 0; c0 < m; c0 += W * CPW) {
+        const int mc = min(W * CPW, m - c0);
+        int G = 1;
+        while (G < W && G * CPW < mc) G *= 2;
+        const int per = (mc + G - 1) / G;
         const int wpg = W / G;
         const int grp = warp / wpg, slice = warp - grp * wpg;
-        const bool active = grp < G;
-        const int cb = (g0 + grp) * CPW;
-        const T *p[CPW];
+        const int cb = c0 + grp * per;
+        const int cn = max(0, min(per, m - cb));
+        const bool active = cn > 0;
+        const T *p[PS ? 1 : CPW];
+        if constexpr (PS) {
+            if (lane < CPW) sp[warp][lane] = lane < cn ? cols[cb + lane] : nullptr;
+            __syncwarp();
+        } else {
 #pragma unroll
-        for (int k = 0; k < CPW; ++k) p[k] = (active && cb + k < m) ? cols[cb + k] : nullptr;
+            for (int k = 0; k < CPW; ++k) p[k] = k < cn ? cols[cb + k] : nullptr;
+        }
         C acc[CPW];
 #pragma unroll
         for (int k = 0; k < CPW; ++k) acc[k] = czero(C());
-        const bool count_r2 = (g0 == 0 && grp == 0);
+        const bool count_r2 = (c0 == 0 && grp == 0);
         if (active) {
             for (long i = row0 + (long)(slice * 32 + lane) * R; i < row1; i += (long)wpg * 32 * R) {
                 C rv[R];
@@ -134,9 +150,14 @@ __global__ void __launch_bounds__(kThreads, (proj_min_blocks<T, CPW>()))
                 }
 #pragma unroll
                 for (int k = 0; k < CPW; ++k) {
-                    if (p[k]) {
+                    const T *pk;
+                    if constexpr (PS)
+                        pk = *reinterpret_cast<const T *const volatile *>(&sp[warp][k]);
+                    else
+                        pk = p[k];
+                    if (pk) {
                         C v[R];
-                        S::load(p[k] + i, v);
+                        S::load(pk + i, v);
 #pragma unroll
                         for (int q = 0; q < R; ++q) fma_conj(acc[k], v[q], rv[q]);
                     }
@@ -152,14 +173,30 @@ __global__ void __launch_bounds__(kThreads, (proj_min_blocks<T, CPW>()))
         __syncthreads();
         if (threadIdx.x < G * CPW) {
             const int gg = threadIdx.x / CPW, k = threadIdx.x - gg * CPW;
-            const int c = (g0 + gg) * CPW + k;
-            if (c < m) {
+            const int c = c0 + gg * per + k;
+            if (k < per && c < m) {
                 C s = czero(C());
                 for (int sl = 0; sl < wpg; ++sl) s = s + red_c[gg * wpg + sl][k];
                 part[(long)blockIdx.x * m + c] = s;
             }
         }
         __syncthreads();
+    }
+    if (m == 0) {
+        // No columns: the pass still returns ||r||^2 (warps split the rows).
+        for (long i = row0 + (long)threadIdx.x * R; i < row1; i += (long)kThreads * R) {
+            C rv[R];
+            load_c<R>(r + i, rv);
+            if (rec.on) {
+                C xv[R], xpv[R];
+                load_c<R>(rec.x + i, xv);
+                load_c<R>(rec.xp + i, xpv);
+#pragma unroll
+                for (int q = 0; q < R; ++q) rv[q] = rv[q] - alpha * xv[q] - beta * xpv[q];
+            }
+#pragma unroll
+            for (int q = 0; q < R; ++q) r2acc += abs2(rv[q]);
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) r2acc += __shfl_down_sync(0xffffffffu, r2acc, o);
@@ -638,7 +675,7 @@ void launch_dot(const C *x, const C *y, long n_pad, double *out, Scratch &s, cud
 template <class T>
 void launch_project(T *const *cols, int m, long n_pad, const typename Store<T>::C *r,
                     Recur<typename Store<T>::C> rec, typename Store<T>::C *h, double *out2,
-                    Scratch &s, cudaStream_t st, int cpw_req) {
+                    Scratch &s, cudaStream_t st, int form_req) {
     using C = typename Store<T>::C;
     constexpr int R = Store<T>::R;
     int nb = std::min(stream_blocks(n_pad, R), s.max_blocks);
@@ -652,20 +689,24 @@ void launch_project(T *const *cols, int m, long n_pad, const typename Store<T>::
                                       out2);
     };
     if constexpr (std::is_same<C, double>::value) {
-        // Columns per warp: 16 keeps one accumulator per column for 128
-        // columns per sweep (2 blocks/SM); 12 and 8 trade a second sweep for
-        // 3-4 resident blocks.  The caller's choice (the operator's
-        // autotuned value), else TRLX_PROJECT_CPW, else 16.
-        static const int cpw_env = [] {
+        // Forms (kProject*): 16 columns per warp keep one accumulator per
+        // column for 128 columns per sweep (2 blocks/SM); 12 and 8 trade a
+        // second sweep for 3-4 resident blocks; 16 with the pointer table in
+        // shared memory frees registers for a third block.  The caller's
+        // choice (the operator's autotuned form), else TRLX_PROJECT_CPW
+        // (8, 12, 16), else 16.
+        static const int form_env = [] {
             const char *e = std::getenv("TRLX_PROJECT_CPW");
             int v = e ? std::atoi(e) : 16;
-            return (v == 8 || v == 12) ? v : 16;
+            return v == 8 ? kProject8 : (v == 12 ? kProject12 : kProject16);
         }();
-        const int cpw = (cpw_req == 8 || cpw_req == 12 || cpw_req == 16) ? cpw_req : cpw_env;
-        if (cpw == 8)
+        const int form = (form_req >= kProject8 && form_req <= kProject16Shared) ? form_req : form_env;
+        if (form == kProject8)
             args(k_project<T, 8>);
-        else if (cpw == 12)
+        else if (form == kProject12)
             args(k_project<T, 12>);
+        else if (form == kProject16Shared)
+            args(k_project<T, 16, true>);
         else
             args(k_project<T, 16>);
     } else {

@@ -42,14 +42,18 @@ template <class C>
 void launch_dot(const C *x, const C *y, long n_pad, double *out, Scratch &s,
                 cudaStream_t st);
 
+// Forms of the FP64-storage projection kernel (other storage types have
+// one): 8, 12 or 16 columns per warp, or 16 with the column-pointer table in
+// shared memory (three resident blocks per SM).
+enum ProjectForm { kProjectDefault = 0, kProject8 = 1, kProject12 = 2, kProject16 = 3, kProject16Shared = 4 };
+
 // h[c] = V[:,c]^H r for c < m; out2[0] = ||r||^2, out2[1] = ||h||^2.
-// cpw: columns per warp of the FP64-storage kernel (8, 12 or 16; 0 = the
-// default, 16, or TRLX_PROJECT_CPW); other storage types have one form.
+// form: a ProjectForm (kProjectDefault: 16 columns, or TRLX_PROJECT_CPW).
 template <class T>
 void launch_project(T *const *cols, int m, long n_pad,
                     const typename Store<T>::C *r,
                     Recur<typename Store<T>::C> rec, typename Store<T>::C *h,
-                    double *out2, Scratch &s, cudaStream_t st, int cpw = 0);
+                    double *out2, Scratch &s, cudaStream_t st, int form = kProjectDefault);
 
 // r_out = r - V h (r computed with the recurrence if rec.on);
 // *out_r2 = ||r_out||^2.  r_out may alias r.

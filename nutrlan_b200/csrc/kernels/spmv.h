@@ -31,9 +31,10 @@ struct trlx_operator {
     // this rank's rows, [nrow, nrow + halo entries) values received from
     // other ranks before every product.
     trlb::Halo *halo = nullptr;
-    // Columns per warp of the FP64 Gram-Schmidt projection for solves with
-    // this operator, set by trlx_operator_autotune (0: the default).
-    int project_cpw = 0;
+    // Form of the FP64 Gram-Schmidt projection kernel (trlb::ProjectForm)
+    // for solves with this operator, set by trlx_operator_autotune (0: the
+    // default form).
+    int project_form = 0;
 };
 
 namespace trlb {

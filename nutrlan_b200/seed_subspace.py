@@ -27,6 +27,7 @@ seeded solve is the start-vector channel, guess = 1), kept to measure what
 the subspace would buy.
 """
 import ctypes as C
+import json
 
 from ._lib import load
 
@@ -143,4 +144,71 @@ def first_cycle_then_trlan(op, Y, ned=16, m=48, tol=1e-8, maxlan=48):
     return d["matvec"] + int(r.info.matvec), r
 
 
-__all__ = ["dense_cycles", "first_cycle_then_trlan"]
+__all__ = ["dense_cycles", "first_cycle_then_trlan", "seed_quality_study"]
+
+
+def seed_quality_study(problems=4, eps=(1e-1, 1e-2, 1e-3, 1e-4, 1e-6), L=256, ned=16, maxlan=48, tol=1e-8,
+                       seed0=10 ** 6, log=print):
+    """Matvecs to residual <= tol * ||A|| on held-out well operators for seeds
+    of known quality: the exact lowest 16 eigenvectors (from a plain solve of
+    the 60 lowest pairs) plus eps times a unit-norm error spread over the
+    next 44 eigenvectors and white noise, fed in three ways: as one start
+    vector (the sum of the seed's Rayleigh-Ritz vectors, then trlan; the
+    product's channel), as a dense restarted subspace (dense_cycles) and as
+    one dense cycle followed by trlan (first_cycle_then_trlan).  The trained
+    network's own seed is measured the same way.  Returns a list of records
+    (one per operator), all on the GPU."""
+    import numpy as np
+    import torch
+    from . import operators as ops
+    from .seednet import SeedNet, seed_start
+    from .solver import DeviceOperator, solve
+    out = []
+    net = SeedNet.pretrained()
+    try:
+        for s in range(seed0, seed0 + problems):
+            A, V = ops.wells_2d(L, seed=s)
+            rec = {"seed": s}
+            with DeviceOperator(A) as op:
+                x0 = torch.as_tensor(ops.start_vector(A.n), device="cuda")
+                plain = solve(op, ned=ned, maxlan=maxlan, tol=tol, restart=1, maxmv=100000, start=x0, device=True)
+                rec["plain"] = int(plain.info.matvec)
+                big = solve(op, ned=60, maxlan=160, tol=1e-10, restart=1, maxmv=200000, start=x0, device=True)
+                U = big.evec[:60].t().contiguous()                       # (n, 60), ascending
+                gen = torch.Generator(device="cuda").manual_seed(s)
+                C = torch.randn((44, ned), dtype=torch.float64, device="cuda", generator=gen)
+                Wn = torch.randn((A.n, ned), dtype=torch.float64, device="cuda", generator=gen)
+                E = U[:, ned:] @ C / np.sqrt(44.0) + 0.1 * Wn / np.sqrt(A.n)
+                Y_net = torch.empty((1, A.n, ned), dtype=torch.float32, device="cuda")
+                net.forward(torch.as_tensor(V, dtype=torch.float32, device="cuda")[None], out=Y_net)
+                seeds = [("net", Y_net[0].double())] + [(f"eps{e:g}", U[:, :ned] + e * E) for e in eps]
+                for name, Y in seeds:
+                    ev = torch.zeros((ned + 1, A.n), dtype=torch.float64, device="cuda")
+                    seed_start(op, Y.float().contiguous(), out=ev[0], project=True)
+                    r = solve(op, ned=ned, maxlan=maxlan, tol=tol, restart=1, maxmv=100000, start=ev[0], evec=ev,
+                              device=True)
+                    d = dense_cycles(op, Y, k=ned, m=maxlan, tol=tol)
+                    f, _ = first_cycle_then_trlan(op, Y, ned=ned, m=maxlan, tol=tol, maxlan=maxlan)
+                    rec[name] = {"start_vector": int(r.info.matvec) + ned, "dense": int(d["matvec"]),
+                                 "dense_converged": bool(d["converged"]), "first_cycle": int(f)}
+            out.append(rec)
+            log(json.dumps(rec))
+    finally:
+        net.close()
+    return out
+
+
+def main(argv=None):
+    import argparse
+    ap = argparse.ArgumentParser(description=seed_quality_study.__doc__)
+    ap.add_argument("--problems", type=int, default=4)
+    ap.add_argument("--out", default=None, help="write the records as JSON here")
+    a = ap.parse_args(argv)
+    recs = seed_quality_study(a.problems)
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(recs, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

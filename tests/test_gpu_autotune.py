@@ -43,7 +43,7 @@ def test_autotune_keeps_the_faster_measured_forms(L):
         assert min(sp.values()) > 0
         assert sp[t["format"]] == min(sp.values())
         pm = t["project_ms"]
-        assert t["project_cpw"] in (8, 12, 16) and pm[str(t["project_cpw"])] == min(pm.values())
+        assert t["project_form"] in pm and pm[t["project_form"]] == min(pm.values())
         assert t["columns"] == 32
         y = product(op, x)
     np.testing.assert_allclose(y, A.matvec(x), rtol=1e-13, atol=1e-13)
@@ -53,6 +53,24 @@ def test_autotuned_solve_matches_reference():
     g = json.load(open(os.path.join(HERE, "golden", "config_runs.json")))["anderson64_full"]
     A = ops.anderson_3d(g["L"], W=g["W"], seed=g["pot_seed"])
     with DeviceOperator(A, fmt="auto", maxlan=g["maxlan"]) as op:
+        r = solve(op, ned=g["ned"], maxlan=g["maxlan"], maxmv=100000, tol=g["tol"], restart=g["restart"],
+                  start=ops.start_vector(A.n, seed=g["start_seed"]), mev=g["mev"], device=True)
+    assert r.stat == 0 and r.nec >= g["ned"]
+    got, want = np.sort(r.eval[:g["ned"]]), np.sort(np.array(g["eval"])[:g["ned"]])
+    assert np.max(np.abs(got - want) / np.abs(want)) <= 1e-10
+    assert abs(r.info.matvec - g["matvec"]) <= 0.05 * g["matvec"]
+
+
+@pytest.mark.parametrize("form", [1, 2, 3, 4])
+def test_every_projection_form_solves_to_the_reference(form):
+    """Each form the autotuner can keep (8, 12, 16 columns per warp; 16 with
+    the pointer table in shared memory), set on the operator, returns the
+    reference's Anderson 64^3 eigenvalues."""
+    g = json.load(open(os.path.join(HERE, "golden", "config_runs.json")))["anderson64_full"]
+    A = ops.anderson_3d(g["L"], W=g["W"], seed=g["pot_seed"])
+    lib = load()
+    with DeviceOperator(A, fmt="sell") as op:
+        assert lib.trlx_operator_set_project_form(op.handle, form) == 0
         r = solve(op, ned=g["ned"], maxlan=g["maxlan"], maxmv=100000, tol=g["tol"], restart=g["restart"],
                   start=ops.start_vector(A.n, seed=g["start_seed"]), mev=g["mev"], device=True)
     assert r.stat == 0 and r.nec >= g["ned"]
@@ -71,3 +89,4 @@ def test_autotune_rejects_operators_it_does_not_tune():
     with DeviceOperator(A, fmt="sell") as op:
         assert lib.trlx_operator_autotune(op.handle, 32, C.byref(res)) == -1
     assert lib.trlx_operator_autotune(None, 32, C.byref(res)) == -1
+    assert lib.trlx_operator_set_project_form(None, 1) == -1

@@ -28,10 +28,13 @@ def small():
     b.close()
 
 
-@pytest.mark.parametrize("threads,fmt", [(256, 0), (512, 0), (1024, 0), (256, 1), (1024, 1)])
-def test_batched_small_against_dense(small, threads, fmt):
+@pytest.mark.parametrize("threads,fmt,cta", [(256, 0, 1024), (512, 0, 1024), (1024, 0, 1024), (256, 1, 1024),
+                                             (1024, 1, 1024), (512, 0, 512), (256, 0, 512), (128, 0, 512),
+                                             (128, 1, 512)])
+def test_batched_small_against_dense(small, threads, fmt, cta):
     Ls, b, diags = small
-    r = b.solve(ned=6, maxlan=24, tol=1e-8, seed=SEED, threads=threads, fmt=fmt)
+    r = b.solve(ned=6, maxlan=24, tol=1e-8, seed=SEED, threads=threads, fmt=fmt, cta=cta)
+    assert r.config.cta_threads == cta
     for p, L in enumerate(Ls):
         stat, nec, mv, nloop = r.info[p]
         assert stat == 0 and nec >= 6, (p, r.info[p])
@@ -98,5 +101,22 @@ def test_batched_large_maxlan_uses_fitting_splits():
             np.testing.assert_allclose(r.eval[p], dense[:16], rtol=1e-10, atol=1e-12)
         with pytest.raises(RuntimeError):
             b.solve(ned=16, maxlan=48, tol=1e-8, seed=SEED, threads=256)
+    finally:
+        b.close()
+
+
+def test_batched_cta_sizes_agree():
+    """The 512-thread CTA form (16-column projection passes, twice the
+    registers) runs the same algorithm as the 1024-thread form: the same
+    eigenvalues to 1e-12 and the same matvec counts, problem by problem."""
+    Ls = [48, 96, 150, 200, 256, 60, 120, 181]
+    b, _ = make_batch(Ls, seed=91)
+    try:
+        r1 = b.solve(ned=8, maxlan=32, tol=1e-8, seed=SEED, threads=512, cta=1024)
+        r2 = b.solve(ned=8, maxlan=32, tol=1e-8, seed=SEED, threads=512, cta=512)
+        assert r1.config.cta_threads == 1024 and r2.config.cta_threads == 512
+        np.testing.assert_allclose(r2.eval, r1.eval, rtol=1e-12)
+        assert np.all(np.abs(r2.info[:, 2] - r1.info[:, 2]) <= 0.02 * r1.info[:, 2] + 2), (r1.info, r2.info)
+        assert np.all(r2.info[:, 1] >= 8)
     finally:
         b.close()

@@ -17,8 +17,8 @@ and run side by side; the B200 build runs on the GPU.
   converged)" too: its check compares the actual error with ten times an
   estimate floored at machine epsilon times the largest value, which
   1e-10-accurate eigenvalues exceed); the two tables agree row by row
-  (Ritz values to 1e-10 relative, actual errors of this build no larger
-  than 10x the reference's largest).
+  (Ritz values within the sum of the two builds' actual errors, actual
+  errors of this build no larger than 10x the reference's largest).
 
 The binaries exist only where the reference sources were available when
 the library was built; without them the test is skipped with that reason.
@@ -102,7 +102,10 @@ def test_reference_complex_example_runs_unchanged(tmp_path):
     assert verdict == verdict_ref and "100 converged" in verdict[0], (verdict, verdict_ref)
     rows, ref_rows = table(ours), table(theirs)
     assert rows.shape == ref_rows.shape == (100, 7)
-    np.testing.assert_allclose(rows[:, 0], ref_rows[:, 0], rtol=1e-10)
+    # both builds' values carry actual errors up to ~1e-9 (their own
+    # "act. error" column): they agree to within the sum of those errors
+    np.testing.assert_allclose(rows[:, 0], ref_rows[:, 0], rtol=1e-13,
+                               atol=np.abs(rows[:, 5]).max() + np.abs(ref_rows[:, 5]).max())
     np.testing.assert_allclose(rows[:, 6], (np.arange(100) + 1.0) ** 2, rtol=1e-3)
     assert np.abs(rows[:, 5]).max() <= 10 * np.abs(ref_rows[:, 5]).max()
     print(f"test_ztrlan: {verdict[0]} in both builds; max |actual error| {np.abs(rows[:, 5]).max():.2e} "
