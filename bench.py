@@ -877,6 +877,8 @@ def main():
     # ---- device-resident arm -------------------------------------------------
     op = DeviceOperator(A, fmt=args.format, maxlan=maxlan)
     fmt_used = op.fmt
+    tuned_form = (1 + ("cpw8", "cpw12", "cpw16", "cpw16_shared_ptrs").index(op.tune["project_form"])
+                  if op.tune else 0)
     config["workload"] = config["workload"].replace("{fmt}", fmt_used.upper())
     if op.tune is not None:
         config["format_choice"] = "autotuned (trlx_operator_autotune)"
@@ -976,6 +978,7 @@ def main():
                 rc = lib.trlx_csr_create(n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, 0, C.byref(handle))
             if rc != 0:
                 raise RuntimeError(f"operator creation from host arrays failed ({rc})")
+            lib.trlx_operator_set_project_form(handle, tuned_form)   # the tuning kept above
             inf = TrlInfo()
             lib.trl_init_info(C.byref(inf), n, maxlan, -1, ned, tol, 1, steps_per_call, None)
             inf.mvparam = handle.value

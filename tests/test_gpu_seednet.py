@@ -227,3 +227,31 @@ def test_tcgen05_convolution_equals_mma_sync(tmp_path, H, W):
     for key in ("Y", "loss"):
         assert _rel(res["tc"][key], res["mma"][key]) <= 1e-6, key
     assert _rel(res["tc"]["g"], res["mma"]["g"]) <= 1e-5
+
+
+def test_row_kernels_match_oracle_directly():
+    """At 64 x 128 the forward pass runs the tcgen05 row convolution
+    (k_conv_rows, W a multiple of 128) and the weight gradient the row-staged
+    tcgen05 kernel (k_wgrad_rows, W a multiple of 64): both against the FP64
+    oracle directly, with the tolerances of the 16 x 64 checks above."""
+    Hr, Wr, B = 64, 128, 2
+    rng = np.random.default_rng(12)
+    V = (-50.0 * rng.random((B, Hr, Wr))).astype(np.float32)
+    U = np.stack([np.linalg.qr(rng.standard_normal((Hr * Wr, NOUT)))[0] for _ in range(B)]).astype(np.float32)
+    p = sn.init_params(13)
+    n = SeedNet(Hr, Wr, max_batch=B)
+    try:
+        n.weights = p.astype(np.float32)
+        Y = n.forward(V)
+        loss, g = n.gradients(V, U, 1.0)
+    finally:
+        n.close()
+    _, Yo = sn.forward(p, V, emulate=True)
+    assert _rel(Y, Yo.reshape(Y.shape)) <= 2e-3
+    lo, go = sn.loss_and_grad(p, V, U, 1.0, emulate=True)
+    np.testing.assert_allclose(loss, lo, rtol=2e-3)
+    for l in range(5):
+        a, b = l * sn.LAYER_LEN, (l + 1) * sn.LAYER_LEN
+        wl = sn.TAPS * sn.NC * sn.NC
+        assert _rel(g[a:a + wl], go[a:a + wl]) <= 2e-2, ("weights", l)
+        assert _rel(g[a + wl:b], go[a + wl:b]) <= 2e-2, ("bias", l)
