@@ -124,68 +124,93 @@ __device__ inline double apply_op(const Params &P, const Problem &pr, const doub
     return block_sum1(a, G);
 }
 
-// h[c] = V[:,c].r (c < m) with r = y - alpha x - beta xp when rec, and r
-// written back into y by the first column pass (the later passes and the
-// update then read one vector instead of three); S.scal[kR2Pre] = |r|^2,
-// S.scal[kH2] = |h|^2.  Rows are taken in pairs with 16-byte loads (basis
-// columns are 256-byte aligned, ld a multiple of 32); an odd last row is
-// handled by thread 0.  Padding rows (n .. ld) are never read.
+// h[c] = V[:,c].r (c < m) with r = y - alpha x - beta xp when rec (r is
+// formed in registers and not stored: the update forms it again and writes
+// it); S.scal[kR2Pre] = |r|^2, S.scal[kH2] = |h|^2.  The columns are cut
+// into chunks of CW; the chunks of a round run side by side, each on its
+// own subgroup of warps sweeping every row, so each row of y (and x, xp) is
+// fetched from memory once per round and found in L1 by the other
+// subgroups, and one reduction covers the whole round.  Rows are taken in
+// pairs with 16-byte loads (basis columns are 256-byte aligned, ld a
+// multiple of 32); an odd last row is handled by the first thread of each
+// subgroup.  Padding rows (n .. ld) are never read.
 __device__ inline double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
 
 template <int CW>
-__device__ inline void project(const double *V, int ld, int n, int m, double *y, bool rec, const double *x,
+__device__ inline void project(const double *V, int ld, int n, int m, const double *y, bool rec, const double *x,
                                const double *xp, double alpha, double beta, const Grp &G) {
     Shared &S = *G.S;
-    double r2 = 0.0;
+    const int lane = G.tid & 31, warp = G.tid >> 5, nw = G.nt >> 5;
     const int np = n >> 1;
-    const bool tail = (n & 1) && G.tid == 0;
-    for (int c0 = 0; c0 < m; c0 += CW) {
+    const int nchunks = (m + CW - 1) / CW;
+    double r2 = 0.0;
+    for (int ch0 = 0; ch0 < max(nchunks, 1); ch0 += nw) {
+        const int nc = max(1, min(nw, nchunks - ch0));  // chunks side by side (one when m == 0)
+        const int wps = nw / nc;                         // warps per subgroup
+        const int sub = warp / wps;
+        const bool act = sub < nc;
+        const int c0 = (ch0 + sub) * CW;
+        const int mm = act ? max(0, min(CW, m - c0)) : 0;
+        const int stride = wps * 32, t = G.tid - sub * stride;
+        const bool count = act && ch0 == 0 && sub == 0;  // one subgroup sums |r|^2
         double acc[CW];
 #pragma unroll
         for (int k = 0; k < CW; ++k) acc[k] = 0.0;
-        const int mm = min(CW, m - c0);
-        const double *Vc = V + (size_t)c0 * ld;
-        for (int p = G.tid; p < np; p += G.nt) {
-            const int i = 2 * p;
-            const double2 yv = ld2(y + i);
-            double r0 = yv.x, r1 = yv.y;
-            if (rec && c0 == 0) {
-                const double2 xv = ld2(x + i), pv = ld2(xp + i);
-                r0 -= alpha * xv.x + beta * pv.x;
-                r1 -= alpha * xv.y + beta * pv.y;
-                *reinterpret_cast<double2 *>(y + i) = make_double2(r0, r1);
-            }
-            if (c0 == 0) {
-                r2 += r0 * r0;
-                r2 += r1 * r1;
-            }
-#pragma unroll
-            for (int k = 0; k < CW; ++k)
-                if (k < mm) {
-                    const double2 v = ld2(Vc + (size_t)k * ld + i);
-                    acc[k] = fma(v.x, r0, acc[k]);
-                    acc[k] = fma(v.y, r1, acc[k]);
+        if (act) {
+            const double *Vc = V + (size_t)c0 * ld;
+            for (int p = t; p < np; p += stride) {
+                const int i = 2 * p;
+                const double2 yv = ld2(y + i);
+                double r0 = yv.x, r1 = yv.y;
+                if (rec) {
+                    const double2 xv = ld2(x + i), pv = ld2(xp + i);
+                    r0 -= alpha * xv.x + beta * pv.x;
+                    r1 -= alpha * xv.y + beta * pv.y;
                 }
-        }
-        if (tail) {
-            const int i = n - 1;
-            double ri = y[i];
-            if (rec && c0 == 0) {
-                ri -= alpha * x[i] + beta * xp[i];
-                y[i] = ri;
-            }
-            if (c0 == 0) r2 += ri * ri;
+                if (count) {
+                    r2 += r0 * r0;
+                    r2 += r1 * r1;
+                }
 #pragma unroll
-            for (int k = 0; k < CW; ++k)
-                if (k < mm) acc[k] = fma(Vc[(size_t)k * ld + i], ri, acc[k]);
+                for (int k = 0; k < CW; ++k)
+                    if (k < mm) {
+                        const double2 v = ld2(Vc + (size_t)k * ld + i);
+                        acc[k] = fma(v.x, r0, acc[k]);
+                        acc[k] = fma(v.y, r1, acc[k]);
+                    }
+            }
+            if ((n & 1) && t == 0) {
+                const int i = n - 1;
+                double ri = y[i];
+                if (rec) ri -= alpha * x[i] + beta * xp[i];
+                if (count) r2 += ri * ri;
+#pragma unroll
+                for (int k = 0; k < CW; ++k)
+                    if (k < mm) acc[k] = fma(Vc[(size_t)k * ld + i], ri, acc[k]);
+            }
         }
-        block_reduce<CW>(acc, &S.h[c0], G);
-    }
-    if (m == 0) {
-        for (int i = G.tid; i < n; i += G.nt) {
-            double ri = y[i];
-            r2 += ri * ri;
+        // Warp partials, then each column summed over its subgroup's warps
+        // in warp order (a fixed order: results do not depend on timing).
+#pragma unroll
+        for (int k = 0; k < CW; ++k) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], o);
         }
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < CW; ++k) S.red[warp][k] = acc[k];
+        }
+        G.sync();
+        if (G.tid < nc * CW) {
+            const int sc = G.tid / CW, k = G.tid - sc * CW;
+            const int c = (ch0 + sc) * CW + k;
+            if (c < m) {
+                double v = 0.0;
+                for (int w = sc * wps; w < (sc + 1) * wps; ++w) v += S.red[w][k];
+                S.h[c] = v;
+            }
+        }
+        G.sync();
     }
     const double s = block_sum1(r2, G);
     if (G.tid == 0) {
@@ -352,7 +377,7 @@ __device__ inline int orth(const Params &P, int pid, double *V, int ld, int n, i
     }
     double beta_new;
     if (usecgs) {
-        update(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, S.h, G);
+        update(V, ld, n, m, r, recur, x, xp, a, beta_prev, S.h, G);  // forms r again and stores it
         double rnrm = sqrt(normrr2);
         const int st = cgs<CW>(P, pid, V, ld, n, m, true, &rnrm, G);
         if (st) return st;
@@ -363,7 +388,7 @@ __device__ inline int orth(const Params &P, int pid, double *V, int ld, int n, i
             for (int c = 0; c < m; ++c) S.g[c] = (c >= m - min(2, m)) ? S.h[c] : 0.0;
         }
         G.sync();
-        update(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, S.g, G);
+        update(V, ld, n, m, r, recur, x, xp, a, beta_prev, S.g, G);
         if (G.tid == 0) S.alpha[jnd - 1] += S.h[m - 1];
         beta_new = sqrt(normrr2);
         G.sync();
