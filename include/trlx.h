@@ -60,7 +60,8 @@ int trlx_operator_nrow(const trlx_operator *op);
    maxlan / 2 columns of the operator's row count in each of the projection
    kernel's forms (median of 5 launches each).  It keeps the faster operator
    form (storage switched in place, the handle stays valid) and the faster
-   projection form for every later solve with this operator.  Temporary
+   projection form for every later solve with this operator (call it
+   before, not during, solves that use the operator).  Temporary
    device memory: two vectors and the projection's columns (at most a
    quarter of the free memory).  Returns 0, -1 for an operator it does not
    tune (complex, SELL-created or distributed), -2 if the temporary memory

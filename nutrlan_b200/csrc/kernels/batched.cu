@@ -125,8 +125,8 @@ __device__ inline double apply_op(const Params &P, const Problem &pr, const doub
 }
 
 // h[c] = V[:,c].r (c < m) with r = y - alpha x - beta xp when rec (r is
-// formed in registers and not stored: the update forms it again and writes
-// it); S.scal[kR2Pre] = |r|^2, S.scal[kH2] = |h|^2.  The columns are cut
+// written back into y by a first pass); S.scal[kR2Pre] = |r|^2,
+// S.scal[kH2] = |h|^2.  The columns are cut
 // into chunks of CW; the chunks of a round run side by side, each on its
 // own subgroup of warps sweeping every row, so each row of y (and x, xp) is
 // fetched from memory once per round and found in L1 by the other
@@ -137,13 +137,26 @@ __device__ inline double apply_op(const Params &P, const Problem &pr, const doub
 __device__ inline double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
 
 template <int CW>
-__device__ inline void project(const double *V, int ld, int n, int m, const double *y, bool rec, const double *x,
+__device__ inline void project(const double *V, int ld, int n, int m, double *y, bool rec, const double *x,
                                const double *xp, double alpha, double beta, const Grp &G) {
     Shared &S = *G.S;
     const int lane = G.tid & 31, warp = G.tid >> 5, nw = G.nt >> 5;
     const int np = n >> 1;
     const int nchunks = (m + CW - 1) / CW;
     double r2 = 0.0;
+    if (rec) {
+        // r = y - alpha x - beta xp written back into y first, so that the
+        // column passes hold no recurrence operands (registers) and the
+        // update reads one vector.
+        for (int p = G.tid; p < np; p += G.nt) {
+            const int i = 2 * p;
+            const double2 yv = ld2(y + i), xv = ld2(x + i), pv = ld2(xp + i);
+            *reinterpret_cast<double2 *>(y + i) =
+                make_double2(yv.x - (alpha * xv.x + beta * pv.x), yv.y - (alpha * xv.y + beta * pv.y));
+        }
+        if ((n & 1) && G.tid == 0) y[n - 1] -= alpha * x[n - 1] + beta * xp[n - 1];
+        G.sync();
+    }
     for (int ch0 = 0; ch0 < max(nchunks, 1); ch0 += nw) {
         const int nc = max(1, min(nw, nchunks - ch0));  // chunks side by side (one when m == 0)
         const int wps = nw / nc;                         // warps per subgroup
@@ -161,12 +174,7 @@ __device__ inline void project(const double *V, int ld, int n, int m, const doub
             for (int p = t; p < np; p += stride) {
                 const int i = 2 * p;
                 const double2 yv = ld2(y + i);
-                double r0 = yv.x, r1 = yv.y;
-                if (rec) {
-                    const double2 xv = ld2(x + i), pv = ld2(xp + i);
-                    r0 -= alpha * xv.x + beta * pv.x;
-                    r1 -= alpha * xv.y + beta * pv.y;
-                }
+                const double r0 = yv.x, r1 = yv.y;
                 if (count) {
                     r2 += r0 * r0;
                     r2 += r1 * r1;
@@ -181,8 +189,7 @@ __device__ inline void project(const double *V, int ld, int n, int m, const doub
             }
             if ((n & 1) && t == 0) {
                 const int i = n - 1;
-                double ri = y[i];
-                if (rec) ri -= alpha * x[i] + beta * xp[i];
+                const double ri = y[i];
                 if (count) r2 += ri * ri;
 #pragma unroll
                 for (int k = 0; k < CW; ++k)
@@ -377,7 +384,7 @@ __device__ inline int orth(const Params &P, int pid, double *V, int ld, int n, i
     }
     double beta_new;
     if (usecgs) {
-        update(V, ld, n, m, r, recur, x, xp, a, beta_prev, S.h, G);  // forms r again and stores it
+        update(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, S.h, G);
         double rnrm = sqrt(normrr2);
         const int st = cgs<CW>(P, pid, V, ld, n, m, true, &rnrm, G);
         if (st) return st;
@@ -388,7 +395,7 @@ __device__ inline int orth(const Params &P, int pid, double *V, int ld, int n, i
             for (int c = 0; c < m; ++c) S.g[c] = (c >= m - min(2, m)) ? S.h[c] : 0.0;
         }
         G.sync();
-        update(V, ld, n, m, r, recur, x, xp, a, beta_prev, S.g, G);
+        update(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, S.g, G);
         if (G.tid == 0) S.alpha[jnd - 1] += S.h[m - 1];
         beta_new = sqrt(normrr2);
         G.sync();
@@ -721,12 +728,11 @@ __device__ void solve(const Params &P, int pid, const Grp &G, double *dyn, long 
 // Phases run largest problems first; in phase f the CTA is split into
 // groups of P.phase_threads[f] threads, each group taking problems from the
 // phase's queue until it is empty, then the whole CTA moves on.
-// CTA: threads per CTA.  The 1024-thread form has 64 registers per thread
-// and projects 8 basis columns per pass over r; the 512-thread form has up
-// to 128 and projects 16, reading r half as often.
-template <int CTA>
+// CTA: threads per CTA; CW: basis columns per projection pass.  The
+// 1024-thread form has 64 registers per thread (CW 8 or 4); the 512-thread
+// form has up to 128 (CW 16).
+template <int CTA, int CW>
 __global__ void __launch_bounds__(CTA, 1) k_batched(Params P) {
-    constexpr int CW = CTA >= 1024 ? 8 : 16;
     extern __shared__ __align__(16) unsigned char smem[];
     for (int f = 0; f < P.nphases; ++f) {
         const int nt = P.phase_threads[f];
@@ -776,34 +782,48 @@ static size_t launch_smem(int maxlan, int min_threads, int cta) {
     return std::max(smem_bytes(maxlan, min_threads, cta), want);
 }
 
-template <int CTA>
+// Columns per projection pass of the 1024-thread form: 8, or 4 under
+// TRLX_BATCH_CW=4 (tuning only; fewer live registers under the 64-register
+// cap).  The 512-thread form uses 16.
+static int cw1024() {
+    static const int cw = [] {
+        const char *e = std::getenv("TRLX_BATCH_CW");
+        return (e && std::atoi(e) == 4) ? 4 : 8;
+    }();
+    return cw;
+}
+
+template <int CTA, int CW>
 static int launch_cta(const Params &P, int blocks, cudaStream_t st) {
     int min_threads = CTA;
     for (int f = 0; f < P.nphases; ++f) min_threads = std::min(min_threads, P.phase_threads[f]);
     const size_t sm = launch_smem(P.maxlan, min_threads, CTA);
-    if (cudaFuncSetAttribute(k_batched<CTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_batched<CTA, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
+        cudaSuccess)
         return -1001;
     Params Q = P;
     Q.smem_total = sm;
-    k_batched<CTA><<<blocks, CTA, sm, st>>>(Q);
+    k_batched<CTA, CW><<<blocks, CTA, sm, st>>>(Q);
     return cudaGetLastError() == cudaSuccess ? 0 : -1001;
 }
 
 int launch(const Params &P, int blocks, cudaStream_t st) {
-    return P.cta == 512 ? launch_cta<512>(P, blocks, st) : launch_cta<1024>(P, blocks, st);
+    if (P.cta == 512) return launch_cta<512, 16>(P, blocks, st);
+    return cw1024() == 4 ? launch_cta<1024, 4>(P, blocks, st) : launch_cta<1024, 8>(P, blocks, st);
 }
 
-template <int CTA>
+template <int CTA, int CW>
 static int blocks_per_sm(int min_threads, int maxlan) {
     int nb = 0;
     const size_t sm = launch_smem(maxlan, min_threads, CTA);
-    cudaFuncSetAttribute(k_batched<CTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batched<CTA>, CTA, sm) != cudaSuccess) return 1;
+    cudaFuncSetAttribute(k_batched<CTA, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batched<CTA, CW>, CTA, sm) != cudaSuccess) return 1;
     return std::max(nb, 1);
 }
 
 int max_blocks_per_sm(int min_threads, int maxlan, int cta) {
-    return cta == 512 ? blocks_per_sm<512>(min_threads, maxlan) : blocks_per_sm<1024>(min_threads, maxlan);
+    if (cta == 512) return blocks_per_sm<512, 16>(min_threads, maxlan);
+    return cw1024() == 4 ? blocks_per_sm<1024, 4>(min_threads, maxlan) : blocks_per_sm<1024, 8>(min_threads, maxlan);
 }
 
 }  // namespace batched
