@@ -44,7 +44,7 @@ struct Shared {
 
 // A group of threads of the CTA that solves one problem: its rank, size,
 // named-barrier id and shared state.  The CTA is split into 1, 2 or 4
-// groups per phase (1024, 512 or 256 threads).
+// groups per phase.
 struct Grp {
     int tid, nt, bar;
     Shared *S;
@@ -746,7 +746,10 @@ __global__ void __launch_bounds__(CTA, 1) k_batched(Params P) {
         const long tile_cap =
             (long)((per_group - head) / sizeof(double)) - 2L * P.maxlan * P.maxlan;
         if (gidx < ngroups) {
-            Grp G{(int)threadIdx.x - gidx * nt, nt, 1 + gidx,
+            // Barrier ids by split level (1 for the whole CTA, 2-3 for
+            // halves, 4-7 for quarters, 8-15 for eighths), so groups of
+            // different phases never share one.
+            Grp G{(int)threadIdx.x - gidx * nt, nt, ngroups + gidx,
                   reinterpret_cast<Shared *>(smem + gidx * per_group)};
             double *dyn = reinterpret_cast<double *>(smem + gidx * per_group + (sizeof(Shared) + 15) / 16 * 16);
             for (;;) {
@@ -758,7 +761,12 @@ __global__ void __launch_bounds__(CTA, 1) k_batched(Params P) {
                 solve<CW>(P, P.order[q], G, dyn, tile_cap);
             }
         }
-        __syncthreads();
+        // When the next phase splits each group further (or not at all),
+        // its groups are made of this group's threads and shared memory
+        // (equal shares nest), so a group goes on without waiting for the
+        // rest of the CTA; a coarser next phase needs the whole CTA.
+        const bool nested = f + 1 < P.nphases && nt % P.phase_threads[f + 1] == 0;
+        if (!nested) __syncthreads();
     }
 }
 
