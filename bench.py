@@ -210,6 +210,18 @@ def run_batched_reference(args, w, world, rank):
                               "d2h_bytes_per_step": 0}}), flush=True)
 
 
+def batched_alg_bytes(info, Ls, w):
+    """Algorithmic bytes of one batched solve: per matvec the stencil's x, y
+    and diagonal (3 vectors), a Gram-Schmidt pass reading the basis twice at
+    the cycle's average size (3/4 maxlan columns) and the recurrence
+    vectors (4); per restart the Ritz recombination, reading jml <= maxlan
+    columns and writing kept >= ned.  Returns (total, steps only)."""
+    sizes = Ls.astype(np.int64) ** 2
+    steps = float(np.sum(info[:, 2] * sizes * 8 * (3 + 2 * 0.75 * w["maxlan"] + 4)))
+    restarts = float(np.sum(info[:, 3] * sizes * 8 * (w["maxlan"] + w["ned"])))
+    return steps + restarts, steps
+
+
 def batched_record(w, rank, solves=2):
     """The batched configuration measured inside the default line: one
     autotuned persistent launch per solve of all `count` problems, timed with
@@ -232,15 +244,16 @@ def batched_record(w, rank, solves=2):
         e1.record()
         torch.cuda.synchronize()
         dt = e0.elapsed_time(e1) * 1e-3 / solves
-        sizes = Ls.astype(np.int64) ** 2
-        alg = float(np.sum(r.info[:, 2] * sizes * 8 * (3 + 2 * 0.75 * w["maxlan"] + 4)))
+        alg, alg_steps = batched_alg_bytes(r.info, Ls, w)
         peak, kind = read_peaks()
         return {"workload": f"batched{w['count']}: L~U[48,256], 5-pt Laplacian + U[0,2] diag, ned={w['ned']}, "
                             f"maxlan={w['maxlan']}, tol={w['tol']}, one persistent launch per solve",
                 "problems_per_s": w["count"] / dt, "ms_per_solve": 1e3 * dt, "solves_timed": solves,
                 "solved": int(np.sum((r.info[:, 0] == 0) & (r.info[:, 1] >= w["ned"]))),
-                "matvecs_total": int(np.sum(r.info[:, 2])), "alg_GBps": alg / dt / 1e9,
-                "hbm_frac": alg / dt / 1e9 / peak, "peak_source": kind,
+                "matvecs_total": int(np.sum(r.info[:, 2])), "restarts_total": int(np.sum(r.info[:, 3])),
+                "alg_GBps": alg / dt / 1e9, "hbm_frac": alg / dt / 1e9 / peak, "peak_source": kind,
+                "alg_GBps_steps_only": alg_steps / dt / 1e9,
+                "alg_bytes": "per matvec (3 + 2 * 0.75 maxlan + 4) * 8 n, per restart (maxlan + ned) * 8 n",
                 "autotune": {"bucket_threads": list(cfg.bucket_threads), "bucket_format": list(cfg.bucket_format),
                              "cta_threads": cfg.cta_threads, "seconds": t_tune}}
     finally:
@@ -280,12 +293,7 @@ def run_batched(args, w, world, rank, local, pg):
     solved = int(np.sum((r.info[:, 0] == 0) & (r.info[:, 1] >= w["ned"])))
     n_total = int(np.sum(Ls.astype(np.int64) ** 2))
     matvecs = int(np.sum(r.info[:, 2]))
-    # Algorithmic bytes of one batch solve: per matvec, stencil (x, y, diag) +
-    # one Gram-Schmidt pass over the current basis (average size ~ 3/4 maxlan
-    # across a thick-restart cycle) read twice.
-    avg_cols = 0.75 * w["maxlan"]
-    sizes = Ls.astype(np.int64) ** 2
-    alg_bytes = float(np.sum(r.info[:, 2] * sizes * 8 * (3 + 2 * avg_cols + 4)))
+    alg_bytes, _ = batched_alg_bytes(r.info, Ls, w)   # steps + restart recombinations
     value = count * world * args.steps / dt
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -366,7 +374,9 @@ def run_complex(args, w, world, rank, local, pg):
     from nutrlan_b200 import load, TrlInfo, TrlxOptions, TrlxStats, DeviceOperator
     lib = load()
     mev = ned + 1
-    op = DeviceOperator(A)
+    op = DeviceOperator(A, fmt="auto", maxlan=maxlan)        # tunes the projection form
+    tuned_form = 1 + ("cpw8", "cpw12", "cpw16", "cpw16_shared_ptrs").index(op.tune["project_form"])
+    config["autotune"] = op.tune
     evec = torch.zeros((mev, n), dtype=torch.complex128, device=dev)
     x0_dev = torch.as_tensor(x0, device=dev)
     eval_ = np.zeros(mev)
@@ -444,6 +454,7 @@ def run_complex(args, w, world, rank, local, pg):
         def e2e_call():
             h = C.c_void_p()
             lib.trlx_zcsr_create(n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, 0, C.byref(h))
+            lib.trlx_operator_set_project_form(h, tuned_form)
             hev[0] = x0
             mv = call(TrlInfo(), opts, maxlan, hev.ctypes.data, h.value, op.applier)
             lib.trlx_operator_destroy(h)

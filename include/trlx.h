@@ -58,13 +58,15 @@ int trlx_operator_nrow(const trlx_operator *op);
    product y = A x + alpha in the CSR form and in the SELL-C-32 form built
    from the same device arrays, and one Gram-Schmidt projection over
    maxlan / 2 columns of the operator's row count in each of the projection
-   kernel's forms (median of 5 launches each).  It keeps the faster operator
+   kernel's forms (median of 5 launches each); for a complex operator
+   (trlx_zcsr_create) only the projection forms 3 and 4 (the others report
+   -1 ms).  It keeps the faster operator
    form (storage switched in place, the handle stays valid) and the faster
    projection form for every later solve with this operator (call it
    before, not during, solves that use the operator).  Temporary
    device memory: two vectors and the projection's columns (at most a
    quarter of the free memory).  Returns 0, -1 for an operator it does not
-   tune (complex, SELL-created or distributed), -2 if the temporary memory
+   tune (SELL-created or distributed), -2 if the temporary memory
    cannot be allocated, -3 on a CUDA error. */
 typedef struct {
     int format;            /* kept operator form: 0 CSR, 1 SELL-C-32        */

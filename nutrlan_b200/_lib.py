@@ -52,8 +52,9 @@ class TrlxTuneResult(C.Structure):
 
     def as_dict(self):
         return {"format": ("csr", "sell")[self.format], "project_form": self.FORMS[self.project_form - 1],
+                "spmv_forms_timed": 2 if self.spmv_ms[1] >= 0 else 1,
                 "spmv_ms": {"csr": self.spmv_ms[0], "sell": self.spmv_ms[1]},
-                "project_ms": {f: self.project_ms[i] for i, f in enumerate(self.FORMS)},
+                "project_ms": {f: self.project_ms[i] for i, f in enumerate(self.FORMS) if self.project_ms[i] >= 0},
                 "columns": self.columns, "seconds": self.seconds}
 
 

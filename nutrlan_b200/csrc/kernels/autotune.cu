@@ -93,7 +93,10 @@ void move_storage(trlx_operator *dst, trlx_operator *src) {
 extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_result *out) {
     if (!A || !out) return -1;
     *out = trlx_tune_result{};
-    if (A->kind != 0 || A->halo) return -1;  // tunes real CSR-created, undistributed operators
+    // Real CSR-created or complex CSR operators, not distributed ones.
+    if ((A->kind != 0 && A->kind != 2) || A->halo) return -1;
+    const bool cplx = A->kind == 2;
+    const int vw = cplx ? 2 : 1;  // doubles per vector element
     const auto t0 = std::chrono::steady_clock::now();
     int prev = 0;
     cudaGetDevice(&prev);
@@ -109,14 +112,14 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
     s.max_blocks = 148 * 8;
     s.max_cols = m;
     DevBuf x, y, part, tick, dsc, basis, table;
-    const size_t vec = sizeof(double) * (size_t)n_pad;
+    const size_t vec = sizeof(double) * vw * (size_t)n_pad;
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     // The projection is timed over m columns when they fit in a quarter of
     // the free memory, else over as many as fit (at least 8).
     int mp = (int)std::min<size_t>((size_t)m, free_b / 4 / std::max<size_t>(vec, 1));
     if (mp < 8 || !x.alloc(vec) || !y.alloc(vec) || !part.alloc((size_t)s.max_blocks * (m + 2) * 16) ||
-        !tick.alloc(sizeof(unsigned) * trlb::kNumTickets) || !dsc.alloc(sizeof(double) * (m + 4)) ||
+        !tick.alloc(sizeof(unsigned) * trlb::kNumTickets) || !dsc.alloc(sizeof(double) * vw * (m + 4)) ||
         !basis.alloc(vec * mp) || !table.alloc(sizeof(double *) * mp)) {
         rc = -2;
     }
@@ -125,14 +128,43 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
         s.partials = part.p;
         s.tickets = static_cast<unsigned *>(tick.p);
         cudaMemsetAsync(tick.p, 0, sizeof(unsigned) * trlb::kNumTickets, st);
-        k_fill_pattern<<<592, 256, 0, st>>>(static_cast<double *>(x.p), n, n_pad, 1u);
+        // Complex vectors are filled as interleaved (re, im) doubles.
+        k_fill_pattern<<<592, 256, 0, st>>>(static_cast<double *>(x.p), vw * n, vw * n_pad, 1u);
         for (int c = 0; c < mp; ++c)
-            k_fill_pattern<<<592, 256, 0, st>>>(static_cast<double *>(basis.p) + (size_t)c * n_pad, n, n_pad,
-                                                 7u + c);
+            k_fill_pattern<<<592, 256, 0, st>>>(static_cast<double *>(basis.p) + (size_t)c * vw * n_pad, vw * n,
+                                                 vw * n_pad, 7u + c);
         std::vector<double *> cols(mp);
-        for (int c = 0; c < mp; ++c) cols[c] = static_cast<double *>(basis.p) + (size_t)c * n_pad;
+        for (int c = 0; c < mp; ++c) cols[c] = static_cast<double *>(basis.p) + (size_t)c * vw * n_pad;
         cudaMemcpyAsync(table.p, cols.data(), sizeof(double *) * mp, cudaMemcpyHostToDevice, st);
         cudaStreamSynchronize(st);
+    }
+    if (!rc && cplx) {
+        // Complex CSR: one operator form; the projection keeps its pointer
+        // table in registers (form 3) or in shared memory (form 4).
+        using trlb::zd;
+        double *alpha = static_cast<double *>(dsc.p);
+        out->format = 0;
+        out->spmv_ms[0] = median_ms(
+            [&] { trlb::spmv_fused_cplx(A, static_cast<zd *>(x.p), static_cast<zd *>(y.p), n_pad, alpha, &s, st); },
+            st);
+        out->spmv_ms[1] = -1.0;
+        trlb::Recur<zd> none;
+        out->project_ms[0] = out->project_ms[1] = -1.0;
+        for (int k = 2; k < 4; ++k) {
+            out->project_ms[k] = median_ms(
+                [&] {
+                    trlb::launch_project<zd>(static_cast<zd *const *>(table.p), mp, n_pad,
+                                             static_cast<const zd *>(x.p), none, static_cast<zd *>(dsc.p),
+                                             static_cast<double *>(dsc.p) + 2 * (m + 1), s, st, trlb::kProject8 + k);
+                },
+                st);
+        }
+        const int best = out->project_ms[3] < out->project_ms[2] ? trlb::kProject16Shared : trlb::kProject16;
+        A->project_form = best;
+        out->project_form = best;
+        out->columns = mp;
+        if (cudaStreamSynchronize(st) != cudaSuccess) rc = -3;
+    } else if (!rc) {
         // ---- operator form ----------------------------------------------
         double *alpha = static_cast<double *>(dsc.p);
         out->spmv_ms[0] = median_ms(

@@ -710,7 +710,13 @@ void launch_project(T *const *cols, int m, long n_pad, const typename Store<T>::
         else
             args(k_project<T, 16>);
     } else {
-        args(k_project<T, proj_cpw<T>()>);
+        // Complex storage: 8 columns per warp, the pointer table in
+        // registers (default) or in shared memory (kProject16Shared, three
+        // blocks per SM).
+        if (form_req == kProject16Shared)
+            args(k_project<T, proj_cpw<T>(), true>);
+        else
+            args(k_project<T, proj_cpw<T>()>);
     }
 }
 

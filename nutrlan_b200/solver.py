@@ -26,9 +26,10 @@ class DeviceOperator:
     """A trlx_operator (CSR, SELL-C-32 or complex CSR) resident on the GPU.
 
     ``fmt="auto"`` creates the CSR form and runs trlx_operator_autotune
-    (``maxlan`` sets the projection width it times): the operator keeps the
-    faster of CSR and SELL-C-32 and the faster projection kernel for its
-    solves; ``self.tune`` holds what was measured."""
+    (``maxlan`` sets the projection width it times): a real operator keeps
+    the faster of CSR and SELL-C-32, and every operator the faster
+    projection kernel form for its solves; ``self.tune`` holds what was
+    measured."""
 
     def __init__(self, csr, fmt="csr", sigma=1, maxlan=128):
         lib = load()
@@ -57,7 +58,7 @@ class DeviceOperator:
         if rc != 0:
             raise RuntimeError(f"trlx operator creation failed ({rc})")
         self.fmt = "zcsr" if self.complex else fmt
-        if auto and not self.complex:
+        if auto:
             res = TrlxTuneResult()
             rc = lib.trlx_operator_autotune(self.handle, int(maxlan), C.byref(res))
             if rc != 0:

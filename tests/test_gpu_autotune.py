@@ -1,5 +1,5 @@
 """Single-solve autotuner (trlx_operator_autotune): it keeps the faster of
-the measured CSR / SELL-C-32 forms and of the measured projection widths,
+the measured CSR / SELL-C-32 forms and of the measured projection forms,
 the tuned operator computes the same product, and a solve with it returns
 the reference's eigenvalues (the golden Anderson 64^3 run of
 tests/golden/config_runs.json) like the untuned CSR operator does."""
@@ -79,12 +79,35 @@ def test_every_projection_form_solves_to_the_reference(form):
     assert abs(r.info.matvec - g["matvec"]) <= 0.05 * g["matvec"]
 
 
+@pytest.mark.parametrize("form", [0, 3, 4])
+def test_complex_autotune_and_forms_solve_to_the_reference(form):
+    """A complex operator tunes only its projection form (pointer table in
+    registers or in shared memory); with each form, and with the tuned one,
+    the Peierls 256^2 solve returns the reference's eigenvalues."""
+    g = json.load(open(os.path.join(HERE, "golden", "config_runs.json")))["peierls256_full"]
+    P = ops.peierls_2d(g["L"], phi=g["phi"], W=g["W"], seed=g["pot_seed"])
+    lib = load()
+    fmt = "auto" if form == 0 else "csr"
+    with DeviceOperator(P, fmt=fmt, maxlan=g["maxlan"]) as op:
+        if form == 0:
+            t = op.tune
+            print(t)
+            assert t["spmv_forms_timed"] == 1 and set(t["project_ms"]) == {"cpw16", "cpw16_shared_ptrs"}
+            assert t["project_ms"][t["project_form"]] == min(t["project_ms"].values())
+        else:
+            assert lib.trlx_operator_set_project_form(op.handle, form) == 0
+        x0 = ops.start_vector(P.n) + 1j * ops.start_vector(P.n, seed=99)
+        r = solve(op, ned=g["ned"], maxlan=g["maxlan"], maxmv=100000, tol=g["tol"], restart=g["restart"],
+                  start=x0, mev=g["mev"], device=True)
+    assert r.stat == 0 and r.nec >= g["ned"]
+    got, want = np.sort(r.eval[:g["ned"]]), np.sort(np.array(g["eval"])[:g["ned"]])
+    assert np.max(np.abs(got - want) / np.abs(want)) <= 1e-10
+    assert abs(r.info.matvec - g["matvec"]) <= 0.05 * g["matvec"]
+
+
 def test_autotune_rejects_operators_it_does_not_tune():
     lib = load()
     res = TrlxTuneResult()
-    P = ops.peierls_2d(16, phi=1.0 / 16.0)
-    with DeviceOperator(P) as op:
-        assert lib.trlx_operator_autotune(op.handle, 32, C.byref(res)) == -1
     A = ops.laplacian_2d(32)
     with DeviceOperator(A, fmt="sell") as op:
         assert lib.trlx_operator_autotune(op.handle, 32, C.byref(res)) == -1
