@@ -37,7 +37,7 @@ struct Shared {
     trl_info info;
     double alpha[kMaxL + 2], beta[kMaxL + 2], alfrot[kMaxL + 2], betrot[kMaxL + 2];
     double lambda[kMaxL + 2], res[kMaxL + 2], h[kMaxL + 2], g[kMaxL + 2], wrk2[2 * (kMaxL + 2)];
-    double red[32][16];
+    double red[32][17];
     double scal[8];
     int ctl[8];
 };
@@ -125,8 +125,8 @@ __device__ inline double apply_op(const Params &P, const Problem &pr, const doub
 }
 
 // h[c] = V[:,c].r (c < m) with r = y - alpha x - beta xp when rec (r is
-// written back into y by a first pass); S.scal[kR2Pre] = |r|^2,
-// S.scal[kH2] = |h|^2.  The columns are cut
+// written back into y by a first pass); returns |r|^2 and |h|^2 to every
+// thread of the group.  The columns are cut
 // into chunks of CW; the chunks of a round run side by side, each on its
 // own subgroup of warps sweeping every row, so each row of y (and x, xp) is
 // fetched from memory once per round and found in L1 by the other
@@ -136,14 +136,18 @@ __device__ inline double apply_op(const Params &P, const Problem &pr, const doub
 // subgroup.  Padding rows (n .. ld) are never read.
 __device__ inline double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
 
+struct Norms {
+    double r2, h2;  // |r|^2 and |h|^2 of a projection
+};
+
 template <int CW>
-__device__ inline void project(const double *V, int ld, int n, int m, double *y, bool rec, const double *x,
-                               const double *xp, double alpha, double beta, const Grp &G) {
+__device__ inline Norms project(const double *V, int ld, int n, int m, double *y, bool rec, const double *x,
+                                const double *xp, double alpha, double beta, const Grp &G) {
     Shared &S = *G.S;
     const int lane = G.tid & 31, warp = G.tid >> 5, nw = G.nt >> 5;
     const int np = n >> 1;
     const int nchunks = (m + CW - 1) / CW;
-    double r2 = 0.0;
+    double r2 = 0.0, r2tot = 0.0;
     if (rec) {
         // r = y - alpha x - beta xp written back into y first, so that the
         // column passes hold no recurrence operands (registers) and the
@@ -197,15 +201,20 @@ __device__ inline void project(const double *V, int ld, int n, int m, double *y,
             }
         }
         // Warp partials, then each column summed over its subgroup's warps
-        // in warp order (a fixed order: results do not depend on timing).
+        // in warp order (a fixed order: results do not depend on timing);
+        // |r|^2 rides along in slot CW of the first round.
 #pragma unroll
         for (int k = 0; k < CW; ++k) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], o);
         }
+        double r2w = r2;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r2w += __shfl_down_sync(0xffffffffu, r2w, o);
         if (lane == 0) {
 #pragma unroll
             for (int k = 0; k < CW; ++k) S.red[warp][k] = acc[k];
+            S.red[warp][CW] = r2w;
         }
         G.sync();
         if (G.tid < nc * CW) {
@@ -217,22 +226,22 @@ __device__ inline void project(const double *V, int ld, int n, int m, double *y,
                 S.h[c] = v;
             }
         }
+        if (ch0 == 0) {  // every thread forms the same total, in warp order
+            r2tot = 0.0;
+            for (int w = 0; w < nw; ++w) r2tot += S.red[w][CW];
+        }
         G.sync();
     }
-    const double s = block_sum1(r2, G);
-    if (G.tid == 0) {
-        S.scal[kR2Pre] = s;
-        double h2 = 0.0;
-        for (int c = 0; c < m; ++c) h2 += S.h[c] * S.h[c];
-        S.scal[kH2] = h2;
-    }
-    G.sync();
+    double h2 = 0.0;
+    for (int c = 0; c < m; ++c) h2 += S.h[c] * S.h[c];
+    return Norms{r2tot, h2};
 }
 
-// r = (y - alpha x - beta xp) - V h (in place in y); S.scal[kR2] = |r|^2.
+// r = (y - alpha x - beta xp) - V h (in place in y); returns |r|^2 to every
+// thread (the reduction's barriers also publish the new y).
 // Row pairs as in project; the column loop issues eight 16-byte loads before
 // their FMAs (each element's FMA chain keeps the column order).
-__device__ inline void update(const double *V, int ld, int n, int m, double *y, bool rec, const double *x,
+__device__ inline double update(const double *V, int ld, int n, int m, double *y, bool rec, const double *x,
                               const double *xp, double alpha, double beta, const double *h, const Grp &G) {
     constexpr int UC = 8;
     Shared &S = *G.S;
@@ -275,9 +284,7 @@ __device__ inline void update(const double *V, int ld, int n, int m, double *y, 
         y[i] = ri;
         r2 += ri * ri;
     }
-    const double s = block_sum1(r2, G);
-    if (G.tid == 0) S.scal[kR2] = s;
-    G.sync();
+    return block_sum1(r2, G);
 }
 
 __device__ inline void scale(double *y, int n, double sc, const Grp &G) {
@@ -307,8 +314,10 @@ __device__ inline void random_vector(double *y, int n, uint64_t seed, const Grp 
 // after a first pass whose scalars are in S.scal (trl_cgs,
 // SRC/trlcore.c:2913-3117).  Returns the status; *rnrm the final norm.
 template <int CW>
-__device__ inline int cgs(const Params &P, int pid, double *V, int ld, int n, int m, bool pass_done, double *rnrm,
-                          const Grp &G) {
+// pass_done: the first pass was made by the caller, whose |h|^2 and |r|^2
+// are h2_done and r2_done.
+__device__ inline int cgs(const Params &P, int pid, double *V, int ld, int n, int m, bool pass_done, double h2_done,
+                          double r2_done, double *rnrm, const Grp &G) {
     Shared &S = *G.S;
     double *r = V + (size_t)m * ld;
     const int maxorth = 3;
@@ -318,14 +327,15 @@ __device__ inline int cgs(const Params &P, int pid, double *V, int ld, int n, in
         bool first = true;
         while (cnt <= maxorth) {
             if (!(first && pass_done)) {
-                project<CW>(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, G);
-                update(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, S.h, G);
+                normdiff2 = project<CW>(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, G).h2;
+                normrr2 = update(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, S.h, G);
+            } else {
+                normdiff2 = h2_done;
+                normrr2 = r2_done;
             }
             first = false;
             if (G.tid == 0) S.info.north++;
             cnt++;
-            normdiff2 = S.scal[kH2];
-            normrr2 = S.scal[kR2];
             *rnrm = sqrt(normrr2);
             if (DBL_EPSILON * normrr2 > normdiff2) break;
             if ((cnt > 1 && (m * DBL_EPSILON * DBL_EPSILON * (normrr2 + normdiff2) < normdiff2)) ||
@@ -353,15 +363,14 @@ __device__ inline int cgs(const Params &P, int pid, double *V, int ld, int n, in
 // S.alpha, the recurrence uses beta_prev; sets S.beta[m-1].
 template <int CW>
 __device__ inline int orth(const Params &P, int pid, double *V, int ld, int n, int m, bool recur, double beta_prev,
-                           int kept, const Grp &G) {
+                           double a, int kept, const Grp &G) {
     Shared &S = *G.S;
     const int jnd = m, jm1 = jnd - 1;
     double *r = V + (size_t)m * ld;
     const double *x = V + (size_t)(m - 1) * ld;
     const double *xp = m >= 2 ? V + (size_t)(m - 2) * ld : nullptr;
-    const double a = S.alpha[jnd - 1];
-    project<CW>(V, ld, n, m, r, recur, x, xp, a, beta_prev, G);
-    const double normrr2 = S.scal[kR2Pre];
+    const Norms pn = project<CW>(V, ld, n, m, r, recur, x, xp, a, beta_prev, G);
+    const double normrr2 = pn.r2;
     if (!(normrr2 >= 0.0) || !(normrr2 <= DBL_MAX)) return -102;
     double tmp = a * a;
     // beta of the previous steps are in S.beta (thread-uniform reads).
@@ -384,9 +393,9 @@ __device__ inline int orth(const Params &P, int pid, double *V, int ld, int n, i
     }
     double beta_new;
     if (usecgs) {
-        update(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, S.h, G);
+        const double r2u = update(V, ld, n, m, r, false, nullptr, nullptr, 0.0, 0.0, S.h, G);
         double rnrm = sqrt(normrr2);
-        const int st = cgs<CW>(P, pid, V, ld, n, m, true, &rnrm, G);
+        const int st = cgs<CW>(P, pid, V, ld, n, m, true, pn.h2, r2u, &rnrm, G);
         if (st) return st;
         beta_new = rnrm;
     } else {
@@ -531,7 +540,7 @@ __device__ void solve(const Params &P, int pid, const Grp &G, double *dyn, long 
         }
         G.sync();
         update(V, ld, n, jnd, V + (size_t)jnd * ld, false, nullptr, nullptr, 0.0, 0.0, S.beta, G);
-        stat = orth<CW>(P, pid, V, ld, n, jnd, false, 0.0, kept, G);
+        stat = orth<CW>(P, pid, V, ld, n, jnd, false, 0.0, a, kept, G);
         if (stat) break;
         if (G.tid < 32) {
             const int lane = G.tid;
@@ -548,12 +557,11 @@ __device__ void solve(const Params &P, int pid, const Grp &G, double *dyn, long 
         while (jnd < info->klan && info->nec < info->ned) {
             jnd++;
             a = apply_op(P, pr, V + (size_t)(jnd - 1) * ld, V + (size_t)jnd * ld, G);
-            if (G.tid == 0) {
+            if (G.tid == 0) {  // published by the projection's first barrier
                 info->matvec++;
                 S.alpha[jnd - 1] = a;
             }
-            G.sync();
-            stat = orth<CW>(P, pid, V, ld, n, jnd, true, S.beta[jnd - 2], kept, G);
+            stat = orth<CW>(P, pid, V, ld, n, jnd, true, S.beta[jnd - 2], a, kept, G);
             if (G.tid == 0) {
                 S.alfrot[jnd - 1] = S.alpha[jnd - 1];
                 S.betrot[jnd - 1] = S.beta[jnd - 1];
