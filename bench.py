@@ -203,7 +203,9 @@ def run_batched_reference(args, w, world, rank):
                       "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                       "data": "synthetic (seeded)",
                       "config": {"workload": f"batched{count}: L~U[48,256], 5-pt Laplacian + U[0,2] diag, "
-                                             f"ned={w['ned']}, maxlan={w['maxlan']}, tol={w['tol']}"},
+                                             f"ned={w['ned']}, maxlan={w['maxlan']}, tol={w['tol']}; sample per "
+                                             f"step: {probs[0]} problems of the batch spread over the size range, "
+                                             "solved one after another by reference trlan"},
                       "cpu_baseline": {"value": val, "unit": "problems/s", "cores": os.cpu_count(),
                                        "kind": "reference", "sample": sample},
                       "e2e": {"value": val, "unit": "problems/s", "h2d_bytes_per_step": 0,
@@ -357,11 +359,15 @@ def run_complex(args, w, world, rank, local, pg):
                 times.append(dt)
                 mvs.append(mv)
         val = sum(mvs) / sum(times)
+        ref_config = dict(config, workload=config["workload"].replace(
+            "complex CSR, basis c128, one thick-restart cycle/step",
+            f"complex CSR callback (OpenMP) + OpenBLAS; sample per step: the first {cpu_sample} Lanczos steps "
+            f"of the same solve (maxlan=maxmv={cpu_sample}, reference ztrlan)"))
         print(json.dumps({"impl": "reference", "metric": metric, "value": val, "unit": "steps/s",
                           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                           "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
                           "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-                          "config": config,
+                          "config": ref_config,
                           "cpu_baseline": {"value": val, "unit": "steps/s", "cores": os.cpu_count(),
                                            "kind": "reference", "sample": cpu_desc},
                           "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0,
