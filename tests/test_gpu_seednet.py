@@ -231,9 +231,10 @@ def test_tcgen05_convolution_equals_mma_sync(tmp_path, H, W):
 
 def test_row_kernels_match_oracle_directly():
     """At 64 x 128 the forward pass runs the tcgen05 row convolution
-    (k_conv_rows, W a multiple of 128) and the weight gradient the row-staged
-    tcgen05 kernel (k_wgrad_rows, W a multiple of 64): both against the FP64
-    oracle directly, with the tolerances of the 16 x 64 checks above."""
+    (k_conv_rows, W a multiple of 128; at 16 x 64 the nine-tap form runs) and
+    the weight gradient the row-staged tcgen05 kernel (k_wgrad_rows, W a
+    multiple of 64): both against the FP64 oracle directly, with the
+    tolerances of the 16 x 64 checks above."""
     Hr, Wr, B = 64, 128, 2
     rng = np.random.default_rng(12)
     V = (-50.0 * rng.random((B, Hr, Wr))).astype(np.float32)
