@@ -476,7 +476,7 @@ def run_complex(args, w, world, rank, local, pg):
                "d2h_bytes_per_step": int(16 * n * mev + 8 * mev)}
 
     solve_rec = None
-    if not args.no_solve and rank == 0:
+    if not args.no_solve and rank == 0 and world == 1:
         from nutrlan_b200 import residual_norms
         solve_rec = {}
         for bits in (64, 32):
@@ -1057,7 +1057,7 @@ def main():
         variants[f"{fmt_used}_fp{alt_bits}"] = time_variant(fmt_used, alt_bits)
 
     solve_rec = None
-    if not args.no_solve and rank == 0:
+    if not args.no_solve and rank == 0 and world == 1:
         from nutrlan_b200 import residual_norms
         solve_rec = {}
         for bits in (64, 32):
