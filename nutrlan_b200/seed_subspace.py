@@ -148,7 +148,7 @@ __all__ = ["dense_cycles", "first_cycle_then_trlan", "seed_quality_study"]
 
 
 def seed_quality_study(problems=4, eps=(1e-1, 1e-2, 1e-3, 1e-4, 1e-6), L=256, ned=16, maxlan=48, tol=1e-8,
-                       seed0=10 ** 6, log=print):
+                       seed0=10 ** 6, log=print, weights=None):
     """Matvecs to residual <= tol * ||A|| on held-out well operators for seeds
     of known quality: the exact lowest 16 eigenvectors (from a plain solve of
     the 60 lowest pairs) plus eps times a unit-norm error spread over the
@@ -164,7 +164,7 @@ def seed_quality_study(problems=4, eps=(1e-1, 1e-2, 1e-3, 1e-4, 1e-6), L=256, ne
     from .seednet import SeedNet, seed_start
     from .solver import DeviceOperator, solve
     out = []
-    net = SeedNet.pretrained()
+    net = SeedNet.pretrained(weights) if weights else SeedNet.pretrained()
     try:
         for s in range(seed0, seed0 + problems):
             A, V = ops.wells_2d(L, seed=s)
@@ -203,8 +203,10 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=seed_quality_study.__doc__)
     ap.add_argument("--problems", type=int, default=4)
     ap.add_argument("--out", default=None, help="write the records as JSON here")
+    ap.add_argument("--weights", default=None, help="network weights (default: the packaged ones)")
+    ap.add_argument("--eps", type=float, nargs="*", default=[1e-1, 1e-2, 1e-3, 1e-4, 1e-6])
     a = ap.parse_args(argv)
-    recs = seed_quality_study(a.problems)
+    recs = seed_quality_study(a.problems, eps=tuple(a.eps), weights=a.weights)
     if a.out:
         with open(a.out, "w") as f:
             json.dump(recs, f, indent=1)
