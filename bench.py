@@ -68,6 +68,13 @@ WORKLOADS = {
 }
 
 
+def _form_index(tune, key):
+    """A tuned projection form as its trlx value (0: the default form)."""
+    if not tune:
+        return 0
+    return 1 + ("cpw8", "cpw12", "cpw16", "cpw16_shared_ptrs").index(tune[key])
+
+
 def build_operator(w, seed):
     from nutrlan_b200 import operators as ops
     if w["kind"] == "anderson":
@@ -381,7 +388,8 @@ def run_complex(args, w, world, rank, local, pg):
     lib = load()
     mev = ned + 1
     op = DeviceOperator(A, fmt="auto", maxlan=maxlan)        # tunes the projection form
-    tuned_form = 1 + ("cpw8", "cpw12", "cpw16", "cpw16_shared_ptrs").index(op.tune["project_form"])
+    tuned_form = _form_index(op.tune, "project_form")
+    tuned_form32 = _form_index(op.tune, "project_form32")
     config["autotune"] = op.tune
     evec = torch.zeros((mev, n), dtype=torch.complex128, device=dev)
     x0_dev = torch.as_tensor(x0, device=dev)
@@ -461,6 +469,7 @@ def run_complex(args, w, world, rank, local, pg):
             h = C.c_void_p()
             lib.trlx_zcsr_create(n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, 0, C.byref(h))
             lib.trlx_operator_set_project_form(h, tuned_form)
+            lib.trlx_operator_set_project_form32(h, tuned_form32)
             hev[0] = x0
             mv = call(TrlInfo(), opts, maxlan, hev.ctypes.data, h.value, op.applier)
             lib.trlx_operator_destroy(h)
@@ -894,8 +903,8 @@ def main():
     # ---- device-resident arm -------------------------------------------------
     op = DeviceOperator(A, fmt=args.format, maxlan=maxlan)
     fmt_used = op.fmt
-    tuned_form = (1 + ("cpw8", "cpw12", "cpw16", "cpw16_shared_ptrs").index(op.tune["project_form"])
-                  if op.tune else 0)
+    tuned_form = _form_index(op.tune, "project_form")
+    tuned_form32 = _form_index(op.tune, "project_form32")
     config["workload"] = config["workload"].replace("{fmt}", fmt_used.upper())
     if op.tune is not None:
         config["format_choice"] = "autotuned (trlx_operator_autotune)"
@@ -996,6 +1005,7 @@ def main():
             if rc != 0:
                 raise RuntimeError(f"operator creation from host arrays failed ({rc})")
             lib.trlx_operator_set_project_form(handle, tuned_form)   # the tuning kept above
+            lib.trlx_operator_set_project_form32(handle, tuned_form32)
             inf = TrlInfo()
             lib.trl_init_info(C.byref(inf), n, maxlan, -1, ned, tol, 1, steps_per_call, None)
             inf.mvparam = handle.value
@@ -1124,7 +1134,8 @@ def main():
     if rank == 0:
         line = {"metric": metric, "value": value, "unit": "steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.basis_bits == 64 else "f32 basis / f64",
                 "data": "synthetic (seeded Anderson potential and start vector)", "config": config,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks, "host_wall_s": wall, "variants": variants, "solve": solve_rec,

@@ -58,12 +58,15 @@ int trlx_operator_nrow(const trlx_operator *op);
    product y = A x + alpha in the CSR form and in the SELL-C-32 form built
    from the same device arrays, and one Gram-Schmidt projection over
    maxlan / 2 columns of the operator's row count in each of the projection
-   kernel's forms (median of 5 launches each); for a complex operator
-   (trlx_zcsr_create) only the projection forms 3 and 4 (the others report
-   -1 ms).  It keeps the faster operator
+   kernel's forms (median of 5 launches each), over FP64 columns and again
+   over FP32 columns (the two basis storage widths of
+   trlx_options.basis_bits); for a complex operator (trlx_zcsr_create) only
+   the projection forms 3 and 4, over complex128 and complex64 columns (the
+   others report -1 ms).  It keeps the faster operator
    form (storage switched in place, the handle stays valid) and the faster
-   projection form for every later solve with this operator (call it
-   before, not during, solves that use the operator).  Temporary
+   projection form for each basis width for every later solve with this
+   operator (call it before, not during, solves that use the operator).
+   Temporary
    device memory: two vectors and the projection's columns (at most a
    quarter of the free memory).  Returns 0, -1 for an operator it does not
    tune (SELL-created or distributed), -2 if the temporary memory
@@ -77,6 +80,8 @@ typedef struct {
     double project_ms[4];  /* one projection in forms 1 .. 4               */
     int columns;           /* projection width timed                        */
     double seconds;        /* wall time of the tuning                       */
+    int project_form32;    /* kept form for a 32-bit basis (same values)    */
+    double project32_ms[4];/* one projection over 32-bit columns, forms 1..4 */
 } trlx_tune_result;
 int trlx_operator_autotune(trlx_operator *op, int maxlan, trlx_tune_result *out);
 /* Sets the projection form of later solves with this operator (a
@@ -84,6 +89,9 @@ int trlx_operator_autotune(trlx_operator *op, int maxlan, trlx_tune_result *out)
    reuse a tuning result on an operator created again from the same matrix.
    Returns 0, or -1 for a null operator or an unknown form. */
 int trlx_operator_set_project_form(trlx_operator *op, int project_form);
+/* The same for solves over a 32-bit basis (trlx_options.basis_bits = 32; a
+   trlx_tune_result.project_form32 value). */
+int trlx_operator_set_project_form32(trlx_operator *op, int project_form);
 
 /* trl_matvec / ztrl_matvec compatible appliers (device x, y). */
 void trlx_matvec(const int nrow, const int ncol, const double *x,

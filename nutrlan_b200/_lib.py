@@ -46,7 +46,8 @@ class TrlxOptions(C.Structure):
 class TrlxTuneResult(C.Structure):
     """trlx_tune_result: what trlx_operator_autotune measured and kept."""
     _fields_ = [("format", c_int), ("project_form", c_int), ("spmv_ms", c_double * 2),
-                ("project_ms", c_double * 4), ("columns", c_int), ("seconds", c_double)]
+                ("project_ms", c_double * 4), ("columns", c_int), ("seconds", c_double),
+                ("project_form32", c_int), ("project32_ms", c_double * 4)]
 
     FORMS = ("cpw8", "cpw12", "cpw16", "cpw16_shared_ptrs")
 
@@ -55,6 +56,9 @@ class TrlxTuneResult(C.Structure):
                 "spmv_forms_timed": 2 if self.spmv_ms[1] >= 0 else 1,
                 "spmv_ms": {"csr": self.spmv_ms[0], "sell": self.spmv_ms[1]},
                 "project_ms": {f: self.project_ms[i] for i, f in enumerate(self.FORMS) if self.project_ms[i] >= 0},
+                "project_form32": self.FORMS[self.project_form32 - 1],
+                "project32_ms": {f: self.project32_ms[i] for i, f in enumerate(self.FORMS)
+                                 if self.project32_ms[i] >= 0},
                 "columns": self.columns, "seconds": self.seconds}
 
 
@@ -92,8 +96,9 @@ def _declare(lib):
     lib.trlx_operator_nrow.restype = c_int
     lib.trlx_operator_autotune.argtypes = [c_void_p, c_int, P(TrlxTuneResult)]
     lib.trlx_operator_autotune.restype = c_int
-    lib.trlx_operator_set_project_form.argtypes = [c_void_p, c_int]
-    lib.trlx_operator_set_project_form.restype = c_int
+    for name in ("trlx_operator_set_project_form", "trlx_operator_set_project_form32"):
+        getattr(lib, name).argtypes = [c_void_p, c_int]
+        getattr(lib, name).restype = c_int
     # Block-row communicators and distributed operators.
     lib.trlx_comm_create_host.argtypes = [c_int, c_int, ALLREDUCE_FN, c_void_p, P(c_void_p)]
     lib.trlx_comm_create_host.restype = c_int

@@ -298,8 +298,12 @@ class Engine {
     // modes
     bool user_dev_ = false;
     const trlx_operator *builtin_ = nullptr;
-    // Projection kernel form tuned for the built-in operator (0: default).
-    int proj_form() const { return builtin_ ? builtin_->project_form : 0; }
+    // Projection kernel form tuned for the built-in operator and this
+    // basis' storage width (0: default).
+    int proj_form() const {
+        if (!builtin_) return 0;
+        return sizeof(T) < sizeof(C) ? builtin_->project_form32 : builtin_->project_form;
+    }
     bool host_op_ = false;
     // Block-row solve: sums over the ranks of the communicator stored in
     // info->mpicomp by trlx_init_info_comm (nullptr: one GPU).

@@ -8,12 +8,13 @@
 //  * one Gram-Schmidt projection h = V^T r over `maxlan / 2` basis columns
 //    of this operator's row count (the average width of a thick-restart
 //    cycle) in each form of the projection kernel (8, 12, 16 columns per
-//    warp; 16 with the pointer table in shared memory);
+//    warp; 16 with the pointer table in shared memory), once over FP64
+//    columns and once over FP32 columns (the two basis storage widths);
 //
 // and keeps the faster of each: the operator's storage is switched in place
 // to the faster form (the handle stays valid; the other form is freed) and
-// the projection form is stored in the operator, where solves with it read
-// it.  Every candidate is timed with CUDA events over `kReps` launches after
+// the two projection forms are stored in the operator, where solves with it
+// read the one for their basis width.  Every candidate is timed with CUDA events over `kReps` launches after
 // a warm-up launch, and the median is kept.  Products are checked against
 // each other (the same alpha up to summation order) before a form is adopted.
 #include <algorithm>
@@ -43,7 +44,8 @@ struct DevBuf {
     }
 };
 
-__global__ void k_fill_pattern(double *v, long n, long n_pad, unsigned salt) {
+template <class V>
+__global__ void k_fill_pattern(V *v, long n, long n_pad, unsigned salt) {
     const long stride = (long)gridDim.x * blockDim.x;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += stride) {
         // Deterministic values in [-1, 1); padding rows stay zero as the
@@ -52,7 +54,7 @@ __global__ void k_fill_pattern(double *v, long n, long n_pad, unsigned salt) {
         x ^= x >> 15;
         x *= 0x2c1b3c6du;
         x ^= x >> 12;
-        v[i] = i < n ? (double)(x & 0xFFFFFF) / 8388608.0 - 1.0 : 0.0;
+        v[i] = i < n ? (V)((double)(x & 0xFFFFFF) / 8388608.0 - 1.0) : (V)0;
     }
 }
 
@@ -86,6 +88,29 @@ void move_storage(trlx_operator *dst, trlx_operator *src) {
     std::swap(dst->sigma, src->sigma);
     std::swap(dst->slice_ptr, src->slice_ptr);
     std::swap(dst->perm, src->perm);
+}
+
+// Refills the first mp columns of the basis buffer as storage type V
+// (vw scalars per element) and returns their column table, copied to
+// `table` on the device.
+template <class V>
+void fill_columns(void *basis, void *table, int mp, long n, long n_pad, int vw, cudaStream_t st) {
+    std::vector<V *> cols(mp);
+    for (int c = 0; c < mp; ++c) {
+        cols[c] = static_cast<V *>(basis) + (size_t)c * vw * n_pad;
+        k_fill_pattern<V><<<592, 256, 0, st>>>(cols[c], vw * n, vw * n_pad, 7u + c);
+    }
+    cudaMemcpyAsync(table, cols.data(), sizeof(V *) * mp, cudaMemcpyHostToDevice, st);
+    cudaStreamSynchronize(st);
+}
+
+// Index of the fastest of the timed forms (negative times: not timed),
+// starting from `dflt`, which stays unless another form measured faster.
+int fastest(const double (&ms)[4], int dflt) {
+    int best = dflt;
+    for (int k = 0; k < 4; ++k)
+        if (ms[k] >= 0.0 && ms[k] < ms[best]) best = k;
+    return best;
 }
 
 }  // namespace
@@ -129,14 +154,8 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
         s.tickets = static_cast<unsigned *>(tick.p);
         cudaMemsetAsync(tick.p, 0, sizeof(unsigned) * trlb::kNumTickets, st);
         // Complex vectors are filled as interleaved (re, im) doubles.
-        k_fill_pattern<<<592, 256, 0, st>>>(static_cast<double *>(x.p), vw * n, vw * n_pad, 1u);
-        for (int c = 0; c < mp; ++c)
-            k_fill_pattern<<<592, 256, 0, st>>>(static_cast<double *>(basis.p) + (size_t)c * vw * n_pad, vw * n,
-                                                 vw * n_pad, 7u + c);
-        std::vector<double *> cols(mp);
-        for (int c = 0; c < mp; ++c) cols[c] = static_cast<double *>(basis.p) + (size_t)c * vw * n_pad;
-        cudaMemcpyAsync(table.p, cols.data(), sizeof(double *) * mp, cudaMemcpyHostToDevice, st);
-        cudaStreamSynchronize(st);
+        k_fill_pattern<double><<<592, 256, 0, st>>>(static_cast<double *>(x.p), vw * n, vw * n_pad, 1u);
+        fill_columns<double>(basis.p, table.p, mp, n, n_pad, vw, st);
     }
     if (!rc && cplx) {
         // Complex CSR: one operator form; the projection keeps its pointer
@@ -162,6 +181,23 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
         const int best = out->project_ms[3] < out->project_ms[2] ? trlb::kProject16Shared : trlb::kProject16;
         A->project_form = best;
         out->project_form = best;
+        // The same forms over complex64 columns.
+        using trlb::zf;
+        fill_columns<float>(basis.p, table.p, mp, n, n_pad, vw, st);
+        out->project32_ms[0] = out->project32_ms[1] = -1.0;
+        for (int k = 2; k < 4; ++k) {
+            out->project32_ms[k] = median_ms(
+                [&] {
+                    trlb::launch_project<zf>(static_cast<zf *const *>(table.p), mp, n_pad,
+                                             static_cast<const zd *>(x.p), none, static_cast<zd *>(dsc.p),
+                                             static_cast<double *>(dsc.p) + 2 * (m + 1), s, st, trlb::kProject8 + k);
+                },
+                st);
+        }
+        const int best32 =
+            out->project32_ms[3] < out->project32_ms[2] ? trlb::kProject16Shared : trlb::kProject16;
+        A->project_form32 = best32;
+        out->project_form32 = best32;
         out->columns = mp;
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = -3;
     } else if (!rc) {
@@ -206,11 +242,24 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
                 },
                 st);
         }
-        int best = trlb::kProject16 - trlb::kProject8;  // the default unless another form measured faster
-        for (int k = 0; k < 4; ++k)
-            if (out->project_ms[k] < out->project_ms[best]) best = k;
+        const int best = fastest(out->project_ms, trlb::kProject16 - trlb::kProject8);
         A->project_form = trlb::kProject8 + best;
         out->project_form = trlb::kProject8 + best;
+        // The same forms over FP32 columns (the first half of the buffer).
+        fill_columns<float>(basis.p, table.p, mp, n, n_pad, vw, st);
+        for (int k = 0; k < 4; ++k) {
+            out->project32_ms[k] = median_ms(
+                [&] {
+                    trlb::launch_project<float>(static_cast<float *const *>(table.p), mp, n_pad,
+                                                static_cast<const double *>(x.p), none,
+                                                static_cast<double *>(dsc.p), static_cast<double *>(dsc.p) + m + 1,
+                                                s, st, trlb::kProject8 + k);
+                },
+                st);
+        }
+        const int best32 = fastest(out->project32_ms, trlb::kProject16 - trlb::kProject8);
+        A->project_form32 = trlb::kProject8 + best32;
+        out->project_form32 = trlb::kProject8 + best32;
         out->columns = mp;
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = -3;
     }
@@ -225,5 +274,11 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
 extern "C" int trlx_operator_set_project_form(trlx_operator *A, int form) {
     if (!A || form < trlb::kProjectDefault || form > trlb::kProject16Shared) return -1;
     A->project_form = form;
+    return 0;
+}
+
+extern "C" int trlx_operator_set_project_form32(trlx_operator *A, int form) {
+    if (!A || form < trlb::kProjectDefault || form > trlb::kProject16Shared) return -1;
+    A->project_form32 = form;
     return 0;
 }

@@ -244,7 +244,6 @@ __device__ inline Norms project(const double *V, int ld, int n, int m, double *y
 __device__ inline double update(const double *V, int ld, int n, int m, double *y, bool rec, const double *x,
                               const double *xp, double alpha, double beta, const double *h, const Grp &G) {
     constexpr int UC = 8;
-    Shared &S = *G.S;
     double r2 = 0.0;
     const int np = n >> 1;
     for (int p = G.tid; p < np; p += G.nt) {

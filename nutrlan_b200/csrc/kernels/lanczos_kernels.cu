@@ -86,10 +86,18 @@ constexpr int proj_min_blocks() {
 }
 
 // PS: the warp's column pointers live in shared memory and are re-read at
-// every use instead of being held in 2 * CPW registers, which lets three
-// blocks of the 16-column form reside per SM.
+// every use instead of being held in 2 * CPW registers.  For 64-bit and
+// complex storage the freed registers buy a third resident block; for FP32
+// storage they hold the 16 columns' float4 loads, all issued before the
+// first is consumed, at two blocks per SM (a third block would leave room
+// for about half of them).
+template <class T>
+constexpr int proj_ps_blocks() {
+    return std::is_same<T, float>::value ? 2 : 3;
+}
+
 template <class T, int CPW, bool PS = false>
-__global__ void __launch_bounds__(kThreads, (PS ? 3 : proj_min_blocks<T, CPW>()))
+__global__ void __launch_bounds__(kThreads, (PS ? proj_ps_blocks<T>() : proj_min_blocks<T, CPW>()))
     k_project(T *const *__restrict__ cols, int m, long n_pad, long chunk,
               const typename Store<T>::C *__restrict__ r, Recur<typename Store<T>::C> rec,
               typename Store<T>::C *part, double *part_r2, unsigned *ticket,

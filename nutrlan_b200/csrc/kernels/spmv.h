@@ -31,10 +31,12 @@ struct trlx_operator {
     // this rank's rows, [nrow, nrow + halo entries) values received from
     // other ranks before every product.
     trlb::Halo *halo = nullptr;
-    // Form of the FP64 Gram-Schmidt projection kernel (trlb::ProjectForm)
-    // for solves with this operator, set by trlx_operator_autotune (0: the
-    // default form).
+    // Form of the Gram-Schmidt projection kernel (trlb::ProjectForm) for
+    // solves with this operator over a 64-bit basis (FP64 / complex128) and
+    // over a 32-bit basis (FP32 / complex64), set by trlx_operator_autotune
+    // (0: the default form).
     int project_form = 0;
+    int project_form32 = 0;
 };
 
 namespace trlb {

@@ -96,3 +96,34 @@ def test_every_trl_info_offset_matches_the_reference_header(tmp_path):
     assert got["sizeof"] == "800" and len(got) == len(fields) + 1
     for f in fields:                      # and the Python mirror agrees with both
         assert int(got[f]) == getattr(TrlInfo, f).offset, f
+
+
+def _mirrors():
+    from nutrlan_b200._lib import TrlxStats, TrlxOptions, TrlxTuneResult
+    from nutrlan_b200.batched import BatchOptions, BatchConfig
+    return {"trlx_stats": TrlxStats, "trlx_options": TrlxOptions, "trlx_tune_result": TrlxTuneResult,
+            "trlx_batch_options": BatchOptions, "trlx_batch_config": BatchConfig}
+
+
+def test_trlx_struct_mirrors_match_the_header(tmp_path):
+    """Every ctypes mirror of a trlx.h struct has the C compiler's size and
+    field offsets (fields appended to a struct keep the earlier offsets)."""
+    mirrors = _mirrors()
+    lines = []
+    for cname, py in mirrors.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, *_ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    src = tmp_path / "mirrors.c"
+    src.write_text("#include <stddef.h>\n#include <stdio.h>\n#include \"trlx.h\"\nint main(){\n"
+                   + "\n".join(lines) + "\nreturn 0;}\n")
+    exe = tmp_path / "mirrors"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for ln in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        cname, key, val = ln.split()
+        got[(cname, key)] = int(val)
+    for cname, py in mirrors.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for fname, *_ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
