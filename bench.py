@@ -72,7 +72,8 @@ def _form_index(tune, key):
     """A tuned projection form as its trlx value (0: the default form)."""
     if not tune:
         return 0
-    return 1 + ("cpw8", "cpw12", "cpw16", "cpw16_shared_ptrs").index(tune[key])
+    from nutrlan_b200._lib import TrlxTuneResult
+    return 1 + TrlxTuneResult.FORMS.index(tune[key])
 
 
 def build_operator(w, seed):

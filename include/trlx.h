@@ -61,8 +61,8 @@ int trlx_operator_nrow(const trlx_operator *op);
    kernel's forms (median of 5 launches each), over FP64 columns and again
    over FP32 columns (the two basis storage widths of
    trlx_options.basis_bits); for a complex operator (trlx_zcsr_create) only
-   the projection forms 3 and 4, over complex128 and complex64 columns (the
-   others report -1 ms).  It keeps the faster operator
+   the projection forms 3, 4 and 5, over complex128 and complex64 columns
+   (the others report -1 ms).  It keeps the faster operator
    form (storage switched in place, the handle stays valid) and the faster
    projection form for each basis width for every later solve with this
    operator (call it before, not during, solves that use the operator).
@@ -75,13 +75,15 @@ typedef struct {
     int format;            /* kept operator form: 0 CSR, 1 SELL-C-32        */
     int project_form;      /* kept projection form: 1, 2, 3: 8, 12, 16
                               columns per warp; 4: 16 columns with the
-                              column-pointer table in shared memory        */
+                              column-pointer table in shared memory; 5: 16
+                              columns, the basis staged through shared
+                              memory by cp.async, one block per SM        */
     double spmv_ms[2];     /* one product: CSR, SELL-C-32 (-1: not built)  */
-    double project_ms[4];  /* one projection in forms 1 .. 4               */
+    double project_ms[5];  /* one projection in forms 1 .. 5               */
     int columns;           /* projection width timed                        */
     double seconds;        /* wall time of the tuning                       */
     int project_form32;    /* kept form for a 32-bit basis (same values)    */
-    double project32_ms[4];/* one projection over 32-bit columns, forms 1..4 */
+    double project32_ms[5];/* one projection over 32-bit columns, forms 1..5 */
 } trlx_tune_result;
 int trlx_operator_autotune(trlx_operator *op, int maxlan, trlx_tune_result *out);
 /* Sets the projection form of later solves with this operator (a

@@ -46,10 +46,10 @@ class TrlxOptions(C.Structure):
 class TrlxTuneResult(C.Structure):
     """trlx_tune_result: what trlx_operator_autotune measured and kept."""
     _fields_ = [("format", c_int), ("project_form", c_int), ("spmv_ms", c_double * 2),
-                ("project_ms", c_double * 4), ("columns", c_int), ("seconds", c_double),
-                ("project_form32", c_int), ("project32_ms", c_double * 4)]
+                ("project_ms", c_double * 5), ("columns", c_int), ("seconds", c_double),
+                ("project_form32", c_int), ("project32_ms", c_double * 5)]
 
-    FORMS = ("cpw8", "cpw12", "cpw16", "cpw16_shared_ptrs")
+    FORMS = ("cpw8", "cpw12", "cpw16", "cpw16_shared_ptrs", "cpw16_staged")
 
     def as_dict(self):
         return {"format": ("csr", "sell")[self.format], "project_form": self.FORMS[self.project_form - 1],

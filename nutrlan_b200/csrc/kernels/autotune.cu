@@ -8,8 +8,9 @@
 //  * one Gram-Schmidt projection h = V^T r over `maxlan / 2` basis columns
 //    of this operator's row count (the average width of a thick-restart
 //    cycle) in each form of the projection kernel (8, 12, 16 columns per
-//    warp; 16 with the pointer table in shared memory), once over FP64
-//    columns and once over FP32 columns (the two basis storage widths);
+//    warp; 16 with the pointer table in shared memory; 16 with the basis
+//    staged through shared memory by cp.async), once over FP64 columns and
+//    once over FP32 columns (the two basis storage widths);
 //
 // and keeps the faster of each: the operator's storage is switched in place
 // to the faster form (the handle stays valid; the other form is freed) and
@@ -106,9 +107,9 @@ void fill_columns(void *basis, void *table, int mp, long n, long n_pad, int vw, 
 
 // Index of the fastest of the timed forms (negative times: not timed),
 // starting from `dflt`, which stays unless another form measured faster.
-int fastest(const double (&ms)[4], int dflt) {
+int fastest(const double (&ms)[trlb::kProjectForms], int dflt) {
     int best = dflt;
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < trlb::kProjectForms; ++k)
         if (ms[k] >= 0.0 && ms[k] < ms[best]) best = k;
     return best;
 }
@@ -159,7 +160,8 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
     }
     if (!rc && cplx) {
         // Complex CSR: one operator form; the projection keeps its pointer
-        // table in registers (form 3) or in shared memory (form 4).
+        // table in registers (form 3) or in shared memory (form 4), or
+        // stages the basis through shared memory (form 5).
         using trlb::zd;
         double *alpha = static_cast<double *>(dsc.p);
         out->format = 0;
@@ -169,7 +171,7 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
         out->spmv_ms[1] = -1.0;
         trlb::Recur<zd> none;
         out->project_ms[0] = out->project_ms[1] = -1.0;
-        for (int k = 2; k < 4; ++k) {
+        for (int k = 2; k < trlb::kProjectForms; ++k) {
             out->project_ms[k] = median_ms(
                 [&] {
                     trlb::launch_project<zd>(static_cast<zd *const *>(table.p), mp, n_pad,
@@ -178,14 +180,14 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
                 },
                 st);
         }
-        const int best = out->project_ms[3] < out->project_ms[2] ? trlb::kProject16Shared : trlb::kProject16;
+        const int best = trlb::kProject8 + fastest(out->project_ms, trlb::kProject16 - trlb::kProject8);
         A->project_form = best;
         out->project_form = best;
         // The same forms over complex64 columns.
         using trlb::zf;
         fill_columns<float>(basis.p, table.p, mp, n, n_pad, vw, st);
         out->project32_ms[0] = out->project32_ms[1] = -1.0;
-        for (int k = 2; k < 4; ++k) {
+        for (int k = 2; k < trlb::kProjectForms; ++k) {
             out->project32_ms[k] = median_ms(
                 [&] {
                     trlb::launch_project<zf>(static_cast<zf *const *>(table.p), mp, n_pad,
@@ -194,8 +196,7 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
                 },
                 st);
         }
-        const int best32 =
-            out->project32_ms[3] < out->project32_ms[2] ? trlb::kProject16Shared : trlb::kProject16;
+        const int best32 = trlb::kProject8 + fastest(out->project32_ms, trlb::kProject16 - trlb::kProject8);
         A->project_form32 = best32;
         out->project_form32 = best32;
         out->columns = mp;
@@ -232,7 +233,7 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
         }
         // ---- projection kernel form -------------------------------------
         trlb::Recur<double> none;
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < trlb::kProjectForms; ++k) {
             out->project_ms[k] = median_ms(
                 [&] {
                     trlb::launch_project<double>(static_cast<double *const *>(table.p), mp, n_pad,
@@ -247,7 +248,7 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
         out->project_form = trlb::kProject8 + best;
         // The same forms over FP32 columns (the first half of the buffer).
         fill_columns<float>(basis.p, table.p, mp, n, n_pad, vw, st);
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < trlb::kProjectForms; ++k) {
             out->project32_ms[k] = median_ms(
                 [&] {
                     trlb::launch_project<float>(static_cast<float *const *>(table.p), mp, n_pad,
@@ -272,13 +273,13 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
 }
 
 extern "C" int trlx_operator_set_project_form(trlx_operator *A, int form) {
-    if (!A || form < trlb::kProjectDefault || form > trlb::kProject16Shared) return -1;
+    if (!A || form < trlb::kProjectDefault || form > trlb::kProjectAsync) return -1;
     A->project_form = form;
     return 0;
 }
 
 extern "C" int trlx_operator_set_project_form32(trlx_operator *A, int form) {
-    if (!A || form < trlb::kProjectDefault || form > trlb::kProject16Shared) return -1;
+    if (!A || form < trlb::kProjectDefault || form > trlb::kProjectAsync) return -1;
     A->project_form32 = form;
     return 0;
 }

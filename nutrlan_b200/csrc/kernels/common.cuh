@@ -68,6 +68,12 @@ struct Store<double> {
         o[0] = v.x;
         o[1] = v.y;
     }
+    // The same 16 bytes from shared memory.
+    __device__ __forceinline__ static void lds(const double *p, C (&o)[R]) {
+        double2 v = *reinterpret_cast<const double2 *>(p);
+        o[0] = v.x;
+        o[1] = v.y;
+    }
     __device__ __forceinline__ static void store(double *p, const C (&o)[R]) {
         *reinterpret_cast<double2 *>(p) = make_double2(o[0], o[1]);
     }
@@ -80,6 +86,13 @@ struct Store<float> {
     static constexpr int R = 4;
     __device__ __forceinline__ static void load(const float *p, C (&o)[R]) {
         float4 v = __ldg(reinterpret_cast<const float4 *>(p));
+        o[0] = v.x;
+        o[1] = v.y;
+        o[2] = v.z;
+        o[3] = v.w;
+    }
+    __device__ __forceinline__ static void lds(const float *p, C (&o)[R]) {
+        float4 v = *reinterpret_cast<const float4 *>(p);
         o[0] = v.x;
         o[1] = v.y;
         o[2] = v.z;
@@ -100,6 +113,10 @@ struct Store<zd> {
         double2 v = __ldg(reinterpret_cast<const double2 *>(p));
         o[0] = zd{v.x, v.y};
     }
+    __device__ __forceinline__ static void lds(const zd *p, C (&o)[R]) {
+        double2 v = *reinterpret_cast<const double2 *>(p);
+        o[0] = zd{v.x, v.y};
+    }
     __device__ __forceinline__ static void store(zd *p, const C (&o)[R]) {
         *reinterpret_cast<double2 *>(p) = make_double2(o[0].x, o[0].y);
     }
@@ -112,6 +129,11 @@ struct Store<zf> {
     static constexpr int R = 2;
     __device__ __forceinline__ static void load(const zf *p, C (&o)[R]) {
         float4 v = __ldg(reinterpret_cast<const float4 *>(p));
+        o[0] = zd{v.x, v.y};
+        o[1] = zd{v.z, v.w};
+    }
+    __device__ __forceinline__ static void lds(const zf *p, C (&o)[R]) {
+        float4 v = *reinterpret_cast<const float4 *>(p);
         o[0] = zd{v.x, v.y};
         o[1] = zd{v.z, v.w};
     }

@@ -230,6 +230,183 @@ __global__ void __launch_bounds__(kThreads, (PS ? proj_ps_blocks<T>() : proj_min
 }
 
 // ---------------------------------------------------------------------------
+// Projection with the basis staged through shared memory by cp.async
+// (kProjectAsync).  The register forms above hold every basis load in
+// flight in registers, next to an FP64 accumulator and a pointer per
+// column, and the register file caps the bytes in flight per SM: FP32 and
+// complex storage stop at 80-90% of the HBM peak.  Here each lane copies its
+// own 16 bytes of each of its warp's 16 columns into a ring of NS stages in
+// shared memory (192 KB, one block per SM), so NS - 1 stages (128 KB per SM)
+// are in flight while the warp consumes the oldest.  A lane reads back only
+// the bytes it copied itself, so the ring needs no barrier: the thread's own
+// cp.async.wait_group orders them.  r, x and x' (shared by the block's warps
+// and mostly served by L1/L2) are plain loads issued one iteration ahead.
+// Column groups, row split and the order of every sum are those of
+// k_project.
+constexpr int kAsyncCols = 16;
+constexpr int kAsyncStages = 3;
+constexpr size_t kAsyncSmem = (size_t)(kThreads / 32) * kAsyncStages * kAsyncCols * 32 * 16;
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_project_async(T *const *__restrict__ cols, int m, long n_pad, long chunk,
+                    const typename Store<T>::C *__restrict__ r, Recur<typename Store<T>::C> rec,
+                    typename Store<T>::C *part, double *part_r2, unsigned *ticket,
+                    typename Store<T>::C *h, double *out2) {
+    using S = Store<T>;
+    using C = typename S::C;
+    constexpr int R = S::R;
+    constexpr int W = kThreads / 32;
+    constexpr int CPW = kAsyncCols, NS = kAsyncStages;
+    static_assert(sizeof(T) * R == 16, "one 16-byte copy per lane and column");
+    extern __shared__ __align__(16) unsigned char ring_raw[];
+    __shared__ C red_c[W][CPW];
+    __shared__ double red_r2[W];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // This lane's 16 bytes of column k in stage q.
+    T *const ring = reinterpret_cast<T *>(ring_raw) + (size_t)warp * NS * CPW * 32 * R;
+    auto slot = [&](int q, int k) { return ring + ((size_t)(q * CPW + k) * 32 + lane) * R; };
+    const long row0 = (long)blockIdx.x * chunk;
+    const long row1 = min(n_pad, row0 + chunk);
+    const double alpha = rec.on ? *rec.alpha : 0.0;
+    const double beta = rec.on ? (rec.beta_r2 ? sqrt(*rec.beta_r2) : rec.beta) : 0.0;
+    double r2acc = 0.0;
+    for (int c0 = 0; c0 < m; c0 += W * CPW) {
+        const int mc = min(W * CPW, m - c0);
+        int G = 1;
+        while (G < W && G * CPW < mc) G *= 2;
+        const int per = (mc + G - 1) / G;
+        const int wpg = W / G;
+        const int grp = warp / wpg, slice = warp - grp * wpg;
+        const int cb = c0 + grp * per;
+        const int cn = max(0, min(per, m - cb));
+        const T *p[CPW];
+#pragma unroll
+        for (int k = 0; k < CPW; ++k) p[k] = k < cn ? cols[cb + k] : nullptr;
+        C acc[CPW];
+#pragma unroll
+        for (int k = 0; k < CPW; ++k) acc[k] = czero(C());
+        const bool count_r2 = (c0 == 0 && grp == 0);
+        const long step = (long)wpg * 32 * R;
+        const long first = row0 + (long)(slice * 32 + lane) * R;  // this lane's first row
+        const long wfirst = row0 + (long)slice * 32 * R;           // the warp's first row
+        const int nit = (cn > 0 && wfirst < row1) ? (int)((row1 - wfirst + step - 1) / step) : 0;
+        auto issue = [&](int t) {
+            const long i = first + (long)t * step;
+            if (t < nit && i < row1) {
+#pragma unroll
+                for (int k = 0; k < CPW; ++k)
+                    if (p[k]) cp_async16(slot(t % NS, k), p[k] + i);
+            }
+            cp_async_commit();
+        };
+        C rn[R], xn[R], xpn[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) rn[q] = xn[q] = xpn[q] = czero(C());
+        auto load_vectors = [&](int t) {
+            const long i = first + (long)t * step;
+            if (t < nit && i < row1) {
+                load_c<R>(r + i, rn);
+                if (rec.on) {
+                    load_c<R>(rec.x + i, xn);
+                    load_c<R>(rec.xp + i, xpn);
+                }
+            }
+        };
+#pragma unroll
+        for (int q = 0; q < NS - 1; ++q) issue(q);
+        load_vectors(0);
+        for (int t = 0; t < nit; ++t) {
+            issue(t + NS - 1);  // into the slot consumed at t - 1
+            C rv[R];
+#pragma unroll
+            for (int q = 0; q < R; ++q) rv[q] = rec.on ? rn[q] - alpha * xn[q] - beta * xpn[q] : rn[q];
+            load_vectors(t + 1);
+            cp_async_wait<NS - 1>();  // this thread's copies of stage t have landed
+            if (first + (long)t * step < row1) {
+                if (count_r2) {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) r2acc += abs2(rv[q]);
+                }
+#pragma unroll
+                for (int k = 0; k < CPW; ++k) {
+                    if (p[k]) {
+                        C v[R];
+                        S::lds(slot(t % NS, k), v);
+#pragma unroll
+                        for (int q = 0; q < R; ++q) fma_conj(acc[k], v[q], rv[q]);
+                    }
+                }
+            }
+        }
+        cp_async_wait<0>();
+#pragma unroll
+        for (int k = 0; k < CPW; ++k) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[k] = acc[k] + shfl_down(acc[k], o);
+            if (lane == 0) red_c[warp][k] = acc[k];
+        }
+        __syncthreads();
+        if (threadIdx.x < G * CPW) {
+            const int gg = threadIdx.x / CPW, k = threadIdx.x - gg * CPW;
+            const int c = c0 + gg * per + k;
+            if (k < per && c < m) {
+                C sacc = czero(C());
+                for (int sl = 0; sl < wpg; ++sl) sacc = sacc + red_c[gg * wpg + sl][k];
+                part[(long)blockIdx.x * m + c] = sacc;
+            }
+        }
+        __syncthreads();
+    }
+    if (m == 0) {
+        for (long i = row0 + (long)threadIdx.x * R; i < row1; i += (long)kThreads * R) {
+            C rv[R];
+            load_c<R>(r + i, rv);
+            if (rec.on) {
+                C xv[R], xpv[R];
+                load_c<R>(rec.x + i, xv);
+                load_c<R>(rec.xp + i, xpv);
+#pragma unroll
+                for (int q = 0; q < R; ++q) rv[q] = rv[q] - alpha * xv[q] - beta * xpv[q];
+            }
+#pragma unroll
+            for (int q = 0; q < R; ++q) r2acc += abs2(rv[q]);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r2acc += __shfl_down_sync(0xffffffffu, r2acc, o);
+    if (lane == 0) red_r2[warp] = r2acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sacc = 0.0;
+        for (int w = 0; w < W; ++w) sacc += red_r2[w];
+        part_r2[blockIdx.x] = sacc;
+    }
+    if (last_block_arrived(ticket)) {
+        __shared__ C red_cols[kThreads];
+        __shared__ double red_r2x[32];
+        const int nb = gridDim.x;
+        const double h2 = reduce_columns(part, nb, m, h, red_cols);
+        const double r2 = sum_partials(part_r2, nb, red_r2x);
+        if (threadIdx.x == 0) {
+            out2[0] = r2;
+            out2[1] = h2;
+            *ticket = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Update for short vectors (few rows per thread): a block works on tiles of
 // 32 * R rows; its 8 warps take every 8th column of the tile, so each
 // thread's chain of dependent loads is m / 8 long instead of m, and the
@@ -686,7 +863,9 @@ void launch_project(T *const *cols, int m, long n_pad, const typename Store<T>::
                     Scratch &s, cudaStream_t st, int form_req) {
     using C = typename Store<T>::C;
     constexpr int R = Store<T>::R;
-    int nb = std::min(stream_blocks(n_pad, R), s.max_blocks);
+    // The staged form runs one block per SM (its ring fills shared memory).
+    const bool staged = form_req == kProjectAsync;
+    int nb = std::min(staged ? num_sms() : stream_blocks(n_pad, R), s.max_blocks);
     long per = (n_pad + nb - 1) / nb;
     long chunk = (per + 32 * R - 1) / (32 * R) * (32 * R);
     nb = (int)((n_pad + chunk - 1) / chunk);
@@ -696,6 +875,18 @@ void launch_project(T *const *cols, int m, long n_pad, const typename Store<T>::
         kern<<<nb, kThreads, 0, st>>>(cols, m, n_pad, chunk, r, rec, part, part_r2, s.tickets + kTicketProject, h,
                                       out2);
     };
+    if (staged) {
+        static const bool smem_ok = cudaFuncSetAttribute(k_project_async<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                         (int)kAsyncSmem) == cudaSuccess;
+        if (!smem_ok) {
+            std::fprintf(stderr, "trlan_b200: the staged projection cannot reserve %zu bytes of shared memory\n",
+                         kAsyncSmem);
+            return;
+        }
+        k_project_async<T><<<nb, kThreads, kAsyncSmem, st>>>(cols, m, n_pad, chunk, r, rec, part, part_r2,
+                                                            s.tickets + kTicketProject, h, out2);
+        return;
+    }
     if constexpr (std::is_same<C, double>::value) {
         // Forms (kProject*): 16 columns per warp keep one accumulator per
         // column for 128 columns per sweep (2 blocks/SM); 12 and 8 trade a

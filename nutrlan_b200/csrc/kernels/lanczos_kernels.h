@@ -42,12 +42,21 @@ template <class C>
 void launch_dot(const C *x, const C *y, long n_pad, double *out, Scratch &s,
                 cudaStream_t st);
 
-// Forms of the projection kernel: for FP64 storage 8, 12 or 16 columns per
-// warp, or 16 with the column-pointer table in shared memory (three
-// resident blocks per SM); for complex storage 8 columns per warp with the
-// table in registers (any form but the last) or in shared memory
-// (kProject16Shared); FP32 storage has one form.
-enum ProjectForm { kProjectDefault = 0, kProject8 = 1, kProject12 = 2, kProject16 = 3, kProject16Shared = 4 };
+// Forms of the projection kernel: for real storage (FP64 or FP32) 8, 12 or
+// 16 columns per warp, or 16 with the column-pointer table in shared memory;
+// for complex storage 8 columns per warp with the table in registers
+// (kProject8 .. kProject16) or in shared memory (kProject16Shared); for
+// every storage type, 16 columns per warp with the basis staged through a
+// shared-memory ring by cp.async, one block per SM (kProjectAsync).
+enum ProjectForm {
+    kProjectDefault = 0,
+    kProject8 = 1,
+    kProject12 = 2,
+    kProject16 = 3,
+    kProject16Shared = 4,
+    kProjectAsync = 5,
+    kProjectForms = 5
+};
 
 // h[c] = V[:,c]^H r for c < m; out2[0] = ||r||^2, out2[1] = ||h||^2.
 // form: a ProjectForm (kProjectDefault: 16 columns, or TRLX_PROJECT_CPW).

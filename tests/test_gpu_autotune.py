@@ -46,7 +46,7 @@ def test_autotune_keeps_the_faster_measured_forms(L):
         pm = t["project_ms"]
         assert t["project_form"] in pm and pm[t["project_form"]] == min(pm.values())
         pm32 = t["project32_ms"]
-        assert len(pm32) == 4 and min(pm32.values()) > 0
+        assert len(pm) == 5 and len(pm32) == 5 and min(pm32.values()) > 0
         assert pm32[t["project_form32"]] == min(pm32.values())
         assert t["columns"] == 32
         y = product(op, x)
@@ -65,11 +65,12 @@ def test_autotuned_solve_matches_reference():
     assert abs(r.info.matvec - g["matvec"]) <= 0.05 * g["matvec"]
 
 
-@pytest.mark.parametrize("form", [1, 2, 3, 4])
+@pytest.mark.parametrize("form", [1, 2, 3, 4, 5])
 def test_every_projection_form_solves_to_the_reference(form):
     """Each form the autotuner can keep (8, 12, 16 columns per warp; 16 with
-    the pointer table in shared memory), set on the operator, returns the
-    reference's Anderson 64^3 eigenvalues."""
+    the pointer table in shared memory; 16 staged through shared memory by
+    cp.async), set on the operator, returns the reference's Anderson 64^3
+    eigenvalues."""
     g = json.load(open(os.path.join(HERE, "golden", "config_runs.json")))["anderson64_full"]
     A = ops.anderson_3d(g["L"], W=g["W"], seed=g["pot_seed"])
     lib = load()
@@ -83,7 +84,7 @@ def test_every_projection_form_solves_to_the_reference(form):
     assert abs(r.info.matvec - g["matvec"]) <= 0.05 * g["matvec"]
 
 
-@pytest.mark.parametrize("form", [1, 2, 3, 4])
+@pytest.mark.parametrize("form", [1, 2, 3, 4, 5])
 def test_every_fp32_basis_projection_form_solves_to_the_reference(form):
     """The same over an FP32 basis (FP64 recurrence, dots and refinement),
     the form set with trlx_operator_set_project_form32: the reference's
@@ -105,11 +106,12 @@ def test_every_fp32_basis_projection_form_solves_to_the_reference(form):
     assert abs(r.info.matvec - g["matvec"]) <= 0.05 * g["matvec"] + 9 * 3 * g["ned"]
 
 
-@pytest.mark.parametrize("form", [0, 3, 4])
+@pytest.mark.parametrize("form", [0, 3, 4, 5])
 def test_complex_autotune_and_forms_solve_to_the_reference(form):
     """A complex operator tunes only its projection form (pointer table in
-    registers or in shared memory); with each form, and with the tuned one,
-    the Peierls 256^2 solve returns the reference's eigenvalues."""
+    registers or in shared memory, or the staged form); with each form, and
+    with the tuned one, the Peierls 256^2 solve returns the reference's
+    eigenvalues."""
     g = json.load(open(os.path.join(HERE, "golden", "config_runs.json")))["peierls256_full"]
     P = ops.peierls_2d(g["L"], phi=g["phi"], W=g["W"], seed=g["pot_seed"])
     lib = load()
@@ -118,9 +120,10 @@ def test_complex_autotune_and_forms_solve_to_the_reference(form):
         if form == 0:
             t = op.tune
             print(t)
-            assert t["spmv_forms_timed"] == 1 and set(t["project_ms"]) == {"cpw16", "cpw16_shared_ptrs"}
+            forms = {"cpw16", "cpw16_shared_ptrs", "cpw16_staged"}
+            assert t["spmv_forms_timed"] == 1 and set(t["project_ms"]) == forms
             assert t["project_ms"][t["project_form"]] == min(t["project_ms"].values())
-            assert set(t["project32_ms"]) == {"cpw16", "cpw16_shared_ptrs"}
+            assert set(t["project32_ms"]) == forms
             assert t["project32_ms"][t["project_form32"]] == min(t["project32_ms"].values())
         else:
             assert lib.trlx_operator_set_project_form(op.handle, form) == 0
@@ -133,9 +136,9 @@ def test_complex_autotune_and_forms_solve_to_the_reference(form):
     assert abs(r.info.matvec - g["matvec"]) <= 0.05 * g["matvec"]
 
 
-@pytest.mark.parametrize("form", [3, 4])
+@pytest.mark.parametrize("form", [3, 4, 5])
 def test_complex64_basis_forms_solve_to_the_reference(form):
-    """Both complex forms over a complex64 basis (complex128 recurrence, dots
+    """Each complex form over a complex64 basis (complex128 recurrence, dots
     and refinement), set with trlx_operator_set_project_form32."""
     from nutrlan_b200 import residual_norms
     g = json.load(open(os.path.join(HERE, "golden", "config_runs.json")))["peierls256_full"]
@@ -164,5 +167,5 @@ def test_autotune_rejects_operators_it_does_not_tune():
     assert lib.trlx_operator_set_project_form(None, 1) == -1
     assert lib.trlx_operator_set_project_form32(None, 1) == -1
     with DeviceOperator(A, fmt="csr") as op:
-        assert lib.trlx_operator_set_project_form32(op.handle, 5) == -1
+        assert lib.trlx_operator_set_project_form32(op.handle, 6) == -1
         assert lib.trlx_operator_set_project_form(op.handle, -1) == -1
