@@ -340,7 +340,7 @@ def run_complex(args, w, world, rank, local, pg):
     metric = f"Lanczos steps/s (SpMV + full CGS reorth), peierls{L} complex Hermitian, smallest {ned}"
     config = {"workload": f"peierls{L}: n={L * L}, flux 1/{int(round(1 / w['phi']))}, disorder "
                           f"U[-{w['W'] / 2:g},{w['W'] / 2:g}], ned={ned}, maxlan={maxlan}, tol={tol}, "
-                          f"complex CSR, basis c128, one thick-restart cycle/step",
+                          f"complex {{fmt}}, basis c128, one thick-restart cycle/step",
               "global_batch": world, "parallelism": f"replicas x{world}",
               "l2": "inputs larger than L2 (basis >= 6 GB, CSR 420 MB)"}
     A = ops.peierls_2d(L, phi=w["phi"], W=w["W"], seed=seed)
@@ -368,7 +368,7 @@ def run_complex(args, w, world, rank, local, pg):
                 mvs.append(mv)
         val = sum(mvs) / sum(times)
         ref_config = dict(config, workload=config["workload"].replace(
-            "complex CSR, basis c128, one thick-restart cycle/step",
+            "complex {fmt}, basis c128, one thick-restart cycle/step",
             f"complex CSR callback (OpenMP) + OpenBLAS; sample per step: the first {cpu_sample} Lanczos steps "
             f"of the same solve (maxlan=maxmv={cpu_sample}, reference ztrlan)"))
         print(json.dumps({"impl": "reference", "metric": metric, "value": val, "unit": "steps/s",
@@ -388,9 +388,10 @@ def run_complex(args, w, world, rank, local, pg):
     from nutrlan_b200 import load, TrlInfo, TrlxOptions, TrlxStats, DeviceOperator
     lib = load()
     mev = ned + 1
-    op = DeviceOperator(A, fmt="auto", maxlan=maxlan)        # tunes the projection form
+    op = DeviceOperator(A, fmt="auto", maxlan=maxlan)        # tunes the format and projection forms
     tuned_form = _form_index(op.tune, "project_form")
     tuned_form32 = _form_index(op.tune, "project_form32")
+    config["workload"] = config["workload"].replace("{fmt}", "SELL-C-32" if op.fmt == "zsell" else "CSR")
     config["autotune"] = op.tune
     evec = torch.zeros((mev, n), dtype=torch.complex128, device=dev)
     x0_dev = torch.as_tensor(x0, device=dev)
@@ -415,12 +416,13 @@ def run_complex(args, w, world, rank, local, pg):
             raise RuntimeError(f"ztrlan stat {info.stat}")
         return info.matvec
 
-    def timed(bits, profile):
+    def timed(bits, profile, oper=None):
+        oper = oper or op
         opts = options(bits, profile)
         info = TrlInfo()
         for _ in range(args.warmup):
             evec[0].copy_(x0_dev)
-            call(info, opts, maxlan, evec.data_ptr(), op.handle.value, op.applier)
+            call(info, opts, maxlan, evec.data_ptr(), oper.handle.value, oper.applier)
         torch.cuda.synchronize()
         barrier(pg)
         sampler = ClockSampler(local) if profile else None
@@ -432,7 +434,7 @@ def run_complex(args, w, world, rank, local, pg):
         e0.record()
         for _ in range(args.steps):
             evec[0].copy_(x0_dev)
-            mv += call(info, opts, maxlan, evec.data_ptr(), op.handle.value, op.applier)
+            mv += call(info, opts, maxlan, evec.data_ptr(), oper.handle.value, oper.applier)
             lib.trlx_get_last_stats(C.byref(stats))
             kt += np.array(stats.kernel_seconds[:])
             kb += np.array(stats.kernel_bytes[:])
@@ -457,7 +459,13 @@ def run_complex(args, w, world, rank, local, pg):
                 "spmv_plus_reorth_GBps": float((kb[0] + kb[1] + kb[2]) / max(kt[0] + kt[1] + kt[2], 1e-30) / 1e9)}
     variants = {}
     if not args.no_variants:
-        variants["zcsr_c64"] = timed(32, 0)[0]
+        variants[f"{op.fmt}_c64"] = timed(32, 0)[0]
+        # The format the autotuner did not keep, with the same projection forms.
+        other = "zcsr" if op.fmt == "zsell" else "zsell"
+        with DeviceOperator(A, fmt=other) as oop:
+            lib.trlx_operator_set_project_form(oop.handle, tuned_form)
+            lib.trlx_operator_set_project_form32(oop.handle, tuned_form32)
+            variants[f"{other}_c128"] = timed(64, 0, oop)[0]
 
     e2e = None
     if not args.no_e2e:
@@ -468,7 +476,12 @@ def run_complex(args, w, world, rank, local, pg):
 
         def e2e_call():
             h = C.c_void_p()
-            lib.trlx_zcsr_create(n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, 0, C.byref(h))
+            if op.fmt == "zsell":
+                rc = lib.trlx_zsell_create(n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, 1, 0, C.byref(h))
+            else:
+                rc = lib.trlx_zcsr_create(n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, 0, C.byref(h))
+            if rc != 0:
+                raise RuntimeError(f"complex operator creation from host arrays failed ({rc})")
             lib.trlx_operator_set_project_form(h, tuned_form)
             lib.trlx_operator_set_project_form32(h, tuned_form32)
             hev[0] = x0

@@ -44,6 +44,12 @@ int trlx_zcsr_create(int nrow, const long long *row_ptr, const int *col_idx,
                      const trl_dcomplex *val, int where,
                      trlx_operator **out);
 
+/* Complex SELL-C-sigma (C = 32, values complex128), built like
+   trlx_sell_create. */
+int trlx_zsell_create(int nrow, const long long *row_ptr, const int *col_idx,
+                      const trl_dcomplex *val, int sigma, int where,
+                      trlx_operator **out);
+
 /* Waits for the device (like cudaFree), then returns the operator's memory
    to the library's device pool. */
 void trlx_operator_destroy(trlx_operator *op);
@@ -53,23 +59,21 @@ long long trlx_operator_nnz(const trlx_operator *op);
 int trlx_operator_nrow(const trlx_operator *op);
 
 /* Single-solve autotuner (no counterpart in the reference, whose operator
-   is an opaque callback).  For a real operator created with
-   trlx_csr_create (not distributed) it times, on the current GPU, one fused
-   product y = A x + alpha in the CSR form and in the SELL-C-32 form built
-   from the same device arrays, and one Gram-Schmidt projection over
+   is an opaque callback).  For an operator created with trlx_csr_create or
+   trlx_zcsr_create (not distributed) it times, on the current GPU, one
+   fused product y = A x + alpha in the CSR form and in the SELL-C-32 form
+   built from the same device arrays, and one Gram-Schmidt projection over
    maxlan / 2 columns of the operator's row count in each of the projection
-   kernel's forms (median of 5 launches each), over FP64 columns and again
-   over FP32 columns (the two basis storage widths of
-   trlx_options.basis_bits); for a complex operator (trlx_zcsr_create) only
-   the projection forms 3, 4 and 5, over complex128 and complex64 columns
-   (the others report -1 ms).  It keeps the faster operator
+   kernel's forms (median of 5 launches each), over 64-bit columns and again
+   over 32-bit columns (the two basis storage widths of
+   trlx_options.basis_bits); complex operators have the projection forms 3,
+   4 and 5 only (the others report -1 ms).  It keeps the faster operator
    form (storage switched in place, the handle stays valid) and the faster
    projection form for each basis width for every later solve with this
    operator (call it before, not during, solves that use the operator).
-   Temporary
-   device memory: two vectors and the projection's columns (at most a
-   quarter of the free memory).  Returns 0, -1 for an operator it does not
-   tune (SELL-created or distributed), -2 if the temporary memory
+   Temporary device memory: two vectors and the projection's columns (at
+   most a quarter of the free memory).  Returns 0, -1 for an operator it
+   does not tune (SELL-created or distributed), -2 if the temporary memory
    cannot be allocated, -3 on a CUDA error. */
 typedef struct {
     int format;            /* kept operator form: 0 CSR, 1 SELL-C-32        */

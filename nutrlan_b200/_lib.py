@@ -85,9 +85,10 @@ def _declare(lib):
         f = getattr(lib, name)
         f.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_int, P(c_void_p)]
         f.restype = c_int
-    lib.trlx_sell_create.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_int, c_int,
-                                     P(c_void_p)]
-    lib.trlx_sell_create.restype = c_int
+    for name in ("trlx_sell_create", "trlx_zsell_create"):
+        f = getattr(lib, name)
+        f.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, P(c_void_p)]
+        f.restype = c_int
     lib.trlx_operator_destroy.argtypes = [c_void_p]
     lib.trlx_operator_destroy.restype = None
     lib.trlx_operator_nnz.argtypes = [c_void_p]

@@ -451,7 +451,7 @@ int Engine<T>::setup() {
         if ((void *)op_ == (void *)&trlx_matvec && info_->mvparam) builtin_ = static_cast<trlx_operator *>(info_->mvparam);
     }
     if (builtin_) {
-        if (builtin_->nrow != nrow_ || (builtin_->kind == 2) != kComplex) {
+        if (builtin_->nrow != nrow_ || trlb::op_complex(builtin_) != kComplex) {
             std::fprintf(stderr, "TRLAN-B200: built-in operator does not match the problem.\n");
             return -6;
         }
@@ -1141,7 +1141,7 @@ int Engine<T>::spec_segment(int *jnd_io, int S, int kept) {
         cudaEventRecord(ev_[6], st_);
         // Short CSR problems: the whole run in one cooperative kernel.
         bool done = false;
-        if (builtin_->kind != 1 && n_pad_ <= (1L << 18)) {
+        if (!trlb::op_sell(builtin_) && n_pad_ <= (1L << 18)) {
             const char *e = std::getenv("TRLX_COOP");
             if (!(e && e[0] == '0')) {
                 const long part_elems = (long)scratch_.max_blocks * (P_ + 2) * (long)(sizeof(zd) / sizeof(C));

@@ -567,111 +567,13 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
-// ---------------------------------------------------------------------------
-// out[:,k] = sum_c in[:,c] Y[c,k] (FP64 accumulate): output tiles of
-// 128 rows x BN columns, K in steps of 16 staged through shared memory with
-// the next K-slice prefetched into registers while the current one is used.
-// Thread (tx, ty) owns rows ty + 16 q (q < 8) and columns tx + TX p
-// (p < BN / TX), TX = 16 for BN = 64 and 8 for BN = 32, so a restart that
-// keeps <= 32 vectors does not compute a half-empty tile.
-constexpr int kBM = 128, kBK = 16;
-
-template <int BN>
-struct RitzShape {
-    static constexpr int TX = BN == 64 ? 16 : 8;      // threads along columns
-    static constexpr int TY = kThreads / TX;          // threads along rows
-    static constexpr int QR = kBM / TY;               // rows per thread
-    static constexpr int PC = BN / TX;                // columns per thread
-};
-
-template <class T, class OutT, int BN>
-__global__ void __launch_bounds__(kThreads)
-    k_ritz(T *const *__restrict__ in_cols, int jml, const double *__restrict__ Y, int ldy, int kept,
-           OutT *const *out_cols, OutT *out, long ldo, long n_valid) {
-    using S = Store<T>;
-    using C = typename S::C;
-    using Sh = RitzShape<BN>;
-    __shared__ C As[kBK][kBM + 1];
-    __shared__ double Bs[kBK][BN + 1];
-    const int t = threadIdx.x, tx = t % Sh::TX, ty = t / Sh::TX;
-    const long i0 = (long)blockIdx.x * kBM;
-    const int k0 = blockIdx.y * BN;
-    // A loads: 16 columns x 128 rows = 2048 elements, 8 per thread:
-    // column kk = t / 16, rows (t % 16) * 8 .. +8.
-    const int a_kk = t >> 4, a_rr = (t & 15) * 8;
-    C areg[8];
-    double breg[BN * kBK / kThreads];
-    auto load_tiles = [&](int c0) {
-        const int c = c0 + a_kk;
-        if (c < jml) {
-            const T *col = in_cols[c] + i0 + a_rr;
-#pragma unroll
-            for (int q = 0; q < 8; ++q) areg[q] = S::to_c(col[q]);
-        } else {
-#pragma unroll
-            for (int q = 0; q < 8; ++q) areg[q] = czero(C());
-        }
-#pragma unroll
-        for (int e = 0; e < BN * kBK / kThreads; ++e) {
-            const int idx = t + e * kThreads;
-            const int kk = idx / BN, kc = idx % BN;
-            const int cc = c0 + kk, k = k0 + kc;
-            breg[e] = (cc < jml && k < kept) ? Y[(long)cc + (long)k * ldy] : 0.0;
-        }
-    };
-    C acc[Sh::QR][Sh::PC];
-#pragma unroll
-    for (int q = 0; q < Sh::QR; ++q)
-#pragma unroll
-        for (int p = 0; p < Sh::PC; ++p) acc[q][p] = czero(C());
-    load_tiles(0);
-    for (int c0 = 0; c0 < jml; c0 += kBK) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) As[a_kk][a_rr + q] = areg[q];
-#pragma unroll
-        for (int e = 0; e < BN * kBK / kThreads; ++e) {
-            const int idx = t + e * kThreads;
-            Bs[idx / BN][idx % BN] = breg[e];
-        }
-        __syncthreads();
-        if (c0 + kBK < jml) load_tiles(c0 + kBK);
-#pragma unroll
-        for (int kk = 0; kk < kBK; ++kk) {
-            C a[Sh::QR];
-            double b[Sh::PC];
-#pragma unroll
-            for (int q = 0; q < Sh::QR; ++q) a[q] = As[kk][ty + Sh::TY * q];
-#pragma unroll
-            for (int p = 0; p < Sh::PC; ++p) b[p] = Bs[kk][tx + Sh::TX * p];
-#pragma unroll
-            for (int q = 0; q < Sh::QR; ++q)
-#pragma unroll
-                for (int p = 0; p < Sh::PC; ++p) fma_real(acc[q][p], a[q], b[p]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int p = 0; p < Sh::PC; ++p) {
-        const int k = k0 + tx + Sh::TX * p;
-        if (k >= kept) continue;
-        OutT *dst = out_cols ? out_cols[k] : out + (long)k * ldo;
-#pragma unroll
-        for (int q = 0; q < Sh::QR; ++q) {
-            const long row = i0 + ty + Sh::TY * q;
-            if (row < n_valid) {
-                if constexpr (std::is_same<OutT, C>::value) {
-                    dst[row] = acc[q][p];
-                } else {
-                    dst[row] = S::from_c(acc[q][p]);
-                }
-            }
-        }
-    }
-}
+constexpr int kBK = 16;  // K columns per shared-memory stage of the Ritz product
 
 // ---------------------------------------------------------------------------
-// Real bases: the same product on the FP64 tensor-core instruction
-// (mma.sync.m8n8k4.f64).  A block of 8 warps computes BM x BN outputs; each
+// Restart recombination out[:,k] = sum_c in[:,c] Y[c,k] with a real Y (FP64
+// accumulate) on the FP64 tensor-core instruction (mma.sync.m8n8k4.f64;
+// FP64 has no tcgen05 kind).  Complex bases use it through their real view
+// (ritz_dispatch).  A block of 8 warps computes BM x BN outputs; each
 // warp owns a 32 x 32 tile (4 x 4 mma tiles of 8 x 8, 32 accumulators per
 // thread), so 8 fragment loads from shared memory feed 16 mma (4096 FMAs).
 // K advances 16 columns per shared-memory stage (4 mma k-steps) with the
@@ -952,11 +854,35 @@ void launch_normalize(typename Store<T>::C *r, long n_pad, const double *r2, dou
     k_normalize<T><<<elementwise_blocks(n_pad), kThreads, 0, st>>>(r, n_pad, r2, fixed, q, vcol);
 }
 
+// The real scalar type of a storage or compute type (complex: its parts).
+template <class X>
+struct RealView {
+    using type = X;
+};
+template <>
+struct RealView<zd> {
+    using type = double;
+};
+template <>
+struct RealView<zf> {
+    using type = float;
+};
+
 template <class T, class OutT>
 void ritz_dispatch(T *const *in_cols, int jml, long n_pad, const double *Y, int ldy, int kept, OutT *const *out_cols,
                    OutT *out, long ldo, long n_valid, cudaStream_t st) {
     if (kept <= 0) return;
-    if constexpr (std::is_same<typename Store<T>::C, double>::value) {
+    if constexpr (!std::is_same<typename RealView<T>::type, T>::value) {
+        // A complex column times a real Y is the real product of its
+        // interleaved (re, im) view: 2 n_pad real rows, the same for the
+        // output columns (2 ldo, 2 n_valid).
+        using RT = typename RealView<T>::type;
+        using RO = typename RealView<OutT>::type;
+        ritz_dispatch<RT, RO>(reinterpret_cast<RT *const *>(in_cols), jml, 2 * n_pad, Y, ldy, kept,
+                              reinterpret_cast<RO *const *>(out_cols), reinterpret_cast<RO *>(out), 2 * ldo,
+                              2 * n_valid, st);
+        return;
+    } else {
         if (kept <= 32) {
             k_ritz_mma<T, OutT, 32><<<dim3((unsigned)(n_pad / MmaShape<32>::BM), 1), kThreads, 0, st>>>(
                 in_cols, jml, Y, ldy, kept, out_cols, out, ldo, n_valid);
@@ -965,14 +891,6 @@ void ritz_dispatch(T *const *in_cols, int jml, long n_pad, const double *Y, int 
             k_ritz_mma<T, OutT, 64><<<grid, kThreads, 0, st>>>(in_cols, jml, Y, ldy, kept, out_cols, out, ldo,
                                                                 n_valid);
         }
-        return;
-    }
-    const unsigned gx = (unsigned)(n_pad / kBM);
-    if (kept <= 32) {
-        k_ritz<T, OutT, 32><<<dim3(gx, 1), kThreads, 0, st>>>(in_cols, jml, Y, ldy, kept, out_cols, out, ldo, n_valid);
-    } else {
-        dim3 grid(gx, (unsigned)((kept + 63) / 64));
-        k_ritz<T, OutT, 64><<<grid, kThreads, 0, st>>>(in_cols, jml, Y, ldy, kept, out_cols, out, ldo, n_valid);
     }
 }
 

@@ -175,7 +175,7 @@ int normalized_sum(SeedWork &w, long n, int k, const double *gram, double *start
 extern "C" int trlx_seed_start(void *op, int nrow, int k, const float *Y, int project, double *start, double *theta,
                                double *res) {
     auto *A = static_cast<trlx_operator *>(op);
-    if (!A || !Y || !start || k < 1 || k > kMaxK || nrow < k || A->nrow != nrow || A->kind == 2) return -1;
+    if (!A || !Y || !start || k < 1 || k > kMaxK || nrow < k || A->nrow != nrow || trlb::op_complex(A)) return -1;
     SeedWork &w = g_work;
     if (!w.ensure(nrow, k)) return -5;
     const long n = nrow;

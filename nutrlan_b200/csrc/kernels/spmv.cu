@@ -136,10 +136,20 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+// acc + a * x (real: one FMA; complex: four).
+__device__ __forceinline__ double mac(double acc, double a, double x) { return fma(a, x, acc); }
+__device__ __forceinline__ zd mac(zd acc, zd a, zd x) {
+    return zd{fma(a.x, x.x, fma(-a.y, x.y, acc.x)), fma(a.x, x.y, fma(a.y, x.x, acc.y))};
+}
+// aacc + Re(conj(x) * y).
+__device__ __forceinline__ double alpha_add(double aacc, double x, double y) { return fma(x, y, aacc); }
+__device__ __forceinline__ double alpha_add(double aacc, zd x, zd y) { return fma(x.x, y.x, fma(x.y, y.y, aacc)); }
+
+template <class V>
 __global__ void __launch_bounds__(kThreads)
     k_sell(int nrow, long n_pad, int nslice, const long long *__restrict__ sp,
-           const int *__restrict__ ci, const double *__restrict__ va, const int *__restrict__ perm,
-           const double *__restrict__ x, double *__restrict__ y, double *part, unsigned *ticket,
+           const int *__restrict__ ci, const V *__restrict__ va, const int *__restrict__ perm,
+           const V *__restrict__ x, V *__restrict__ y, double *part, unsigned *ticket,
            double *alpha_out) {
     const int lane = threadIdx.x & 31;
     const long warps = (long)gridDim.x * (kThreads / 32);
@@ -147,21 +157,21 @@ __global__ void __launch_bounds__(kThreads)
     for (long s = (long)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); s < nslice; s += warps) {
         const long b = sp[s];
         const int w = (int)((sp[s + 1] - b) >> 5);
-        double acc = 0.0;
-        const double *v = va + b + lane;
+        V acc = czero(V());
+        const V *v = va + b + lane;
         const int *c = ci + b + lane;
 #pragma unroll 4
-        for (int k = 0; k < w; ++k) acc = fma(__ldg(v + (long)k * 32), __ldg(x + __ldg(c + (long)k * 32)), acc);
+        for (int k = 0; k < w; ++k) acc = mac(acc, ldg_c(v + (long)k * 32), ldg_c(x + __ldg(c + (long)k * 32)));
         const long srow = s * 32 + lane;
         if (srow < nrow) {
             const int row = perm ? perm[srow] : (int)srow;
             y[row] = acc;
-            if (alpha_out) aacc = fma(__ldg(x + row), acc, aacc);
+            if (alpha_out) aacc = alpha_add(aacc, ldg_c(x + row), acc);
         }
     }
     // Zero the padding rows [nrow, n_pad).
     for (long i = nrow + (long)blockIdx.x * kThreads + threadIdx.x; i < n_pad; i += (long)gridDim.x * kThreads)
-        y[i] = 0.0;
+        y[i] = czero(V());
     if (!alpha_out) return;
     __shared__ double red[32];
     double s2 = block_sum(aacc, red);
@@ -224,9 +234,9 @@ void spmv_fused_real(const trlx_operator *A, const double *x, double *y, long n_
     } else {
         int nb = spmv_blocks((long)A->nslice * 32, kThreads);
         if (s) nb = std::min(nb, s->max_blocks);
-        k_sell<<<nb, kThreads, 0, st>>>(A->nrow, n_pad, A->nslice, A->slice_ptr, A->col,
-                                        static_cast<const double *>(A->val), A->perm, x, y, part, tk,
-                                        alpha_out);
+        k_sell<double><<<nb, kThreads, 0, st>>>(A->nrow, n_pad, A->nslice, A->slice_ptr, A->col,
+                                                static_cast<const double *>(A->val), A->perm, x, y, part, tk,
+                                                alpha_out);
     }
 }
 
@@ -234,6 +244,13 @@ void spmv_fused_cplx(const trlx_operator *A, const zd *x, zd *y, long n_pad, dou
                      Scratch *s, cudaStream_t st) {
     double *part = s ? reinterpret_cast<double *>(s->partials) : nullptr;
     unsigned *tk = s ? s->tickets + kTicketSpmv : nullptr;
+    if (A->kind == 3) {
+        int nb = spmv_blocks((long)A->nslice * 32, kThreads);
+        if (s) nb = std::min(nb, s->max_blocks);
+        k_sell<zd><<<nb, kThreads, 0, st>>>(A->nrow, n_pad, A->nslice, A->slice_ptr, A->col,
+                                            static_cast<const zd *>(A->val), A->perm, x, y, part, tk, alpha_out);
+        return;
+    }
     if (use_row_tiles(n_pad)) {
         int nb = spmv_blocks(n_pad, kThreads);
         if (s) nb = std::min(nb, s->max_blocks);
@@ -255,7 +272,7 @@ void spmv_plain(const trlx_operator *A, const void *x, void *y, cudaStream_t st)
         spmv_fused_real(A, xe, static_cast<double *>(y), A->nrow, nullptr, nullptr, st);
         return;
     }
-    if (A->kind == 2)
+    if (op_complex(A))
         spmv_fused_cplx(A, static_cast<const zd *>(x), static_cast<zd *>(y), A->nrow, nullptr, nullptr, st);
     else
         spmv_fused_real(A, static_cast<const double *>(x), static_cast<double *>(y), A->nrow, nullptr,
@@ -263,9 +280,9 @@ void spmv_plain(const trlx_operator *A, const void *x, void *y, cudaStream_t st)
 }
 
 double spmv_bytes(const trlx_operator *A) {
-    const double vs = A->kind == 2 ? 16.0 : 8.0;
+    const double vs = op_complex(A) ? 16.0 : 8.0;
     double b = (double)A->nnz * (vs + 4.0) + 2.0 * vs * A->nrow;
-    if (A->kind == 1)
+    if (op_sell(A))
         b += 8.0 * (A->nslice + 1) + (A->perm ? 4.0 * A->nrow : 0.0);
     else
         b += 8.0 * (A->nrow + 1.0);
@@ -386,9 +403,10 @@ __global__ void k_slice_width(int nrow, int nslice, const long long *__restrict_
     }
 }
 
+template <class V>
 __global__ void k_sell_fill(int nrow, int nslice, const long long *__restrict__ rp, const int *__restrict__ ci,
-                            const double *__restrict__ va, const int *__restrict__ perm,
-                            const long long *__restrict__ sp, int *__restrict__ sc, double *__restrict__ sv) {
+                            const V *__restrict__ va, const int *__restrict__ perm,
+                            const long long *__restrict__ sp, int *__restrict__ sc, V *__restrict__ sv) {
     const int lane = threadIdx.x & 31;
     const long warps = ((long)gridDim.x * blockDim.x) >> 5;
     for (long s = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nslice; s += warps) {
@@ -406,7 +424,7 @@ __global__ void k_sell_fill(int nrow, int nslice, const long long *__restrict__ 
                 sv[d] = va[beg + k];
             } else {
                 sc[d] = pad_col;
-                sv[d] = 0.0;
+                sv[d] = czero(V());
             }
         }
     }
@@ -427,9 +445,10 @@ void launch_slice_width(int nrow, int nslice, const long long *rp, const int *pe
     k_slice_width<<<grid, 256>>>(nrow, nslice, rp, perm, width);
 }
 
-void launch_sell_fill(int nrow, int nslice, const long long *rp, const int *ci, const double *va, const int *perm,
-                      const long long *sp, int *sc, double *sv, int grid) {
-    k_sell_fill<<<grid, 256>>>(nrow, nslice, rp, ci, va, perm, sp, sc, sv);
+template <class V>
+void launch_sell_fill(int nrow, int nslice, const long long *rp, const int *ci, const V *va, const int *perm,
+                      const long long *sp, int *sc, V *sv, int grid) {
+    k_sell_fill<V><<<grid, 256>>>(nrow, nslice, rp, ci, va, perm, sp, sc, sv);
 }
 
 }  // namespace trlb
@@ -586,8 +605,12 @@ extern "C" int trlx_zcsr_create(int nrow, const long long *row_ptr, const int *c
     return 0;
 }
 
-extern "C" int trlx_sell_create(int nrow, const long long *row_ptr, const int *col_idx,
-                                const double *val, int sigma, int where, trlx_operator **out) {
+namespace {
+
+// SELL-C-32 from CSR input with values of type V (double: kind 1, zd: kind 3).
+template <class V>
+int sell_create(int nrow, const long long *row_ptr, const int *col_idx, const V *val, int sigma, int where,
+                int kind, trlx_operator **out) {
     if (!out || check_csr(nrow, row_ptr, col_idx, val)) return -1;
     if (sigma < 1) sigma = 1;
     const bool dev = where == TRLX_DEVICE_ARRAYS;
@@ -614,7 +637,7 @@ extern "C" int trlx_sell_create(int nrow, const long long *row_ptr, const int *c
         if (identity) order.clear();
     }
     auto *A = new trlx_operator();
-    A->kind = 1;
+    A->kind = kind;
     A->nrow = nrow;
     A->nslice = (nrow + 31) / 32;
     A->sigma = sigma;
@@ -622,7 +645,7 @@ extern "C" int trlx_sell_create(int nrow, const long long *row_ptr, const int *c
     // CSR arrays on the device (the caller's own when they already are).
     long long *d_rp = dev ? const_cast<long long *>(row_ptr) : nullptr;
     int *d_ci = dev ? const_cast<int *>(col_idx) : nullptr;
-    double *d_va = dev ? const_cast<double *>(val) : nullptr;
+    V *d_va = dev ? const_cast<V *>(val) : nullptr;
     int *d_w = nullptr;
     int rc = 0;
     if (!dev) {
@@ -645,10 +668,10 @@ extern "C" int trlx_sell_create(int nrow, const long long *row_ptr, const int *c
     if (!rc) rc = to_device(sp.data(), sp.size(), TRLX_HOST_ARRAYS, &A->slice_ptr);
     const long long total = sp[nslice];
     A->nnz = total;
-    double *dv = nullptr;
+    V *dv = nullptr;
     if (!rc && (op_alloc(reinterpret_cast<void **>(&A->col), sizeof(int) * std::max<long long>(total, 1)) !=
                     cudaSuccess ||
-                op_alloc(reinterpret_cast<void **>(&dv), sizeof(double) * std::max<long long>(total, 1)) !=
+                op_alloc(reinterpret_cast<void **>(&dv), sizeof(V) * std::max<long long>(total, 1)) !=
                     cudaSuccess))
         rc = -2;
     A->val = dv;
@@ -669,6 +692,19 @@ extern "C" int trlx_sell_create(int nrow, const long long *row_ptr, const int *c
     }
     *out = A;
     return 0;
+}
+
+}  // namespace
+
+extern "C" int trlx_sell_create(int nrow, const long long *row_ptr, const int *col_idx,
+                                const double *val, int sigma, int where, trlx_operator **out) {
+    return sell_create<double>(nrow, row_ptr, col_idx, val, sigma, where, 1, out);
+}
+
+extern "C" int trlx_zsell_create(int nrow, const long long *row_ptr, const int *col_idx,
+                                 const trl_dcomplex *val, int sigma, int where, trlx_operator **out) {
+    return sell_create<trlb::zd>(nrow, row_ptr, col_idx, reinterpret_cast<const trlb::zd *>(val), sigma, where, 3,
+                                 out);
 }
 
 extern "C" void trlx_operator_destroy(trlx_operator *A) {
@@ -886,13 +922,13 @@ extern "C" int trlx_dist_sell_create(trlx_comm *comm, int nloc, const long long 
 extern "C" void trlx_matvec(const int nrow, const int ncol, const double *x, const int ldx, double *y,
                             const int ldy, void *mvparam) {
     auto *A = static_cast<trlx_operator *>(mvparam);
-    if (!A || A->kind == 2 || nrow != A->nrow) return;
+    if (!A || trlb::op_complex(A) || nrow != A->nrow) return;
     for (int j = 0; j < ncol; ++j) trlb::spmv_plain(A, x + (long)j * ldx, y + (long)j * ldy, 0);
 }
 
 extern "C" void trlx_zmatvec(const int nrow, const int ncol, const trl_dcomplex *x, const int ldx,
                              trl_dcomplex *y, const int ldy, void *mvparam) {
     auto *A = static_cast<trlx_operator *>(mvparam);
-    if (!A || A->kind != 2 || nrow != A->nrow) return;
+    if (!A || !trlb::op_complex(A) || nrow != A->nrow) return;
     for (int j = 0; j < ncol; ++j) trlb::spmv_plain(A, x + (long)j * ldx, y + (long)j * ldy, 0);
 }

@@ -1,4 +1,4 @@
-// Built-in sparse operators (CSR, SELL-C-sigma, complex CSR) and their
+// Built-in sparse operators (CSR and SELL-C-sigma, real and complex) and their
 // fused product kernels.  The engine calls spmv_fused() when the user's
 // `op` is trlx_matvec / trlx_zmatvec; the fused kernel produces y = A x and
 // alpha = Re(x^H y) in one pass over the matrix (the reference computes the
@@ -14,7 +14,7 @@ struct Halo;
 }
 
 struct trlx_operator {
-    int kind = 0;  // 0 real CSR, 1 real SELL-C-32, 2 complex CSR
+    int kind = 0;  // 0 real CSR, 1 real SELL-C-32, 2 complex CSR, 3 complex SELL-C-32
     int nrow = 0;
     long long nnz = 0;
     // CSR
@@ -40,6 +40,9 @@ struct trlx_operator {
 };
 
 namespace trlb {
+
+inline bool op_complex(const trlx_operator *A) { return A->kind == 2 || A->kind == 3; }
+inline bool op_sell(const trlx_operator *A) { return A->kind == 1 || A->kind == 3; }
 
 // y = A x and, if alpha_out != null, *alpha_out = Re(x^H y) (deterministic).
 // x, y are compute vectors of n_pad rows (padding rows of y are written 0).

@@ -23,13 +23,14 @@ from ._lib import load, TrlxStats, TrlxOptions, TrlxTuneResult
 
 
 class DeviceOperator:
-    """A trlx_operator (CSR, SELL-C-32 or complex CSR) resident on the GPU.
+    """A trlx_operator (CSR or SELL-C-32, real or complex) resident on the
+    GPU.
 
     ``fmt="auto"`` creates the CSR form and runs trlx_operator_autotune
-    (``maxlan`` sets the projection width it times): a real operator keeps
-    the faster of CSR and SELL-C-32, and every operator the faster
-    projection kernel form for its solves; ``self.tune`` holds what was
-    measured."""
+    (``maxlan`` sets the projection width it times): the operator keeps the
+    faster of CSR and SELL-C-32 and the faster projection kernel forms for
+    its solves; ``self.tune`` holds what was measured.  ``self.fmt`` is
+    "csr"/"sell" for real and "zcsr"/"zsell" for complex operators."""
 
     def __init__(self, csr, fmt="csr", sigma=1, maxlan=128):
         lib = load()
@@ -43,7 +44,11 @@ class DeviceOperator:
         self.handle = C.c_void_p()
         rp = np.ascontiguousarray(csr.row_ptr, np.int64)
         ci = np.ascontiguousarray(csr.col, np.int32)
-        if self.complex:
+        if self.complex and fmt in ("sell", "zsell"):
+            va = np.ascontiguousarray(csr.val, np.complex128)
+            rc = lib.trlx_zsell_create(csr.n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data,
+                                       int(sigma), 0, C.byref(self.handle))
+        elif self.complex:
             va = np.ascontiguousarray(csr.val, np.complex128)
             rc = lib.trlx_zcsr_create(csr.n, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, 0,
                                       C.byref(self.handle))
@@ -57,7 +62,8 @@ class DeviceOperator:
                                      C.byref(self.handle))
         if rc != 0:
             raise RuntimeError(f"trlx operator creation failed ({rc})")
-        self.fmt = "zcsr" if self.complex else fmt
+        fmt = "sell" if fmt == "zsell" else ("csr" if fmt == "zcsr" else fmt)
+        self.fmt = ("z" + fmt) if self.complex else fmt
         if auto:
             res = TrlxTuneResult()
             rc = lib.trlx_operator_autotune(self.handle, int(maxlan), C.byref(res))
@@ -65,7 +71,7 @@ class DeviceOperator:
                 self.close()
                 raise RuntimeError(f"trlx_operator_autotune failed ({rc})")
             self.tune = res.as_dict()
-            self.fmt = self.tune["format"]
+            self.fmt = ("z" if self.complex else "") + self.tune["format"]
         self.nnz = lib.trlx_operator_nnz(self.handle)
         # The exported applier, used as `op` so the engine takes its fused path.
         name = "trlx_zmatvec" if self.complex else "trlx_matvec"

@@ -108,10 +108,10 @@ def test_every_fp32_basis_projection_form_solves_to_the_reference(form):
 
 @pytest.mark.parametrize("form", [0, 3, 4, 5])
 def test_complex_autotune_and_forms_solve_to_the_reference(form):
-    """A complex operator tunes only its projection form (pointer table in
-    registers or in shared memory, or the staged form); with each form, and
-    with the tuned one, the Peierls 256^2 solve returns the reference's
-    eigenvalues."""
+    """A complex operator tunes its format (complex CSR or SELL-C-32) and
+    its projection form (pointer table in registers or in shared memory, or
+    the staged form); with each form, and with the tuned ones, the Peierls
+    256^2 solve returns the reference's eigenvalues."""
     g = json.load(open(os.path.join(HERE, "golden", "config_runs.json")))["peierls256_full"]
     P = ops.peierls_2d(g["L"], phi=g["phi"], W=g["W"], seed=g["pot_seed"])
     lib = load()
@@ -121,7 +121,9 @@ def test_complex_autotune_and_forms_solve_to_the_reference(form):
             t = op.tune
             print(t)
             forms = {"cpw16", "cpw16_shared_ptrs", "cpw16_staged"}
-            assert t["spmv_forms_timed"] == 1 and set(t["project_ms"]) == forms
+            assert t["spmv_forms_timed"] == 2 and set(t["project_ms"]) == forms
+            assert t["spmv_ms"][t["format"]] == min(t["spmv_ms"].values())
+            assert op.fmt == "z" + t["format"]
             assert t["project_ms"][t["project_form"]] == min(t["project_ms"].values())
             assert set(t["project32_ms"]) == forms
             assert t["project32_ms"][t["project_form32"]] == min(t["project32_ms"].values())

@@ -117,10 +117,11 @@ def _peierls_start(n):
     return ops.start_vector(n) + 1j * ops.start_vector(n, seed=99)
 
 
-def test_peierls2048_one_cycle_matches_reference():
+@pytest.mark.parametrize("fmt", ["zcsr", "zsell"])
+def test_peierls2048_one_cycle_matches_reference(fmt):
     g = GOLD["peierls2048_cycle"]
     A = ops.peierls_2d(g["L"], phi=g["phi"], W=g["W"], seed=g["pot_seed"])
-    with DeviceOperator(A) as op:
+    with DeviceOperator(A, fmt=fmt) as op:
         r = solve(op, ned=g["ned"], maxlan=g["maxlan"], maxmv=g["maxmv"], tol=1e-8, restart=g["restart"],
                   start=_peierls_start(A.n), mev=g["mev"], device=True)
     del r.evec
@@ -129,14 +130,15 @@ def test_peierls2048_one_cycle_matches_reference():
     assert r.stat == g["stat"]
     assert (r.nec, r.info.matvec, r.info.nloop) == (g["nec"], g["matvec"], g["nloop"])
     rel = _rel(r.eval[:k], g["eval"])
-    print(f"peierls2048: max rel Ritz-value diff {rel:.2e}")
+    print(f"peierls2048 {fmt}: max rel Ritz-value diff {rel:.2e}")
     assert rel <= RITZ_RTOL
 
 
-def test_peierls256_full_solve_matches_reference():
+@pytest.mark.parametrize("fmt", ["zcsr", "zsell"])
+def test_peierls256_full_solve_matches_reference(fmt):
     g = GOLD["peierls256_full"]
     A = ops.peierls_2d(g["L"], phi=g["phi"], W=g["W"], seed=g["pot_seed"])
-    _full_solve_check(g, A, _peierls_start(A.n), cplx=True)
+    _full_solve_check(g, A, _peierls_start(A.n), cplx=True, fmt=fmt)
 
 
 def test_batched_sample_matches_reference():

@@ -118,13 +118,15 @@ def test_builtin_operator_matches_csr_product(fmt, family):
     np.testing.assert_allclose(dy.cpu().numpy(), want, rtol=1e-13, atol=1e-12)
 
 
-def test_complex_operator_matches_csr_product():
+@pytest.mark.parametrize("fmt,sigma", [("zcsr", 1), ("zsell", 1), ("zsell", 16)])
+def test_complex_operator_matches_csr_product(fmt, sigma):
     lib = load()
     A = ops.peierls_2d(32, phi=1.0 / 8.0)
     rng = np.random.default_rng(4)
     x = rng.standard_normal(A.n) + 1j * rng.standard_normal(A.n)
     want = K.csr_matvec(A.row_ptr, A.col, A.val, x)
-    with DeviceOperator(A) as op:
+    with DeviceOperator(A, fmt=fmt, sigma=sigma) as op:
+        assert op.fmt == fmt
         dx, dy = dev(x), torch.zeros(A.n, dtype=torch.complex128, device="cuda")
         lib.trlx_zmatvec.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                      C.c_void_p]
@@ -133,3 +135,35 @@ def test_complex_operator_matches_csr_product():
     np.testing.assert_allclose(dy.cpu().numpy(), want, atol=1e-12)
     # Hermitian: x^H A x is real
     assert abs(np.vdot(x, want).imag) < 1e-9 * abs(np.vdot(x, want))
+
+
+@pytest.mark.parametrize("sigma", [1, 64])
+def test_complex_sell_ragged_rows_match_csr_product(sigma):
+    """Complex SELL-C-32 on rows of very different lengths (empty rows, one
+    row of 900 entries; sigma = 64 sorts rows within windows and stores the
+    permutation) against the CSR product on the host."""
+    lib = load()
+    rng = np.random.default_rng(12)
+    n = 2999
+    lens = rng.integers(0, 40, n)
+    lens[::89] = 0
+    lens[7] = 900
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    col = rng.integers(0, n, rp[-1]).astype(np.int32)
+    val = rng.standard_normal(rp[-1]) + 1j * rng.standard_normal(rp[-1])
+    A = ops.CSR(n, rp, col, val)
+    x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    want = K.csr_matvec(rp, col, val, x)
+    with DeviceOperator(A, fmt="zsell", sigma=sigma) as op:
+        assert op.nnz >= rp[-1]
+        dx, dy = dev(x), torch.zeros(n, dtype=torch.complex128, device="cuda")
+        lib.trlx_zmatvec.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                     C.c_void_p]
+        lib.trlx_zmatvec(n, 1, dx.data_ptr(), n, dy.data_ptr(), n, op.handle)
+        # A complex operator is not a real one: trlx_matvec leaves y alone.
+        dz = torch.full((n,), 7.0, dtype=torch.float64, device="cuda")
+        lib.trlx_matvec.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+        lib.trlx_matvec(n, 1, dz.data_ptr(), n, dz.data_ptr(), n, op.handle)
+        torch.cuda.synchronize()
+    np.testing.assert_allclose(dy.cpu().numpy(), want, rtol=1e-13, atol=1e-12)
+    assert torch.all(dz == 7.0)
