@@ -62,9 +62,11 @@ int trlx_operator_nrow(const trlx_operator *op);
    is an opaque callback).  For an operator created with trlx_csr_create or
    trlx_zcsr_create (not distributed) it times, on the current GPU, one
    fused product y = A x + alpha in the CSR form and in the SELL-C-32 form
-   built from the same device arrays, and one Gram-Schmidt projection over
-   maxlan / 2 columns of the operator's row count in each of the projection
-   kernel's forms (median of 5 launches each), over 64-bit columns and again
+   built from the same device arrays, and Gram-Schmidt projections over
+   maxlan / 4, maxlan / 2 and 3 maxlan / 4 columns (at most 32, 64 and 96)
+   of the operator's row count in each of the projection kernel's forms
+   (median of 5 launches each, summed over the three widths), over 64-bit
+   columns and again
    over 32-bit columns (the two basis storage widths of
    trlx_options.basis_bits); complex operators have the projection forms 3,
    4 and 5 only (the others report -1 ms).  It keeps the faster operator
@@ -79,15 +81,16 @@ typedef struct {
     int format;            /* kept operator form: 0 CSR, 1 SELL-C-32        */
     int project_form;      /* kept projection form: 1, 2, 3: 8, 12, 16
                               columns per warp; 4: 16 columns with the
-                              column-pointer table in shared memory; 5: 16
-                              columns, the basis staged through shared
-                              memory by cp.async, one block per SM        */
+                              column-pointer table in shared memory; 5: 8
+                              columns per warp, 16 warps, the basis staged
+                              through shared memory by cp.async, one
+                              block per SM                                 */
     double spmv_ms[2];     /* one product: CSR, SELL-C-32 (-1: not built)  */
-    double project_ms[5];  /* one projection in forms 1 .. 5               */
-    int columns;           /* projection width timed                        */
+    double project_ms[5];  /* projections at the three widths, forms 1 .. 5 */
+    int columns;           /* middle projection width timed                 */
     double seconds;        /* wall time of the tuning                       */
     int project_form32;    /* kept form for a 32-bit basis (same values)    */
-    double project32_ms[5];/* one projection over 32-bit columns, forms 1..5 */
+    double project32_ms[5];/* the same over 32-bit columns, forms 1..5     */
 } trlx_tune_result;
 int trlx_operator_autotune(trlx_operator *op, int maxlan, trlx_tune_result *out);
 /* Sets the projection form of later solves with this operator (a

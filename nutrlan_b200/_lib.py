@@ -49,7 +49,7 @@ class TrlxTuneResult(C.Structure):
                 ("project_ms", c_double * 5), ("columns", c_int), ("seconds", c_double),
                 ("project_form32", c_int), ("project32_ms", c_double * 5)]
 
-    FORMS = ("cpw8", "cpw12", "cpw16", "cpw16_shared_ptrs", "cpw16_staged")
+    FORMS = ("cpw8", "cpw12", "cpw16", "cpw16_shared_ptrs", "cpw8_staged")
 
     def as_dict(self):
         return {"format": ("csr", "sell")[self.format], "project_form": self.FORMS[self.project_form - 1],

@@ -6,9 +6,9 @@
 //  * one fused product y = A x, alpha = Re(x^H y) (the kernel every Lanczos
 //    step starts with) in the CSR form and in the SELL-C-32 form built from
 //    the same device arrays;
-//  * one Gram-Schmidt projection h = V^T r over `maxlan / 2` basis columns
-//    of this operator's row count (the average width of a thick-restart
-//    cycle) in each form of the projection kernel (8, 12, 16 columns per
+//  * Gram-Schmidt projections h = V^T r over maxlan / 4, maxlan / 2 and
+//    3 maxlan / 4 basis columns of this operator's row count (a thick-restart
+//    cycle's range of widths) in each form of the projection kernel (8, 12, 16 columns per
 //    warp; 16 with the pointer table in shared memory; 16 with the basis
 //    staged through shared memory by cp.async), once over FP64 columns and
 //    once over FP32 columns (the two basis storage widths);
@@ -131,7 +131,12 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
     int rc = 0;
     const long n = A->nrow;
     const long n_pad = (n + 255) / 256 * 256;
-    const int m = std::max(8, std::min(128, maxlan / 2));
+    // The projection is timed at three basis widths spread over a cycle,
+    // mp / 3, 2 mp / 3 and mp with mp = 3 maxlan / 4 (at most 128), and a
+    // form's time is their sum: the forms' efficiency depends on how the
+    // width splits into column groups, so one width would favour whichever
+    // form divides it evenly.
+    const int m = std::max(8, std::min(128, 3 * maxlan / 4));
     cudaStream_t st = nullptr;
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     // Vectors, reduction scratch and the projection's basis columns.
@@ -142,8 +147,8 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
     const size_t vec = sizeof(double) * vw * (size_t)n_pad;
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
-    // The projection is timed over m columns when they fit in a quarter of
-    // the free memory, else over as many as fit (at least 8).
+    // The widest timing uses m columns when they fit in a quarter of the
+    // free memory, else as many as fit (at least 8).
     int mp = (int)std::min<size_t>((size_t)m, free_b / 4 / std::max<size_t>(vec, 1));
     if (mp < 8 || !x.alloc(vec) || !y.alloc(vec) || !part.alloc((size_t)s.max_blocks * (m + 2) * 16) ||
         !tick.alloc(sizeof(unsigned) * trlb::kNumTickets) || !dsc.alloc(sizeof(double) * vw * (m + 4)) ||
@@ -151,6 +156,12 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
         rc = -2;
     }
     trlx_operator *other = nullptr;
+    const int widths[3] = {std::max(1, mp / 3), std::max(1, 2 * mp / 3), mp};
+    auto over_widths = [&](auto launch_at) {
+        double t = 0.0;
+        for (int w : widths) t += median_ms([&] { launch_at(w); }, st);
+        return t;
+    };
     if (!rc) {
         s.partials = part.p;
         s.tickets = static_cast<unsigned *>(tick.p);
@@ -184,13 +195,11 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
         trlb::Recur<zd> none;
         out->project_ms[0] = out->project_ms[1] = -1.0;
         for (int k = 2; k < trlb::kProjectForms; ++k) {
-            out->project_ms[k] = median_ms(
-                [&] {
-                    trlb::launch_project<zd>(static_cast<zd *const *>(table.p), mp, n_pad,
-                                             static_cast<const zd *>(x.p), none, static_cast<zd *>(dsc.p),
-                                             static_cast<double *>(dsc.p) + 2 * (m + 1), s, st, trlb::kProject8 + k);
-                },
-                st);
+            out->project_ms[k] = over_widths([&](int w) {
+                trlb::launch_project<zd>(static_cast<zd *const *>(table.p), w, n_pad, static_cast<const zd *>(x.p),
+                                         none, static_cast<zd *>(dsc.p), static_cast<double *>(dsc.p) + 2 * (m + 1),
+                                         s, st, trlb::kProject8 + k);
+            });
         }
         const int best = trlb::kProject8 + fastest(out->project_ms, trlb::kProject16 - trlb::kProject8);
         A->project_form = best;
@@ -200,18 +209,16 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
         fill_columns<float>(basis.p, table.p, mp, n, n_pad, vw, st);
         out->project32_ms[0] = out->project32_ms[1] = -1.0;
         for (int k = 2; k < trlb::kProjectForms; ++k) {
-            out->project32_ms[k] = median_ms(
-                [&] {
-                    trlb::launch_project<zf>(static_cast<zf *const *>(table.p), mp, n_pad,
-                                             static_cast<const zd *>(x.p), none, static_cast<zd *>(dsc.p),
-                                             static_cast<double *>(dsc.p) + 2 * (m + 1), s, st, trlb::kProject8 + k);
-                },
-                st);
+            out->project32_ms[k] = over_widths([&](int w) {
+                trlb::launch_project<zf>(static_cast<zf *const *>(table.p), w, n_pad, static_cast<const zd *>(x.p),
+                                         none, static_cast<zd *>(dsc.p), static_cast<double *>(dsc.p) + 2 * (m + 1),
+                                         s, st, trlb::kProject8 + k);
+            });
         }
         const int best32 = trlb::kProject8 + fastest(out->project32_ms, trlb::kProject16 - trlb::kProject8);
         A->project_form32 = best32;
         out->project_form32 = best32;
-        out->columns = mp;
+        out->columns = widths[1];
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = -3;
     } else if (!rc) {
         // ---- operator form ----------------------------------------------
@@ -246,14 +253,11 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
         // ---- projection kernel form -------------------------------------
         trlb::Recur<double> none;
         for (int k = 0; k < trlb::kProjectForms; ++k) {
-            out->project_ms[k] = median_ms(
-                [&] {
-                    trlb::launch_project<double>(static_cast<double *const *>(table.p), mp, n_pad,
-                                                 static_cast<const double *>(x.p), none,
-                                                 static_cast<double *>(dsc.p), static_cast<double *>(dsc.p) + m + 1,
-                                                 s, st, trlb::kProject8 + k);
-                },
-                st);
+            out->project_ms[k] = over_widths([&](int w) {
+                trlb::launch_project<double>(static_cast<double *const *>(table.p), w, n_pad,
+                                             static_cast<const double *>(x.p), none, static_cast<double *>(dsc.p),
+                                             static_cast<double *>(dsc.p) + m + 1, s, st, trlb::kProject8 + k);
+            });
         }
         const int best = fastest(out->project_ms, trlb::kProject16 - trlb::kProject8);
         A->project_form = trlb::kProject8 + best;
@@ -261,19 +265,16 @@ extern "C" int trlx_operator_autotune(trlx_operator *A, int maxlan, trlx_tune_re
         // The same forms over FP32 columns (the first half of the buffer).
         fill_columns<float>(basis.p, table.p, mp, n, n_pad, vw, st);
         for (int k = 0; k < trlb::kProjectForms; ++k) {
-            out->project32_ms[k] = median_ms(
-                [&] {
-                    trlb::launch_project<float>(static_cast<float *const *>(table.p), mp, n_pad,
-                                                static_cast<const double *>(x.p), none,
-                                                static_cast<double *>(dsc.p), static_cast<double *>(dsc.p) + m + 1,
-                                                s, st, trlb::kProject8 + k);
-                },
-                st);
+            out->project32_ms[k] = over_widths([&](int w) {
+                trlb::launch_project<float>(static_cast<float *const *>(table.p), w, n_pad,
+                                            static_cast<const double *>(x.p), none, static_cast<double *>(dsc.p),
+                                            static_cast<double *>(dsc.p) + m + 1, s, st, trlb::kProject8 + k);
+            });
         }
         const int best32 = fastest(out->project32_ms, trlb::kProject16 - trlb::kProject8);
         A->project_form32 = trlb::kProject8 + best32;
         out->project_form32 = trlb::kProject8 + best32;
-        out->columns = mp;
+        out->columns = widths[1];
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = -3;
     }
     if (other) trlx_operator_destroy(other);

@@ -235,17 +235,23 @@ __global__ void __launch_bounds__(kThreads, (PS ? proj_ps_blocks<T>() : proj_min
 // flight in registers, next to an FP64 accumulator and a pointer per
 // column, and the register file caps the bytes in flight per SM: FP32 and
 // complex storage stop at 80-90% of the HBM peak.  Here each lane copies its
-// own 16 bytes of each of its warp's 16 columns into a ring of NS stages in
-// shared memory (192 KB, one block per SM), so NS - 1 stages (128 KB per SM)
-// are in flight while the warp consumes the oldest.  A lane reads back only
+// own 16 bytes of each of its warp's CPW columns into a ring of NS stages in
+// shared memory (NW = 16 warps x 8 columns x 3 stages = 192 KB, one block of
+// 512 threads per SM), so NS - 1 stages (128 KB per SM) are in flight while
+// the warp consumes the oldest.  A lane reads back only
 // the bytes it copied itself, so the ring needs no barrier: the thread's own
 // cp.async.wait_group orders them.  r, x and x' (shared by the block's warps
 // and mostly served by L1/L2) are plain loads issued one iteration ahead.
 // Column groups, row split and the order of every sum are those of
 // k_project.
-constexpr int kAsyncCols = 16;
-constexpr int kAsyncStages = 3;
-constexpr size_t kAsyncSmem = (size_t)(kThreads / 32) * kAsyncStages * kAsyncCols * 32 * 16;
+// 16 warps of 8 columns and three stages measured best among 8 x 16,
+// 16 x 8, 16 x 6 (four stages) and 32 x 4 (spills for complex storage) on
+// FP64, FP32, complex128 and complex64 columns at 16-128 columns.
+constexpr int kAsyncWarps = 16, kAsyncCols = 8, kAsyncStages = 3;
+template <int NW, int CPW, int NS>
+constexpr size_t async_smem() {
+    return (size_t)NW * NS * CPW * 32 * 16;
+}
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -257,8 +263,8 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-template <class T>
-__global__ void __launch_bounds__(kThreads, 1)
+template <class T, int NW, int CPW, int NS>
+__global__ void __launch_bounds__(NW * 32, 1)
     k_project_async(T *const *__restrict__ cols, int m, long n_pad, long chunk,
                     const typename Store<T>::C *__restrict__ r, Recur<typename Store<T>::C> rec,
                     typename Store<T>::C *part, double *part_r2, unsigned *ticket,
@@ -266,8 +272,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     using S = Store<T>;
     using C = typename S::C;
     constexpr int R = S::R;
-    constexpr int W = kThreads / 32;
-    constexpr int CPW = kAsyncCols, NS = kAsyncStages;
+    constexpr int W = NW, NT = NW * 32;
     static_assert(sizeof(T) * R == 16, "one 16-byte copy per lane and column");
     extern __shared__ __align__(16) unsigned char ring_raw[];
     __shared__ C red_c[W][CPW];
@@ -369,7 +374,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         __syncthreads();
     }
     if (m == 0) {
-        for (long i = row0 + (long)threadIdx.x * R; i < row1; i += (long)kThreads * R) {
+        for (long i = row0 + (long)threadIdx.x * R; i < row1; i += (long)NT * R) {
             C rv[R];
             load_c<R>(r + i, rv);
             if (rec.on) {
@@ -393,7 +398,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         part_r2[blockIdx.x] = sacc;
     }
     if (last_block_arrived(ticket)) {
-        __shared__ C red_cols[kThreads];
+        __shared__ C red_cols[NT];
         __shared__ double red_r2x[32];
         const int nb = gridDim.x;
         const double h2 = reduce_columns(part, nb, m, h, red_cols);
@@ -778,15 +783,17 @@ void launch_project(T *const *cols, int m, long n_pad, const typename Store<T>::
                                       out2);
     };
     if (staged) {
-        static const bool smem_ok = cudaFuncSetAttribute(k_project_async<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                         (int)kAsyncSmem) == cudaSuccess;
-        if (!smem_ok) {
-            std::fprintf(stderr, "trlan_b200: the staged projection cannot reserve %zu bytes of shared memory\n",
-                         kAsyncSmem);
-            return;
-        }
-        k_project_async<T><<<nb, kThreads, kAsyncSmem, st>>>(cols, m, n_pad, chunk, r, rec, part, part_r2,
-                                                            s.tickets + kTicketProject, h, out2);
+        auto staged_launch = [&](auto kern, int nw, size_t smem) {
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+                std::fprintf(stderr, "trlan_b200: the staged projection cannot reserve %zu bytes of shared memory\n",
+                             smem);
+                return;
+            }
+            kern<<<nb, nw * 32, smem, st>>>(cols, m, n_pad, chunk, r, rec, part, part_r2,
+                                            s.tickets + kTicketProject, h, out2);
+        };
+        staged_launch(k_project_async<T, kAsyncWarps, kAsyncCols, kAsyncStages>, kAsyncWarps,
+                      async_smem<kAsyncWarps, kAsyncCols, kAsyncStages>());
         return;
     }
     if constexpr (std::is_same<C, double>::value) {

@@ -46,7 +46,7 @@ void launch_dot(const C *x, const C *y, long n_pad, double *out, Scratch &s,
 // 16 columns per warp, or 16 with the column-pointer table in shared memory;
 // for complex storage 8 columns per warp with the table in registers
 // (kProject8 .. kProject16) or in shared memory (kProject16Shared); for
-// every storage type, 16 columns per warp with the basis staged through a
+// every storage type, 16 warps of 8 columns with the basis staged through a
 // shared-memory ring by cp.async, one block per SM (kProjectAsync).
 enum ProjectForm {
     kProjectDefault = 0,
