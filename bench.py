@@ -64,6 +64,7 @@ WORKLOADS = {
     "anderson128": dict(kind="anderson", L=128, W=4.0, ned=32, maxlan=128, tol=1e-8),
     "laplace128": dict(kind="laplace", L=128, ned=10, maxlan=64, tol=1.4901e-8),
     "peierls2048": dict(kind="peierls", L=2048, phi=1.0 / 64.0, W=2.0, ned=16, maxlan=96, tol=1e-8),
+    "peierls1024": dict(kind="peierls", L=1024, phi=1.0 / 64.0, W=2.0, ned=16, maxlan=96, tol=1e-8),
     "wells256": dict(kind="wells", L=256, ned=16, maxlan=48, tol=1e-8, problems=16),
 }
 
@@ -74,6 +75,19 @@ def _form_index(tune, key):
         return 0
     from nutrlan_b200._lib import TrlxTuneResult
     return 1 + TrlxTuneResult.FORMS.index(tune[key])
+
+
+def _forced_forms(args, lib, op, forms, config):
+    """--project-form: set one projection form for both basis widths on the
+    operator (profiling and A/B runs); returns the (64-bit, 32-bit) forms."""
+    from nutrlan_b200._lib import TrlxTuneResult
+    if args.project_form == "auto":
+        return forms
+    f = 1 + TrlxTuneResult.FORMS.index(args.project_form)
+    lib.trlx_operator_set_project_form(op.handle, f)
+    lib.trlx_operator_set_project_form32(op.handle, f)
+    config["project_form_forced"] = args.project_form
+    return f, f
 
 
 def build_operator(w, seed):
@@ -341,10 +355,11 @@ def run_complex(args, w, world, rank, local, pg):
     config = {"workload": f"peierls{L}: n={L * L}, flux 1/{int(round(1 / w['phi']))}, disorder "
                           f"U[-{w['W'] / 2:g},{w['W'] / 2:g}], ned={ned}, maxlan={maxlan}, tol={tol}, "
                           f"complex {{fmt}}, basis c128, one thick-restart cycle/step",
-              "global_batch": world, "parallelism": f"replicas x{world}",
-              "l2": "inputs larger than L2 (basis >= 6 GB, CSR 420 MB)"}
+              "global_batch": world, "parallelism": f"replicas x{world}"}
     A = ops.peierls_2d(L, phi=w["phi"], W=w["W"], seed=seed)
     n = A.n
+    config["l2"] = (f"inputs larger than L2 (basis {maxlan * n * 16 / 1e9:.1f} GB, "
+                    f"CSR {(A.nnz * 20 + 8 * n) / 1e6:.0f} MB)")
     x0 = ops.start_vector(n) + 1j * ops.start_vector(n, seed=99)
     cpu_sample = args.cpu_sample
 
@@ -389,8 +404,8 @@ def run_complex(args, w, world, rank, local, pg):
     lib = load()
     mev = ned + 1
     op = DeviceOperator(A, fmt="auto", maxlan=maxlan)        # tunes the format and projection forms
-    tuned_form = _form_index(op.tune, "project_form")
-    tuned_form32 = _form_index(op.tune, "project_form32")
+    tuned_form, tuned_form32 = _forced_forms(
+        args, lib, op, (_form_index(op.tune, "project_form"), _form_index(op.tune, "project_form32")), config)
     config["workload"] = config["workload"].replace("{fmt}", "SELL-C-32" if op.fmt == "zsell" else "CSR")
     config["autotune"] = op.tune
     evec = torch.zeros((mev, n), dtype=torch.complex128, device=dev)
@@ -802,6 +817,9 @@ def main():
     ap.add_argument("--format", choices=["auto", "csr", "sell"], default="auto",
                     help="operator format; auto: trlx_operator_autotune picks CSR or SELL-C-32 "
                          "and the projection width by measurement")
+    ap.add_argument("--project-form", default="auto",
+                    choices=["auto", "cpw8", "cpw12", "cpw16", "cpw16_shared_ptrs", "cpw8_staged"],
+                    help="projection kernel form for both basis widths (auto: the autotuner's choice)")
     ap.add_argument("--cpu-sample", type=int, default=32,
                     help="Lanczos steps in the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -917,8 +935,8 @@ def main():
     # ---- device-resident arm -------------------------------------------------
     op = DeviceOperator(A, fmt=args.format, maxlan=maxlan)
     fmt_used = op.fmt
-    tuned_form = _form_index(op.tune, "project_form")
-    tuned_form32 = _form_index(op.tune, "project_form32")
+    tuned_form, tuned_form32 = _forced_forms(
+        args, lib, op, (_form_index(op.tune, "project_form"), _form_index(op.tune, "project_form32")), config)
     config["workload"] = config["workload"].replace("{fmt}", fmt_used.upper())
     if op.tune is not None:
         config["format_choice"] = "autotuned (trlx_operator_autotune)"
@@ -1047,7 +1065,12 @@ def main():
     variants = {}
     if not args.no_variants:
         def time_variant(fmt, bits):
-            vop = op if fmt == fmt_used else DeviceOperator(A, fmt=fmt)
+            vop = op
+            if fmt != fmt_used:
+                # The other format with the same projection forms.
+                vop = DeviceOperator(A, fmt=fmt)
+                lib.trlx_operator_set_project_form(vop.handle, tuned_form)
+                lib.trlx_operator_set_project_form32(vop.handle, tuned_form32)
             vopts = TrlxOptions()
             lib.trlx_default_options(C.byref(vopts))
             vopts.basis_bits = bits
