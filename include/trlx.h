@@ -281,6 +281,10 @@ typedef struct {
     int bucket_format[3];
     double tune_seconds;
     int cta_threads;         /* threads per CTA of the launch              */
+    int graph_replays;       /* the solve's launch sequence (queue reset +
+                                persistent kernel) is a CUDA graph captured
+                                once per launch configuration: how many
+                                solves have replayed it, this one included */
 } trlx_batch_config;
 
 void trlx_batch_default_options(trlx_batch_options *o);

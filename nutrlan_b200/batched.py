@@ -21,7 +21,7 @@ class BatchOptions(C.Structure):
 
 class BatchConfig(C.Structure):
     _fields_ = [("bucket_threads", C.c_int * 3), ("bucket_format", C.c_int * 3),
-                ("tune_seconds", C.c_double), ("cta_threads", C.c_int)]
+                ("tune_seconds", C.c_double), ("cta_threads", C.c_int), ("graph_replays", C.c_int)]
 
 
 def _declare(lib):

@@ -42,6 +42,14 @@ struct trlx_batch {
     int bucket_format[3] = {0, 0, 0};
     int cta = 1024;
     double tune_seconds = 0.0;
+    // The solve's launch sequence (queue reset + the persistent kernel),
+    // captured once as a CUDA graph per distinct launch configuration and
+    // replayed on the batch's own stream.
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    Params graph_params{};
+    int graph_blocks = 0;
+    int graph_launches = 0;  // replays of the current graph
 };
 
 namespace {
@@ -103,7 +111,8 @@ int prepare(trlx_batch *b, int ned, int maxlan) {
 }
 
 Params base_params(trlx_batch *b, const trlx_batch_options *o) {
-    Params P{};
+    Params P;
+    std::memset(&P, 0, sizeof P);  // padding too: launch configurations are compared bytewise
     P.nprob = b->nprob;
     P.ned = o->ned;
     P.maxlan = o->maxlan;
@@ -168,15 +177,43 @@ int build_csr(trlx_batch *b, const std::vector<double> &hdiag) {
     return rc;
 }
 
-// One persistent launch: SMs x resident CTAs of P.cta threads.
+// One persistent launch: SMs x resident CTAs of P.cta threads.  The queue
+// reset and the launch are one CUDA graph, captured the first time a launch
+// configuration is seen and replayed while it stays the same.
 int run(trlx_batch *b, Params P, int nsm) {
-    if (cudaMemset(b->d_queue, 0, sizeof(unsigned) * 4) != cudaSuccess) return -1001;
     int min_threads = P.cta;
     for (int f = 0; f < P.nphases; ++f) min_threads = std::min(min_threads, P.phase_threads[f]);
+    // Sets the kernel's shared-memory attribute before any capture.
     const int blocks = nsm * trlb::batched::max_blocks_per_sm(min_threads, P.maxlan, P.cta);
-    int rc = trlb::batched::launch(P, blocks, 0);
-    if (rc) return rc;
-    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1001;
+    if (!b->stream && cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return -1001;
+    const bool same = b->graph && b->graph_blocks == blocks && std::memcmp(&b->graph_params, &P, sizeof P) == 0;
+    if (!same) {
+        if (b->graph) cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) return -1001;
+        cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned) * 4, b->stream);
+        const int rc = trlb::batched::launch(P, blocks, b->stream);
+        const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+        if (rc || ce != cudaSuccess || !g) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return rc ? rc : -1001;
+        }
+        const cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+            b->graph = nullptr;
+            cudaGetLastError();
+            return -1001;
+        }
+        b->graph_params = P;
+        b->graph_blocks = blocks;
+        b->graph_launches = 0;
+    }
+    if (cudaGraphLaunch(b->graph, b->stream) != cudaSuccess) return -1001;
+    b->graph_launches++;
+    return cudaStreamSynchronize(b->stream) == cudaSuccess ? 0 : -1001;
 }
 
 }  // namespace
@@ -414,6 +451,7 @@ int trlx_batch_solve(trlx_batch *b, const trlx_batch_options *o, double *eval, d
         }
         used->tune_seconds = b->tune_seconds;
         used->cta_threads = cta;
+        used->graph_replays = b->graph_launches;
     }
     return 0;
 }
@@ -447,6 +485,8 @@ void trlx_batch_destroy(trlx_batch *b) {
     cudaFree(b->d_res);
     cudaFree(b->d_info);
     cudaFree(b->d_queue);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
 

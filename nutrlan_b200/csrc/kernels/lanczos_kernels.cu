@@ -771,7 +771,19 @@ void launch_project(T *const *cols, int m, long n_pad, const typename Store<T>::
     using C = typename Store<T>::C;
     constexpr int R = Store<T>::R;
     // The staged form runs one block per SM (its ring fills shared memory).
-    const bool staged = form_req == kProjectAsync;
+    // The staged form needs 192 KB of dynamic shared memory per block; a
+    // device that does not grant it runs the default register form.
+    const auto staged_kern = k_project_async<T, kAsyncWarps, kAsyncCols, kAsyncStages>;
+    constexpr size_t staged_smem = async_smem<kAsyncWarps, kAsyncCols, kAsyncStages>();
+    bool staged = false;
+    if (form_req == kProjectAsync) {
+        staged = cudaFuncSetAttribute(staged_kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)staged_smem) ==
+                 cudaSuccess;
+        if (!staged) {
+            cudaGetLastError();
+            form_req = kProjectDefault;
+        }
+    }
     int nb = std::min(staged ? num_sms() : stream_blocks(n_pad, R), s.max_blocks);
     long per = (n_pad + nb - 1) / nb;
     long chunk = (per + 32 * R - 1) / (32 * R) * (32 * R);
@@ -783,17 +795,8 @@ void launch_project(T *const *cols, int m, long n_pad, const typename Store<T>::
                                       out2);
     };
     if (staged) {
-        auto staged_launch = [&](auto kern, int nw, size_t smem) {
-            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
-                std::fprintf(stderr, "trlan_b200: the staged projection cannot reserve %zu bytes of shared memory\n",
-                             smem);
-                return;
-            }
-            kern<<<nb, nw * 32, smem, st>>>(cols, m, n_pad, chunk, r, rec, part, part_r2,
-                                            s.tickets + kTicketProject, h, out2);
-        };
-        staged_launch(k_project_async<T, kAsyncWarps, kAsyncCols, kAsyncStages>, kAsyncWarps,
-                      async_smem<kAsyncWarps, kAsyncCols, kAsyncStages>());
+        staged_kern<<<nb, kAsyncWarps * 32, staged_smem, st>>>(cols, m, n_pad, chunk, r, rec, part, part_r2,
+                                                              s.tickets + kTicketProject, h, out2);
         return;
     }
     if constexpr (std::is_same<C, double>::value) {

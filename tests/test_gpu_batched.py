@@ -120,3 +120,19 @@ def test_batched_cta_sizes_agree():
         assert np.all(r2.info[:, 1] >= 8)
     finally:
         b.close()
+
+
+def test_batched_solve_replays_its_captured_graph(small):
+    """A solve's launch sequence is a CUDA graph captured once per launch
+    configuration: the same configuration again replays it (with the same
+    results), a different one captures a new graph."""
+    Ls, b, diags = small
+    kw = dict(ned=6, maxlan=24, tol=1e-8, seed=SEED, threads=512, fmt=0, cta=1024)
+    r1 = b.solve(**kw)
+    r2 = b.solve(**kw)
+    assert r2.config.graph_replays == r1.config.graph_replays + 1 >= 2
+    np.testing.assert_array_equal(r1.eval, r2.eval)
+    np.testing.assert_array_equal(r1.info, r2.info)
+    r3 = b.solve(**dict(kw, threads=256))
+    assert r3.config.graph_replays == 1
+    np.testing.assert_allclose(r3.eval, r1.eval, rtol=1e-10)
