@@ -145,8 +145,12 @@ __device__ __forceinline__ zd mac(zd acc, zd a, zd x) {
 __device__ __forceinline__ double alpha_add(double aacc, double x, double y) { return fma(x, y, aacc); }
 __device__ __forceinline__ double alpha_add(double aacc, zd x, zd y) { return fma(x.x, y.x, fma(x.y, y.y, aacc)); }
 
+// Eight blocks per SM (32 registers): the product is latency-bound, and the
+// full 64 warps beat the complex form's unconstrained 40 registers (6 blocks;
+// a few bytes of spills outside the entry loop): 0.132 -> 0.104 ms per
+// product on Peierls 2048^2, 0.314 -> 0.299 ms for the real form at 256^3.
 template <class V>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 8)
     k_sell(int nrow, long n_pad, int nslice, const long long *__restrict__ sp,
            const int *__restrict__ ci, const V *__restrict__ va, const int *__restrict__ perm,
            const V *__restrict__ x, V *__restrict__ y, double *part, unsigned *ticket,
