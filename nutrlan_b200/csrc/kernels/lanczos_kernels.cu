@@ -563,12 +563,26 @@ __global__ void __launch_bounds__(kThreads)
     k_normalize(typename Store<T>::C *r, long n_pad, const double *r2, double fixed,
                 typename Store<T>::C *q, T *vcol) {
     using S = Store<T>;
+    using C = typename S::C;
+    // Four elements per thread per round, their loads issued together
+    // (coalesced: element u of a round is `stride` after element u - 1).
+    constexpr int U = 4;
     const double sc = r2 ? 1.0 / sqrt(*r2) : fixed;
     const long stride = (long)gridDim.x * blockDim.x;
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += stride) {
-        auto v = r[i] * sc;
-        q[i] = v;
-        if (vcol) vcol[i] = S::from_c(v);
+    for (long i0 = (long)blockIdx.x * blockDim.x + threadIdx.x; i0 < n_pad; i0 += U * stride) {
+        C v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (i0 + u * stride < n_pad) v[u] = r[i0 + u * stride];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long i = i0 + u * stride;
+            if (i < n_pad) {
+                const C w = v[u] * sc;
+                q[i] = w;
+                if (vcol) vcol[i] = S::from_c(w);
+            }
+        }
     }
 }
 
