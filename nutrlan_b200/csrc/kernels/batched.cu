@@ -98,17 +98,39 @@ __device__ inline double apply_op(const Params &P, const Problem &pr, const doub
     double a = 0.0;
     const int n = pr.n;
     if (P.format == kFormatStencil5) {
+        // Two rows per thread per round with all their loads issued first
+        // (neighbour indices clamped into the grid, the boundary terms
+        // dropped afterwards), so twice the loads are in flight; each row's
+        // arithmetic and the order of the alpha sum are unchanged.
+        constexpr int U = 2;
         const int L = pr.L;
         const double *d = P.diag + pr.diag_off;
-        for (int i = G.tid; i < n; i += G.nt) {
-            const int ix = i % L, iy = i / L;
-            double s = (4.0 + d[i]) * x[i];
-            if (ix > 0) s -= x[i - 1];
-            if (ix < L - 1) s -= x[i + 1];
-            if (iy > 0) s -= x[i - L];
-            if (iy < L - 1) s -= x[i + L];
-            y[i] = s;
-            a += x[i] * s;
+        for (int i0 = G.tid; i0 < n; i0 += U * G.nt) {
+            double xc[U], xl[U], xr[U], xd[U], xu[U], dd[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int i = min(i0 + u * G.nt, n - 1);
+                xc[u] = x[i];
+                dd[u] = d[i];
+                xl[u] = x[max(i - 1, 0)];
+                xr[u] = x[min(i + 1, n - 1)];
+                xd[u] = x[max(i - L, 0)];
+                xu[u] = x[min(i + L, n - 1)];
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int i = i0 + u * G.nt;
+                if (i < n) {
+                    const int ix = i % L, iy = i / L;
+                    double s = (4.0 + dd[u]) * xc[u];
+                    if (ix > 0) s -= xl[u];
+                    if (ix < L - 1) s -= xr[u];
+                    if (iy > 0) s -= xd[u];
+                    if (iy < L - 1) s -= xu[u];
+                    y[i] = s;
+                    a += xc[u] * s;
+                }
+            }
         }
     } else {
         const long long *rp = P.row_ptr + pr.rp_off;
@@ -152,11 +174,17 @@ __device__ inline Norms project(const double *V, int ld, int n, int m, double *y
         // r = y - alpha x - beta xp written back into y first, so that the
         // column passes hold no recurrence operands (registers) and the
         // update reads one vector.
-        for (int p = G.tid; p < np; p += G.nt) {
-            const int i = 2 * p;
-            const double2 yv = ld2(y + i), xv = ld2(x + i), pv = ld2(xp + i);
-            *reinterpret_cast<double2 *>(y + i) =
-                make_double2(yv.x - (alpha * xv.x + beta * pv.x), yv.y - (alpha * xv.y + beta * pv.y));
+        // Two row pairs per thread per round, loads first.
+        for (int p0 = G.tid; p0 < np; p0 += 2 * G.nt) {
+            const int p1 = p0 + G.nt;
+            const int i0 = 2 * p0, i1 = 2 * min(p1, np - 1);
+            const double2 y0 = ld2(y + i0), x0 = ld2(x + i0), q0 = ld2(xp + i0);
+            const double2 y1 = ld2(y + i1), x1 = ld2(x + i1), q1 = ld2(xp + i1);
+            *reinterpret_cast<double2 *>(y + i0) =
+                make_double2(y0.x - (alpha * x0.x + beta * q0.x), y0.y - (alpha * x0.y + beta * q0.y));
+            if (p1 < np)
+                *reinterpret_cast<double2 *>(y + i1) =
+                    make_double2(y1.x - (alpha * x1.x + beta * q1.x), y1.y - (alpha * x1.y + beta * q1.y));
         }
         if ((n & 1) && G.tid == 0) y[n - 1] -= alpha * x[n - 1] + beta * xp[n - 1];
         G.sync();
@@ -287,7 +315,16 @@ __device__ inline double update(const double *V, int ld, int n, int m, double *y
 }
 
 __device__ inline void scale(double *y, int n, double sc, const Grp &G) {
-    for (int i = G.tid; i < n; i += G.nt) y[i] *= sc;
+    // Four elements per thread per round, loads first.
+    constexpr int U = 4;
+    for (int i0 = G.tid; i0 < n; i0 += U * G.nt) {
+        double v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) v[u] = y[min(i0 + u * G.nt, n - 1)];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (i0 + u * G.nt < n) y[i0 + u * G.nt] = v[u] * sc;
+    }
     G.sync();
 }
 
