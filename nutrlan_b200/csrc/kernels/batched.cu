@@ -294,10 +294,16 @@ __device__ inline double update(const double *V, int ld, int n, int m, double *y
                 r1 = fma(-v[k].y, h[c + k], r1);
             }
         }
-        for (; c < m; ++c) {
-            const double2 v = ld2(V + (size_t)c * ld + i);
-            r0 = fma(-v.x, h[c], r0);
-            r1 = fma(-v.y, h[c], r1);
+        if (c < m) {  // the last partial chunk, its loads issued together
+            double2 v[UC];
+#pragma unroll
+            for (int k = 0; k < UC; ++k) v[k] = c + k < m ? ld2(V + (size_t)(c + k) * ld + i) : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int k = 0; k < UC; ++k)
+                if (c + k < m) {
+                    r0 = fma(-v[k].x, h[c + k], r0);
+                    r1 = fma(-v[k].y, h[c + k], r1);
+                }
         }
         *reinterpret_cast<double2 *>(y + i) = make_double2(r0, r1);
         r2 += r0 * r0;
