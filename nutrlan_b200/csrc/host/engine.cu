@@ -1062,7 +1062,8 @@ int Engine<T>::final_vectors(int jnd, int kept) {
 // ---- speculative regular steps ---------------------------------------------
 // For short vectors the host round trip of every Lanczos step (read alpha
 // and the norms, take trl_orth's decisions, launch the next step) costs more
-// than the step's kernels.  With a built-in operator and an FP64/c128 basis
+// than the step's kernels, and for long ones it is still 1-2% of a step.
+// With a built-in operator and an FP64/c128 basis
 // the engine issues a run of steps without waiting, each assuming the
 // outcome trl_orth takes in almost every step: the full classical
 // Gram-Schmidt path with one pass (its stop test passes) and a beta that is
@@ -1079,7 +1080,7 @@ bool Engine<T>::spec_enabled() const {
     if constexpr (!kWide) {
         return false;
     } else {
-        if (!builtin_ || uo_ || comm_ || builtin_->halo || n_pad_ > (1L << 21)) return false;
+        if (!builtin_ || uo_ || comm_ || builtin_->halo) return false;
         const char *e = std::getenv("TRLX_SPECULATE");
         return !(e && e[0] == '0');
     }
