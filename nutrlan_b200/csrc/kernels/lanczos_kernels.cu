@@ -85,6 +85,87 @@ constexpr int proj_min_blocks() {
                : (Store<T>::R == 4 ? (CPW >= 12 ? 2 : 3) : (CPW >= 16 ? 2 : (CPW >= 12 ? 3 : 4)));
 }
 
+// Shared by the projection kernels (register and staged forms).
+// End of one sweep: each warp's CPW column sums are reduced over its lanes,
+// then each column over the warps of its group in warp order, into the
+// block's partials.
+template <class C, int CPW>
+__device__ __forceinline__ void project_sweep_end(C (&acc)[CPW], C (*red_c)[CPW], int c0, int G, int per, int wpg,
+                                                  int m, C *part) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < CPW; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[k] = acc[k] + shfl_down(acc[k], o);
+        if (lane == 0) red_c[warp][k] = acc[k];
+    }
+    __syncthreads();
+    if (threadIdx.x < G * CPW) {
+        const int gg = threadIdx.x / CPW, k = threadIdx.x - gg * CPW;
+        const int c = c0 + gg * per + k;
+        if (k < per && c < m) {
+            C s = czero(C());
+            for (int sl = 0; sl < wpg; ++sl) s = s + red_c[gg * wpg + sl][k];
+            part[(long)blockIdx.x * m + c] = s;
+        }
+    }
+    __syncthreads();
+}
+
+// With no columns (m == 0) the pass still returns ||r||^2 of the block's
+// rows; the NT threads split the rows.
+template <int R, int NT, class C>
+__device__ __forceinline__ double project_norm_only(const C *r, Recur<C> rec, double alpha, double beta, long row0,
+                                                    long row1) {
+    double r2acc = 0.0;
+    for (long i = row0 + (long)threadIdx.x * R; i < row1; i += (long)NT * R) {
+        C rv[R];
+        load_c<R>(r + i, rv);
+        if (rec.on) {
+            C xv[R], xpv[R];
+            load_c<R>(rec.x + i, xv);
+            load_c<R>(rec.xp + i, xpv);
+#pragma unroll
+            for (int q = 0; q < R; ++q) rv[q] = rv[q] - alpha * xv[q] - beta * xpv[q];
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) r2acc += abs2(rv[q]);
+    }
+    return r2acc;
+}
+
+// The block's ||r||^2 partial (warps in order), then, in the last block to
+// finish, the grid totals: h (column sums in block order), ||h||^2 and
+// ||r||^2.  NT is the block size.
+template <class C, int NT>
+__device__ __forceinline__ void project_finish(double r2acc, C *part, double *part_r2, unsigned *ticket, C *h,
+                                               double *out2, int m) {
+    constexpr int W = NT / 32;
+    __shared__ double red_r2[W];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r2acc += __shfl_down_sync(0xffffffffu, r2acc, o);
+    if (lane == 0) red_r2[warp] = r2acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < W; ++w) s += red_r2[w];
+        part_r2[blockIdx.x] = s;
+    }
+    if (last_block_arrived(ticket)) {
+        __shared__ C red_cols[NT];
+        __shared__ double red_r2x[32];
+        const int nb = gridDim.x;
+        const double h2 = reduce_columns(part, nb, m, h, red_cols);
+        const double r2 = sum_partials(part_r2, nb, red_r2x);
+        if (threadIdx.x == 0) {
+            out2[0] = r2;
+            out2[1] = h2;
+            *ticket = 0;
+        }
+    }
+}
+
 // PS: the warp's column pointers live in shared memory and are re-read at
 // every use instead of being held in 2 * CPW registers.  For 64-bit and
 // complex storage the freed registers buy a third resident block; for FP32
@@ -107,7 +188,6 @@ __global__ void __launch_bounds__(kThreads, (PS ? proj_ps_blocks<T>() : proj_min
     constexpr int R = S::R;
     constexpr int W = kThreads / 32;
     __shared__ C red_c[W][CPW];
-    __shared__ double red_r2[W];
     __shared__ const T *sp[PS ? W : 1][PS ? CPW : 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long row0 = (long)blockIdx.x * chunk;
@@ -172,61 +252,10 @@ __global__ void __launch_bounds__(kThreads, (PS ? proj_ps_blocks<T>() : proj_min
                 }
             }
         }
-#pragma unroll
-        for (int k = 0; k < CPW; ++k) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc[k] = acc[k] + shfl_down(acc[k], o);
-            if (lane == 0) red_c[warp][k] = acc[k];
-        }
-        __syncthreads();
-        if (threadIdx.x < G * CPW) {
-            const int gg = threadIdx.x / CPW, k = threadIdx.x - gg * CPW;
-            const int c = c0 + gg * per + k;
-            if (k < per && c < m) {
-                C s = czero(C());
-                for (int sl = 0; sl < wpg; ++sl) s = s + red_c[gg * wpg + sl][k];
-                part[(long)blockIdx.x * m + c] = s;
-            }
-        }
-        __syncthreads();
+        project_sweep_end<C, CPW>(acc, red_c, c0, G, per, wpg, m, part);
     }
-    if (m == 0) {
-        // No columns: the pass still returns ||r||^2 (warps split the rows).
-        for (long i = row0 + (long)threadIdx.x * R; i < row1; i += (long)kThreads * R) {
-            C rv[R];
-            load_c<R>(r + i, rv);
-            if (rec.on) {
-                C xv[R], xpv[R];
-                load_c<R>(rec.x + i, xv);
-                load_c<R>(rec.xp + i, xpv);
-#pragma unroll
-                for (int q = 0; q < R; ++q) rv[q] = rv[q] - alpha * xv[q] - beta * xpv[q];
-            }
-#pragma unroll
-            for (int q = 0; q < R; ++q) r2acc += abs2(rv[q]);
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) r2acc += __shfl_down_sync(0xffffffffu, r2acc, o);
-    if (lane == 0) red_r2[warp] = r2acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int w = 0; w < W; ++w) s += red_r2[w];
-        part_r2[blockIdx.x] = s;
-    }
-    if (last_block_arrived(ticket)) {
-        __shared__ C red_cols[kThreads];
-        __shared__ double red_r2x[32];
-        const int nb = gridDim.x;
-        const double h2 = reduce_columns(part, nb, m, h, red_cols);
-        const double r2 = sum_partials(part_r2, nb, red_r2x);
-        if (threadIdx.x == 0) {
-            out2[0] = r2;
-            out2[1] = h2;
-            *ticket = 0;
-        }
-    }
+    if (m == 0) r2acc = project_norm_only<R, kThreads>(r, rec, alpha, beta, row0, row1);
+    project_finish<C, kThreads>(r2acc, part, part_r2, ticket, h, out2, m);
 }
 
 // ---------------------------------------------------------------------------
@@ -276,7 +305,6 @@ __global__ void __launch_bounds__(NW * 32, 1)
     static_assert(sizeof(T) * R == 16, "one 16-byte copy per lane and column");
     extern __shared__ __align__(16) unsigned char ring_raw[];
     __shared__ C red_c[W][CPW];
-    __shared__ double red_r2[W];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // This lane's 16 bytes of column k in stage q.
     T *const ring = reinterpret_cast<T *>(ring_raw) + (size_t)warp * NS * CPW * 32 * R;
@@ -355,60 +383,10 @@ __global__ void __launch_bounds__(NW * 32, 1)
             }
         }
         cp_async_wait<0>();
-#pragma unroll
-        for (int k = 0; k < CPW; ++k) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc[k] = acc[k] + shfl_down(acc[k], o);
-            if (lane == 0) red_c[warp][k] = acc[k];
-        }
-        __syncthreads();
-        if (threadIdx.x < G * CPW) {
-            const int gg = threadIdx.x / CPW, k = threadIdx.x - gg * CPW;
-            const int c = c0 + gg * per + k;
-            if (k < per && c < m) {
-                C sacc = czero(C());
-                for (int sl = 0; sl < wpg; ++sl) sacc = sacc + red_c[gg * wpg + sl][k];
-                part[(long)blockIdx.x * m + c] = sacc;
-            }
-        }
-        __syncthreads();
+        project_sweep_end<C, CPW>(acc, red_c, c0, G, per, wpg, m, part);
     }
-    if (m == 0) {
-        for (long i = row0 + (long)threadIdx.x * R; i < row1; i += (long)NT * R) {
-            C rv[R];
-            load_c<R>(r + i, rv);
-            if (rec.on) {
-                C xv[R], xpv[R];
-                load_c<R>(rec.x + i, xv);
-                load_c<R>(rec.xp + i, xpv);
-#pragma unroll
-                for (int q = 0; q < R; ++q) rv[q] = rv[q] - alpha * xv[q] - beta * xpv[q];
-            }
-#pragma unroll
-            for (int q = 0; q < R; ++q) r2acc += abs2(rv[q]);
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) r2acc += __shfl_down_sync(0xffffffffu, r2acc, o);
-    if (lane == 0) red_r2[warp] = r2acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double sacc = 0.0;
-        for (int w = 0; w < W; ++w) sacc += red_r2[w];
-        part_r2[blockIdx.x] = sacc;
-    }
-    if (last_block_arrived(ticket)) {
-        __shared__ C red_cols[NT];
-        __shared__ double red_r2x[32];
-        const int nb = gridDim.x;
-        const double h2 = reduce_columns(part, nb, m, h, red_cols);
-        const double r2 = sum_partials(part_r2, nb, red_r2x);
-        if (threadIdx.x == 0) {
-            out2[0] = r2;
-            out2[1] = h2;
-            *ticket = 0;
-        }
-    }
+    if (m == 0) r2acc = project_norm_only<R, NT>(r, rec, alpha, beta, row0, row1);
+    project_finish<C, NT>(r2acc, part, part_r2, ticket, h, out2, m);
 }
 
 // ---------------------------------------------------------------------------
