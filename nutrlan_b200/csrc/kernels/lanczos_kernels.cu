@@ -602,8 +602,13 @@ __global__ void __launch_bounds__(kThreads)
     using Sh = MmaShape<BN>;
     constexpr int BM = Sh::BM, APITCH = BM + 4, BPITCH = BN + 4;
     static_assert(APITCH % 16 == 4 && BPITCH % 16 == 4 && (APITCH * 8) % 16 == 0, "bank-spread pitches");
-    constexpr int R = S::R;              // elements per 16-byte load
-    constexpr int CH = BM / R / 16;      // 16-byte chunks per thread per stage
+    // Rows per load: two for every storage type (a 16-byte FP64 load, an
+    // 8-byte FP32 one), so that each thread's two rows land in shared memory
+    // as one conflict-free 16-byte store (four FP32 rows per thread spread a
+    // half-warp's stores over twice the banks' wavefronts).
+    constexpr int R = 2;
+    static_assert(std::is_same<T, double>::value || std::is_same<T, float>::value, "real storage only");
+    constexpr int CH = BM / R / 16;      // loads per thread per stage
     constexpr int BPT = BN * kBK / kThreads;
     __shared__ __align__(16) double As[kBK][APITCH];
     __shared__ double Bs[kBK][BPITCH];
@@ -624,10 +629,16 @@ __global__ void __launch_bounds__(kThreads)
             const T *col = in_cols[c] + i0;
 #pragma unroll
             for (int j = 0; j < CH; ++j) {
-                double v[R];
-                S::load(col + (a_ch + 16 * j) * R, v);
-#pragma unroll
-                for (int r = 0; r < R; ++r) areg[j * R + r] = v[r];
+                const T *p = col + (a_ch + 16 * j) * R;
+                if constexpr (std::is_same<T, float>::value) {
+                    const float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+                    areg[j * R] = v.x;
+                    areg[j * R + 1] = v.y;
+                } else {
+                    const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+                    areg[j * R] = v.x;
+                    areg[j * R + 1] = v.y;
+                }
             }
         } else {
 #pragma unroll
